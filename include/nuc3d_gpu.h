@@ -1,0 +1,137 @@
+/*
+ * nuc3d_gpu.h -- C ABI of the B200 implementation of NUC3d's per-block right-hand
+ * side and TVD-RK3 update (libnuc3d_b200.so).
+ *
+ * Plain C types only.  Every entry point returns 0 (NUC3D_OK) or an error code;
+ * nuc3d_last_error() gives a message for the calling thread.  Host arrays are
+ * the reference's field3d layout: [nz][ny][nx] doubles, i fastest
+ * (src/field.h:11-81, index k*nx*ny + j*nx + i); multi-component arrays are
+ * stacked component-major (component c of cell idx at c*N + idx).
+ *
+ * What each entry point replaces in juncas/NUC3d (paths relative to the project):
+ *   nuc3d_create            fieldOperator3d (src/fieldOperator.cpp:20-87, Method.in),
+ *                           physicsModel (src/physicsModel.cpp:13-112, PhysModel.in)
+ *   nuc3d_block_add         block::initial's per-rank block + BC_Topo
+ *                           (src/block.cpp:31-100, src/boundaryConditions.cpp:25-93)
+ *   nuc3d_block_set_metrics block::getJacobians output (src/block.cpp:237-325):
+ *                           EulerData3D::jacobian, xi_xyz, eta_xyz, zeta_xyz, dx, dy, dz
+ *                           (src/euler3d.h:38-46)
+ *   nuc3d_block_set_q/get_q PDEData3d::Q_work = U/J (src/PDEData3d.hpp:39-44),
+ *                           restart read/write (src/block.cpp:754-855)
+ *   nuc3d_rhs               EulerData3D::solve / NaiverStokesData3d::solve
+ *                           (src/euler3d.cpp:248-262, src/NaiverStokes3d.cpp:36-49) + getDt
+ *   nuc3d_block_get_rhs     PDEData3d::RHS (src/PDEData3d.hpp:44)
+ *   nuc3d_step              block::solve: 3 x (RHS; PDEData3d::solve -> tvdrk3rd)
+ *                           (src/block.cpp:569-594, src/PDEData3d.cpp:152-170,
+ *                           src/TVD-RK3.cpp:16-137), time += dt
+ *   (MPI halo exchange, src/MPICommunicator.cpp:36-115, has no entry point: blocks
+ *    added to one context read each other's cells directly on the device.)
+ */
+#ifndef NUC3D_GPU_H
+#define NUC3D_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  NUC3D_OK = 0,
+  NUC3D_EINVAL = 1,    /* bad argument or configuration */
+  NUC3D_ECUDA = 2,     /* CUDA runtime error */
+  NUC3D_ESTATE = 3,    /* call out of order (e.g. stepping before finalize) */
+  NUC3D_ENUMERIC = 4,  /* a kernel flagged negative pressure or a non-finite state */
+  NUC3D_ENOTSUP = 5    /* configuration the library does not implement */
+};
+
+/* status bits returned by nuc3d_get_status */
+enum {
+  NUC3D_ST_NEG_PRESSURE = 1, /* EoS pressure < 0: the reference exits (src/physicsModel.cpp:1009-1016) */
+  NUC3D_ST_ENERGY_RESET = 2, /* internal energy < 0 was reset (src/physicsModel.cpp:324-332) */
+  NUC3D_ST_NONFINITE = 4,    /* the RK update produced a NaN or Inf */
+  NUC3D_ST_BAD_LAUNCH = 8
+};
+
+typedef struct nuc3d_ctx nuc3d_ctx;
+
+typedef struct {
+  /* Method.in: scheme_{x,y,z}_ivs and scheme_{x,y,z}_vis (src/fieldOperator.cpp:20-33).
+     ivs: "weno5js" | "weno5z" | "weno7js"; vis: "cd6". */
+  const char *scheme_ivs[3];
+  const char *scheme_vis[3];
+  /* PhysModel.in positional entries (src/physicsModel.cpp:65-69):
+     riemann "LF" | "AUSM" | "AUSMp"; model "Euler3d" | "NavierStokes3d". */
+  const char *riemann;
+  const char *model;
+  /* PhysModel.in key/values (src/physicsModel.cpp:41-51) */
+  double reynolds, mach, prandtl, gamma, t_ref, t_inf, t_wall;
+  /* IOController.in cfl (src/IOcontroller.cpp:22-29) */
+  double cfl;
+  /* 1: reference operation order, no FMA contraction (bit-comparable with the
+        reference on x86-64); 0: throughput arithmetic (agrees to round-off). */
+  int exact;
+  /* 1: reproduce the interior positive-split WENO5-Z smoothness indicator of
+        src/weno5z.cpp:80 (reference behaviour); 0: textbook WENO5-Z. */
+  int weno5z_compat;
+} nuc3d_config;
+
+const char *nuc3d_last_error(void);
+
+int nuc3d_create(const nuc3d_config *cfg, int device, nuc3d_ctx **out);
+int nuc3d_destroy(nuc3d_ctx *ctx);
+
+/* Add a block of nx*ny*nz cells.  Faces are ordered xi-, xi+, eta-, eta+, zeta-, zeta+
+   as in BC_Topo_<rank>.in (src/boundaryConditions.cpp:69-93):
+     bc_type[f] = -1 for a physical face, else the index of the neighbour block;
+     bc_id[f]   = physical: 0 inlet, 1 outlet, 2 wall, 3 symmetry; else the neighbour's face.
+   bc_values: 6*5 doubles (rho, u, v, w, p per face, used by inlet faces); may be NULL. */
+int nuc3d_block_add(nuc3d_ctx *ctx, int nx, int ny, int nz, const int bc_type[6],
+                    const int bc_id[6], const double *bc_values, int *block_id);
+
+/* Metrics of a block (host arrays, N doubles per component):
+   jac: 1/det(d(x,y,z)/d(xi,eta,zeta)); xi_xyz, eta_xyz, zeta_xyz: 3N each;
+   dxyz: 9N (x_xi, x_eta, x_zeta, y_xi, y_eta, y_zeta, z_xi, z_eta, z_zeta), needed
+   only by symmetry faces, may be NULL otherwise. */
+int nuc3d_block_set_metrics(nuc3d_ctx *ctx, int block, const double *jac, const double *xi_xyz,
+                            const double *eta_xyz, const double *zeta_xyz, const double *dxyz);
+
+/* Validate the block topology and upload the descriptors.  Call once, after all
+   blocks are added and before any evaluation. */
+int nuc3d_finalize(nuc3d_ctx *ctx);
+
+/* Conservative state Q = U/J of a block (5N doubles, host memory). */
+int nuc3d_block_set_q(nuc3d_ctx *ctx, int block, const double *q);
+int nuc3d_block_get_q(nuc3d_ctx *ctx, int block, double *q);
+/* Device pointer of the block's current state (5N doubles), for callers that keep
+   their data in HBM. */
+int nuc3d_block_q_device(nuc3d_ctx *ctx, int block, double **dev_q);
+
+/* One right-hand-side evaluation of every block at the current state (no update).
+   dt_local receives min over blocks and directions of 1/max(|U|+c|grad xi|),
+   the reference's dt before the cfl factor (src/euler3d.cpp:429-435). */
+int nuc3d_rhs(nuc3d_ctx *ctx, double *dt_local);
+int nuc3d_block_get_rhs(nuc3d_ctx *ctx, int block, double *rhs);
+
+/* nsteps TVD-RK3 steps (each: three stages; dt fixed at stage 0 as cfl/max eigenvalue).
+   Asynchronous on the context's stream; nuc3d_sync waits and checks the status. */
+int nuc3d_step(nuc3d_ctx *ctx, int nsteps);
+int nuc3d_sync(nuc3d_ctx *ctx);
+/* time accumulated over the steps and the dt of the last step */
+int nuc3d_get_time(nuc3d_ctx *ctx, double *time, double *dt);
+int nuc3d_set_time(nuc3d_ctx *ctx, double time);
+int nuc3d_get_status(nuc3d_ctx *ctx, unsigned *status);
+
+/* CUDA stream (cudaStream_t) the context launches on; NULL = its own stream. */
+int nuc3d_set_stream(nuc3d_ctx *ctx, void *stream);
+/* 1: replay the three stages of a step as one CUDA graph (default); 0: launch directly. */
+int nuc3d_use_graph(nuc3d_ctx *ctx, int on);
+
+/* Debug taps: NS primitives (u, v, w, T: 4N) and contravariant viscous fluxes
+   ([dir][var 1..4]: 12N) of the last evaluation. */
+int nuc3d_block_get_prim(nuc3d_ctx *ctx, int block, double *prim);
+int nuc3d_block_get_vis(nuc3d_ctx *ctx, int block, double *vis);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NUC3D_GPU_H */

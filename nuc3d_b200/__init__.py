@@ -1,0 +1,285 @@
+"""nuc3d_b200 -- NUC3d's per-block right-hand side and TVD-RK3 update on one B200.
+
+Python view of the C ABI in include/nuc3d_gpu.h (libnuc3d_b200.so, built in-tree
+by ``python -m nuc3d_b200.build``).  The configuration mirrors the reference's
+input files: ``Config.scheme_ivs``/``scheme_vis`` are Method.in's
+scheme_{x,y,z}_ivs/_vis (src/fieldOperator.cpp:20-33), ``riemann``/``model`` and
+the physical constants are PhysModel.in (src/physicsModel.cpp:41-69), ``cfl`` is
+IOController.in's (src/IOcontroller.cpp:22-29).  A block is described the way
+BC_Topo_<rank>.in does it (src/boundaryConditions.cpp:69-93).
+
+There is no CPU path: importing this package without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from .metrics import metrics_from_nodes  # noqa: F401  (host-side block::getJacobians)
+
+_LIB_PATH = Path(__file__).resolve().parent / "libnuc3d_b200.so"
+
+NUC3D_OK, NUC3D_EINVAL, NUC3D_ECUDA, NUC3D_ESTATE, NUC3D_ENUMERIC, NUC3D_ENOTSUP = range(6)
+ST_NEG_PRESSURE, ST_ENERGY_RESET, ST_NONFINITE = 1, 2, 4
+BC_INLET, BC_OUTLET, BC_WALL, BC_SYMM = 0, 1, 2, 3
+
+EXPORTED = (
+    "nuc3d_last_error", "nuc3d_create", "nuc3d_destroy", "nuc3d_block_add",
+    "nuc3d_block_set_metrics", "nuc3d_finalize", "nuc3d_block_set_q", "nuc3d_block_get_q",
+    "nuc3d_block_q_device", "nuc3d_rhs", "nuc3d_block_get_rhs", "nuc3d_step", "nuc3d_sync",
+    "nuc3d_get_time", "nuc3d_set_time", "nuc3d_get_status", "nuc3d_set_stream",
+    "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis",
+)
+
+
+class Nuc3dError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"nuc3d error {code}: {msg}")
+        self.code = code
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = [
+        ("scheme_ivs", ctypes.c_char_p * 3),
+        ("scheme_vis", ctypes.c_char_p * 3),
+        ("riemann", ctypes.c_char_p),
+        ("model", ctypes.c_char_p),
+        ("reynolds", ctypes.c_double), ("mach", ctypes.c_double), ("prandtl", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("t_ref", ctypes.c_double), ("t_inf", ctypes.c_double),
+        ("t_wall", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("exact", ctypes.c_int), ("weno5z_compat", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def load_library() -> ctypes.CDLL:
+    """The CUDA library; raises if it was not built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise ImportError(f"{_LIB_PATH} is missing: build it with `python -m nuc3d_b200.build`")
+    lib = ctypes.CDLL(str(_LIB_PATH))
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    PD = ctypes.POINTER(ctypes.c_double)
+    lib.nuc3d_last_error.restype = ctypes.c_char_p
+    lib.nuc3d_create.argtypes = [ctypes.POINTER(_Cfg), I, ctypes.POINTER(P)]
+    lib.nuc3d_destroy.argtypes = [P]
+    lib.nuc3d_block_add.argtypes = [P, I, I, I, ctypes.POINTER(I), ctypes.POINTER(I), PD,
+                                    ctypes.POINTER(I)]
+    lib.nuc3d_block_set_metrics.argtypes = [P, I, PD, PD, PD, PD, PD]
+    lib.nuc3d_finalize.argtypes = [P]
+    lib.nuc3d_block_set_q.argtypes = [P, I, P]
+    lib.nuc3d_block_get_q.argtypes = [P, I, P]
+    lib.nuc3d_block_q_device.argtypes = [P, I, ctypes.POINTER(P)]
+    lib.nuc3d_rhs.argtypes = [P, PD]
+    lib.nuc3d_block_get_rhs.argtypes = [P, I, PD]
+    lib.nuc3d_step.argtypes = [P, I]
+    lib.nuc3d_sync.argtypes = [P]
+    lib.nuc3d_get_time.argtypes = [P, PD, PD]
+    lib.nuc3d_set_time.argtypes = [P, D]
+    lib.nuc3d_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint)]
+    lib.nuc3d_set_stream.argtypes = [P, P]
+    lib.nuc3d_use_graph.argtypes = [P, I]
+    lib.nuc3d_block_get_prim.argtypes = [P, I, PD]
+    lib.nuc3d_block_get_vis.argtypes = [P, I, PD]
+    for name in EXPORTED:
+        if name != "nuc3d_last_error":
+            getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != NUC3D_OK:
+        raise Nuc3dError(rc, load_library().nuc3d_last_error().decode())
+
+
+def _pd(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+@dataclass
+class Config:
+    """Method.in + PhysModel.in + cfl of the reference."""
+
+    scheme_ivs: tuple = ("weno5js", "weno5js", "weno5js")
+    scheme_vis: tuple = ("cd6", "cd6", "cd6")
+    riemann: str = "LF"
+    model: str = "Euler3d"
+    reynolds: float = 1000.0
+    mach: float = 0.5
+    prandtl: float = 0.72
+    gamma: float = 1.4
+    t_ref: float = 110.4
+    t_inf: float = 288.0
+    t_wall: float = 1.0
+    cfl: float = 0.5
+    exact: bool = True
+    weno5z_compat: bool = True
+
+    def _c(self) -> _Cfg:
+        c = _Cfg()
+        for d in range(3):
+            c.scheme_ivs[d] = self.scheme_ivs[d].encode()
+            c.scheme_vis[d] = self.scheme_vis[d].encode()
+        c.riemann = self.riemann.encode()
+        c.model = self.model.encode()
+        for k in ("reynolds", "mach", "prandtl", "gamma", "t_ref", "t_inf", "t_wall", "cfl"):
+            setattr(c, k, float(getattr(self, k)))
+        c.exact = int(bool(self.exact))
+        c.weno5z_compat = int(bool(self.weno5z_compat))
+        return c
+
+
+@dataclass
+class BlockSpec:
+    shape: tuple                      # (nx, ny, nz) cells
+    bc_type: tuple                    # 6 faces: -1 physical, else neighbour block index
+    bc_id: tuple                      # physical BC id or neighbour face
+    bc_values: np.ndarray | None = None  # (6, 5) inlet primitive states
+    dims: tuple = field(init=False)
+
+    def __post_init__(self):
+        self.dims = tuple(int(x) for x in self.shape)
+
+
+class Solver:
+    """One context: a set of blocks advanced together on one GPU."""
+
+    def __init__(self, cfg: Config, device: int = 0):
+        self.lib = load_library()
+        self.cfg = cfg
+        self._ctx = ctypes.c_void_p()
+        self._cfg_c = cfg._c()
+        _check(self.lib.nuc3d_create(ctypes.byref(self._cfg_c), device, ctypes.byref(self._ctx)))
+        self.blocks: list[tuple] = []
+
+    # -- set-up ---------------------------------------------------------------
+    def add_block(self, nx, ny, nz, bc_type, bc_id, bc_values=None) -> int:
+        t = (ctypes.c_int * 6)(*[int(x) for x in bc_type])
+        i = (ctypes.c_int * 6)(*[int(x) for x in bc_id])
+        vals = None
+        if bc_values is not None:
+            vals = _f64(bc_values).reshape(30)
+            self._keep = vals
+        out = ctypes.c_int()
+        _check(self.lib.nuc3d_block_add(self._ctx, nx, ny, nz, t, i,
+                                        _pd(vals) if vals is not None else None,
+                                        ctypes.byref(out)))
+        self.blocks.append((nx, ny, nz))
+        return out.value
+
+    def set_metrics(self, b, jac, xi_xyz, eta_xyz, zeta_xyz, dxyz=None) -> None:
+        arrs = [_f64(a) for a in (jac, xi_xyz, eta_xyz, zeta_xyz)]
+        dx = _f64(dxyz) if dxyz is not None else None
+        _check(self.lib.nuc3d_block_set_metrics(self._ctx, b, *[_pd(a) for a in arrs],
+                                                _pd(dx) if dx is not None else None))
+
+    def set_mesh(self, b, x, y, z) -> dict:
+        """Metrics of block b from its node coordinates (block::getJacobians)."""
+        m = metrics_from_nodes(x, y, z)
+        self.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
+        return m
+
+    def finalize(self) -> None:
+        _check(self.lib.nuc3d_finalize(self._ctx))
+
+    # -- state ----------------------------------------------------------------
+    def _shape5(self, b):
+        nx, ny, nz = self.blocks[b]
+        return (5, nz, ny, nx)
+
+    def set_q(self, b, q) -> None:
+        q = _f64(q)
+        if q.shape != self._shape5(b):
+            q = q.reshape(self._shape5(b))
+        _check(self.lib.nuc3d_block_set_q(self._ctx, b, q.ctypes.data))
+        _check(self.lib.nuc3d_sync(self._ctx))
+
+    def set_q_ptr(self, b, host_ptr: int) -> None:
+        """Asynchronous upload from a host pointer (e.g. pinned memory)."""
+        _check(self.lib.nuc3d_block_set_q(self._ctx, b, ctypes.c_void_p(host_ptr)))
+
+    def get_q(self, b) -> np.ndarray:
+        out = np.empty(self._shape5(b), dtype=np.float64)
+        _check(self.lib.nuc3d_block_get_q(self._ctx, b, out.ctypes.data))
+        return out
+
+    def get_q_ptr(self, b, host_ptr: int) -> None:
+        _check(self.lib.nuc3d_block_get_q(self._ctx, b, ctypes.c_void_p(host_ptr)))
+
+    def q_device_ptr(self, b) -> int:
+        p = ctypes.c_void_p()
+        _check(self.lib.nuc3d_block_q_device(self._ctx, b, ctypes.byref(p)))
+        return p.value
+
+    # -- evaluation -----------------------------------------------------------
+    def rhs(self) -> float:
+        dt = ctypes.c_double()
+        _check(self.lib.nuc3d_rhs(self._ctx, ctypes.byref(dt)))
+        return dt.value
+
+    def get_rhs(self, b) -> np.ndarray:
+        out = np.empty(self._shape5(b), dtype=np.float64)
+        _check(self.lib.nuc3d_block_get_rhs(self._ctx, b, _pd(out)))
+        return out
+
+    def get_prim(self, b) -> np.ndarray:
+        nx, ny, nz = self.blocks[b]
+        out = np.empty((4, nz, ny, nx), dtype=np.float64)
+        _check(self.lib.nuc3d_block_get_prim(self._ctx, b, _pd(out)))
+        return out
+
+    def get_vis(self, b) -> np.ndarray:
+        nx, ny, nz = self.blocks[b]
+        out = np.empty((3, 4, nz, ny, nx), dtype=np.float64)
+        _check(self.lib.nuc3d_block_get_vis(self._ctx, b, _pd(out)))
+        return out
+
+    def step(self, n: int = 1, sync: bool = True) -> None:
+        _check(self.lib.nuc3d_step(self._ctx, int(n)))
+        if sync:
+            self.sync()
+
+    def sync(self) -> None:
+        _check(self.lib.nuc3d_sync(self._ctx))
+
+    def time_dt(self) -> tuple:
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.nuc3d_get_time(self._ctx, ctypes.byref(t), ctypes.byref(dt)))
+        return t.value, dt.value
+
+    def set_time(self, t: float) -> None:
+        _check(self.lib.nuc3d_set_time(self._ctx, float(t)))
+
+    def status(self) -> int:
+        s = ctypes.c_uint()
+        _check(self.lib.nuc3d_get_status(self._ctx, ctypes.byref(s)))
+        return s.value
+
+    def use_graph(self, on: bool) -> None:
+        _check(self.lib.nuc3d_use_graph(self._ctx, int(bool(on))))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        _check(self.lib.nuc3d_set_stream(self._ctx, ctypes.c_void_p(stream_ptr or 0)))
+
+    def close(self) -> None:
+        if self._ctx:
+            self.lib.nuc3d_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,107 @@
+// common.h -- host/device descriptors shared by the NUC3d B200 kernels and the C-ABI.
+//
+// Data layout in HBM (one block = one structured grid of nx*ny*nz cells):
+//   every field is a plain [nz][ny][nx] array of doubles (i fastest), the layout of
+//   the reference's field3d (src/field.h:11-81, index k*nx*ny + j*nx + i);
+//   multi-component fields are stacked component-major: comp*N + idx.
+// Direction-transposed copies of the reference (src/euler3d.cpp:75-80) are not
+// materialised: each sweep kernel walks its own axis through strides.
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+namespace nuc3d {
+
+enum Scheme : int { SCH_WENO5JS = 0, SCH_WENO5Z = 1, SCH_WENO7JS = 2, SCH_CRWENO5 = 3, SCH_HCCS = 4 };
+enum Riemann : int { RIE_LF = 0, RIE_AUSM = 1, RIE_AUSMP = 2 };
+enum Model : int { MODEL_EULER = 0, MODEL_NS = 1 };
+enum BcId : int { BC_INLET = 0, BC_OUTLET = 1, BC_WALL = 2, BC_SYMM = 3 };
+
+// Status bits written by kernels (atomicOr) and read back by the host.
+enum StatusBits : unsigned {
+  ST_NEG_PRESSURE = 1u,    // EoS pressure < 0 (the reference exits, src/physicsModel.cpp:1009-1016)
+  ST_ENERGY_RESET = 2u,    // internal energy < 0, E reset (src/physicsModel.cpp:324-332)
+  ST_NONFINITE = 4u,       // a non-finite value was produced by the RK update
+  ST_BAD_LAUNCH = 8u,      // a kernel found an inconsistent descriptor and skipped work
+};
+
+// Reference bufferSize per scheme (src/fieldOperator.cpp:127-283).
+inline __host__ __device__ int scheme_tilesize(int s) {
+  return (s == SCH_WENO7JS || s == SCH_HCCS) ? 4 : 3;
+}
+
+struct FaceDev {
+  int type;        // -1: physical boundary; >= 0: neighbour block index
+  int id;          // physical: BcId; neighbour: the neighbour's face 0..5
+  double bcv[5];   // inlet primitive state (rho, u, v, w, p), from BC_Topo values
+};
+
+// Everything a kernel needs to know about one block.  Pointers are device pointers.
+struct BlockDev {
+  int n[3];              // nx, ny, nz (cells)
+  int pad_;
+  long long N;           // nx*ny*nz
+  double *q[3];          // TVD-RK3 state buffers: q[0] = Q_n, q[1] = Q_1, q[2] = Q_2 (5*N each)
+  double *rhs;           // 5*N
+  const double *jac;     // N
+  const double *met[3];  // met[d] = 3*N: (d_x, d_y, d_z) of computational coordinate d
+  const double *dxyz;    // 9*N: x_xi, x_eta, x_zeta, y_xi, y_eta, y_zeta, z_xi, z_eta, z_zeta (or null)
+  double *prim;          // NS: u, v, w, T (4*N)
+  double *vis;           // NS: contravariant viscous fluxes, [dir][var 1..4] (12*N)
+  double *dvis;          // NS exact mode: d(Fv)/dxi and d(Gv)/deta, vars 1..4 (8*N)
+  FaceDev face[6];
+};
+
+struct SolverParams {
+  int scheme[3];         // per direction
+  int ts[3];             // per-direction bufferSize (scheme_tilesize)
+  int bfs;               // bfsize = max ts: width of the reference's ghost slabs
+  int riemann;
+  int model;
+  int weno5z_compat;     // 1: reproduce the interior positive is2 of src/weno5z.cpp:80
+  double gamma, mach, reynolds, prandtl, t_ref, t_inf, t_wall, cfl;
+};
+
+// Per-launch work list: tiles of every block, laid end to end.
+constexpr int kMaxBlocks = 512;
+struct TileMap {
+  int nblocks;
+  int tile_start[kMaxBlocks + 1];  // prefix sums of tiles per block
+};
+
+// Device-resident scalars of the time loop.
+struct StepState {
+  unsigned long long max_eig_bits;  // max over blocks and directions of |U|+c|grad xi| (bits of a double >= 0)
+  double dt;                        // cfl / max_eig, fixed at stage 0 of each step
+  double time;                      // accumulated time
+  unsigned status;                  // StatusBits
+  unsigned pad_;
+};
+
+// What the host hands to a stage launch.
+struct Launch {
+  const BlockDev *d_blocks;
+  StepState *d_state;
+  SolverParams P;
+  TileMap tm_dir[3];
+  TileMap tm_cells;
+  cudaStream_t stream;
+};
+
+// One right-hand-side evaluation of every block at RK stage `stage`
+// (state q[stage]); rk: also apply the TVD-RK3 update; eig: reduce the
+// eigenvalue maximum that fixes dt.  Defined once per arithmetic mode.
+// configure(): one-time kernel attributes (dynamic shared memory opt-in).
+// tile_count(): CTAs of the dir-sweep over one block of n cells.
+namespace exact {
+cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t configure();
+int tile_count(int dir, const int n[3]);
+}
+namespace fast {
+cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t configure();
+int tile_count(int dir, const int n[3]);
+}
+
+}  // namespace nuc3d

@@ -1,0 +1,703 @@
+// kernels.cuh -- the per-stage kernels of the block RHS + TVD-RK3 update.
+//
+// Included twice: kernels_exact.cu (NUC3D_NS = exact, built with -fmad=false, the
+// reference's operation order, bit-comparable with the CPU oracle) and
+// kernels_fast.cu (NUC3D_NS = fast, FMA contraction and one-division WENO weights).
+//
+// One RK stage s (state Q_s = q[s]; stage 0 also fixes dt):
+//   [NS]  prim_kernel   u, v, w, T of every cell              (src/physicsModel.cpp:258-357)
+//   [NS]  grad_kernel   12 cd6 gradients, Sutherland, stress,   (src/NaiverStokes3d.cpp:63-326)
+//                       contravariant viscous fluxes
+//   sweep<0>  xi:   split F+/F- (src/physicsModel.cpp:420-760), ghost fill from the neighbour
+//                   block or the BC (src/boundaryConditions.cpp:95-1086), WENO faces
+//                   (src/euler3d.cpp:305-366), dF = F[i+1/2]-F[i-1/2] (:143-174),
+//                   RHS = dF; stage 0 also reduces max(|U|+c|grad xi|) over 3 directions
+//   sweep<1>  eta:  RHS += dG
+//   sweep<2>  zeta: RHS += dH, [NS] RHS -= dFv + dGv + dHv (src/NaiverStokes3d.cpp:401-513),
+//                   then the TVD-RK3 stage update (src/TVD-RK3.cpp:16-137) into q[s+1 mod 3]
+// Ghost cells across block faces are read directly from the neighbour block's
+// arrays in HBM; this replaces the MPI halo exchange (src/MPICommunicator.cpp:36-115).
+#pragma once
+#include <cuda_runtime.h>
+#include "schemes.cuh"
+
+namespace nuc3d {
+namespace NUC3D_NS {
+
+constexpr int kThreads = 256;
+
+// Tile of one sweep CTA: TW lines side by side, TL cells along each line.
+// xi lines are contiguous in memory; eta/zeta tiles put TW consecutive i in a row.
+template <int DIR> struct Tile;
+template <> struct Tile<0> { static constexpr int TW = 4, TL = 64; };
+template <> struct Tile<1> { static constexpr int TW = 8, TL = 32; };
+template <> struct Tile<2> { static constexpr int TW = 8, TL = 32; };
+
+template <int SCH> struct Halo { static constexpr int R = (SCH == SCH_WENO7JS) ? 4 : 3; };
+
+struct Geo {
+  int L, nW, nO;
+  long long sL, sW, sO;
+};
+
+__host__ __device__ inline Geo make_geo(int dir, const int n[3]) {
+  Geo g;
+  long long nxy = (long long)n[0] * n[1];
+  if (dir == 0) {
+    g.L = n[0]; g.nW = n[1]; g.nO = n[2]; g.sL = 1; g.sW = n[0]; g.sO = nxy;
+  } else if (dir == 1) {
+    g.L = n[1]; g.nW = n[0]; g.nO = n[2]; g.sL = n[0]; g.sW = 1; g.sO = nxy;
+  } else {
+    g.L = n[2]; g.nW = n[0]; g.nO = n[1]; g.sL = nxy; g.sW = 1; g.sO = n[0];
+  }
+  return g;
+}
+
+template <int DIR>
+__host__ __device__ inline int sweep_tiles(const int n[3]) {
+  Geo g = make_geo(DIR, n);
+  return ((g.L + Tile<DIR>::TL - 1) / Tile<DIR>::TL) * ((g.nW + Tile<DIR>::TW - 1) / Tile<DIR>::TW) *
+         g.nO;
+}
+
+template <int DIR, int SCH>
+__host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
+  constexpr int R = Halo<SCH>::R, TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
+  size_t n = (size_t)10 * TW * (TL + 2 * R) + (size_t)5 * TW * (TL + 1);
+  if (ns) n += (size_t)4 * TW * (TL + 6);
+  if (DIR == 2) n += (size_t)5 * TW * TL;
+  return n * sizeof(double);
+}
+
+__device__ __forceinline__ int find_block(const TileMap &tm, int t) {
+  int lo = 0, hi = tm.nblocks - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (tm.tile_start[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Cell across face 2*d+side seen from line position g (g < 0 or g >= n[d]) of the
+// line whose slab coordinates are (a, b).  The reference copies a raw slab of
+// bfsize cells (bufferData::setBufferSend, src/bufferData.cpp:103-239) and indexes
+// it g+bfsize on the left, g-n on the right (src/weno5js.cpp:257-262,475-480);
+// slab coordinates are (j,k) for xi faces, (k,i) for eta, (i,j) for zeta.
+// Returns the neighbour block (or -1 for a physical face) and its cell index.
+__device__ __forceinline__ int ghost_cell(const BlockDev *__restrict__ blocks, const BlockDev &B,
+                                          int d, int g, int a, int b, int bfs, long long &nidx) {
+  const int L = B.n[d];
+  const int side = g < 0 ? 0 : 1;
+  const FaceDev &F = B.face[2 * d + side];
+  if (F.type < 0) return -1;
+  const int slot = side == 0 ? g + bfs : g - L;
+  const int A = d == 0 ? B.n[1] : (d == 1 ? B.n[2] : B.n[0]);
+  const long long rem = a + (long long)A * b;
+  const BlockDev &NB = blocks[F.type];
+  const int d2 = F.id >> 1, s2 = F.id & 1;
+  const int A2 = d2 == 0 ? NB.n[1] : (d2 == 1 ? NB.n[2] : NB.n[0]);
+  const int a2 = (int)(rem % A2), b2 = (int)(rem / A2);
+  const int pos2 = s2 == 0 ? slot : NB.n[d2] - bfs + slot;
+  int i, j, k;
+  if (d2 == 0) { i = pos2; j = a2; k = b2; }
+  else if (d2 == 1) { i = b2; j = pos2; k = a2; }
+  else { i = a2; j = b2; k = pos2; }
+  nidx = ((long long)k * NB.n[1] + j) * NB.n[0] + i;
+  return F.type;
+}
+
+__device__ __forceinline__ void load_q(const double *__restrict__ Qs, long long N, long long idx,
+                                       double q[5]) {
+#pragma unroll
+  for (int v = 0; v < 5; ++v) q[v] = __ldg(Qs + v * N + idx);
+}
+
+// Split flux of a cell of block B along direction d (own cell or a neighbour's ghost).
+__device__ __forceinline__ void cell_split(const BlockDev &B, int stage, long long idx, int d,
+                                           const SolverParams &P, double fp[5], double fn[5],
+                                           CellPrim &s, double q[5], unsigned &st) {
+  const long long N = B.N;
+  load_q(B.q[stage], N, idx, q);
+  const double jac = __ldg(B.jac + idx);
+  con2prim(q, jac, P.gamma, P.mach, s, st);
+  q[4] = s.q4;
+  const double *m = B.met[d];
+  split_cell(P.riemann, q, s, __ldg(m + idx), __ldg(m + N + idx), __ldg(m + 2 * N + idx), jac, fp, fn);
+}
+
+// Ghost split flux at a physical face (src/boundaryConditions.cpp:140-1086): the
+// point solver evaluated at the edge cell's metric with the BC state.  Only the
+// ghost next to the face enters the reconstruction (face 0 takes the last ghost
+// slot for F+, face n the first slot for F-: src/reconstructionBoundaryScheme.cpp:88-106,289-308),
+// and for the mirrored wall/symmetry ghosts that slot mirrors the edge cell itself
+// (iblock = 0 or n-1, src/boundaryConditions.cpp:525-526).
+__device__ __forceinline__ void bc_ghost_flux(const BlockDev &B, int stage, int d, int side,
+                                              long long eidx, const SolverParams &P, double out[5],
+                                              unsigned &st) {
+  const FaceDev &F = B.face[2 * d + side];
+  const long long N = B.N;
+  const double jac = __ldg(B.jac + eidx);
+  const double *m = B.met[d];
+  const double xx = __ldg(m + eidx), xy = __ldg(m + N + eidx), xz = __ldg(m + 2 * N + eidx);
+  double qb[5];
+  if (F.id == BC_INLET) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qb[v] = F.bcv[v];
+  } else {
+    double q[5];
+    CellPrim s;
+    load_q(B.q[stage], N, eidx, q);
+    con2prim(q, jac, P.gamma, P.mach, s, st);
+    qb[0] = s.rho; qb[1] = s.u; qb[2] = s.v; qb[3] = s.w; qb[4] = s.p;
+    if (F.id == BC_WALL) {
+      // src/boundaryConditions.cpp:564-567
+      qb[0] = qb[4] * P.gamma * P.mach * P.mach / P.t_wall;
+      qb[1] = 0.0; qb[2] = 0.0; qb[3] = 0.0;
+    } else if (F.id == BC_SYMM) {
+      // contravariant velocities and the mirror of the face-normal one
+      // (src/boundaryConditions.cpp:882-888, 971-977, 1061-1067)
+      const double *m0 = B.met[0], *m1 = B.met[1], *m2 = B.met[2];
+      const double u = qb[1], v = qb[2], w = qb[3];
+      double U = __ldg(m0 + eidx) * u + __ldg(m0 + N + eidx) * v + __ldg(m0 + 2 * N + eidx) * w;
+      double V = __ldg(m1 + eidx) * u + __ldg(m1 + N + eidx) * v + __ldg(m1 + 2 * N + eidx) * w;
+      double W = __ldg(m2 + eidx) * u + __ldg(m2 + N + eidx) * v + __ldg(m2 + 2 * N + eidx) * w;
+      const double *X = B.dxyz;
+      double t[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) t[c] = __ldg(X + c * N + eidx);
+      // t = x_xi x_eta x_zeta y_xi y_eta y_zeta z_xi z_eta z_zeta
+      if (d == 0) {
+        qb[1] = -t[0] * U + t[1] * V + t[2] * W;
+        qb[2] = -t[3] * U + t[4] * V + t[5] * W;
+        qb[3] = -t[6] * U + t[7] * V + t[8] * W;
+      } else if (d == 1) {
+        qb[1] = t[0] * U - t[1] * V + t[2] * W;
+        qb[2] = t[3] * U - t[4] * V + t[5] * W;
+        qb[3] = t[6] * U - t[7] * V + t[8] * W;
+      } else {
+        qb[1] = t[0] * U + t[1] * V - t[2] * W;
+        qb[2] = t[3] * U + t[4] * V - t[5] * W;
+        qb[3] = t[6] * U + t[7] * V - t[8] * W;
+      }
+    }
+  }
+  split_point(P.riemann, qb, jac, xx, xy, xz, P.gamma, side, out, st);
+}
+
+// Reconstructed F+ at face f from the split fluxes P(c) of cells c (line coordinates).
+// Faces next to a physical face use ReconstructionboundaryScheme
+// (src/reconstructionBoundaryScheme.cpp:52-313); the right side is tested first
+// because the reference applies BR after BL.
+template <int SCH, class Acc>
+__device__ __forceinline__ double recon_pos(int f, int L, int ts, bool physL, bool physR,
+                                            bool compat, Acc P) {
+  if (physR && f > L - ts) {
+    switch (L - f) {
+      case 0: return P(L - 1);
+      case 1: return rb_second(P(L - 2), P(L - 1));
+      case 2: return rb_third(P(L - 4), P(L - 3), P(L - 2));
+      default: return weno5js(P(L - 6), P(L - 5), P(L - 4), P(L - 3), P(L - 2));
+    }
+  }
+  if (physL && f < ts) {
+    switch (f) {
+      case 0: return P(-1);
+      case 1: return rb_second(P(0), P(1));
+      case 2: return rb_third(P(0), P(1), P(2));
+      default: return weno5js(P(0), P(1), P(2), P(3), P(4));
+    }
+  }
+  if (SCH == SCH_WENO7JS) {
+    double s[7] = {P(f - 4), P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), P(f + 2)};
+    return weno7js(s);
+  } else if (SCH == SCH_WENO5Z) {
+    return weno5z(P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), compat && f >= ts && f <= L - ts);
+  } else {
+    return weno5js(P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1));
+  }
+}
+
+template <int SCH, class Acc>
+__device__ __forceinline__ double recon_neg(int f, int L, int ts, bool physL, bool physR, Acc Nf) {
+  if (physR && f > L - ts) {
+    switch (L - f) {
+      case 0: return Nf(L);
+      case 1: return rb_second(Nf(L - 1), Nf(L - 2));
+      case 2: return rb_third(Nf(L - 1), Nf(L - 2), Nf(L - 3));
+      default: return weno5js(Nf(L - 1), Nf(L - 2), Nf(L - 3), Nf(L - 4), Nf(L - 5));
+    }
+  }
+  if (physL && f < ts) {
+    switch (f) {
+      case 0: return Nf(0);
+      case 1: return rb_second(Nf(1), Nf(0));
+      case 2: return rb_third(Nf(3), Nf(2), Nf(1));
+      default: return weno5js(Nf(5), Nf(4), Nf(3), Nf(2), Nf(1));
+    }
+  }
+  if (SCH == SCH_WENO7JS) {
+    double s[7] = {Nf(f + 3), Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), Nf(f - 3)};
+    return weno7js(s);
+  } else if (SCH == SCH_WENO5Z) {
+    return weno5z(Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), false);
+  } else {
+    return weno5js(Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2));
+  }
+}
+
+// d/dxi of a cell-centred field at line position c: boundaryScheme within ts cells
+// of a physical face (src/fieldOperator.cpp:523-624, src/boundaryScheme.cpp:311-406),
+// cd6 elsewhere (ghost values come from the neighbour across the face).
+template <class Acc>
+__device__ __forceinline__ double diff_at(int c, int L, int ts, bool physL, bool physR, Acc V) {
+  if (physR && c >= L - ts) {
+    switch (L - 1 - c) {
+      case 0: return V(c) - V(c - 1);
+      case 1: return bnd_second(V(c - 1), V(c + 1));
+      case 2: return bnd_fourth(V(c - 2), V(c - 1), V(c + 1), V(c + 2));
+      default: return bnd_sixth(V(c - 3), V(c - 2), V(c - 1), V(c + 1), V(c + 2), V(c + 3));
+    }
+  }
+  if (physL && c < ts) {
+    switch (c) {
+      case 0: return V(c + 1) - V(c);
+      case 1: return bnd_second(V(c - 1), V(c + 1));
+      case 2: return bnd_fourth(V(c - 2), V(c - 1), V(c + 1), V(c + 2));
+      default: return bnd_sixth(V(c - 3), V(c - 2), V(c - 1), V(c + 1), V(c + 2), V(c + 3));
+    }
+  }
+  return cd6(V(c - 3), V(c - 2), V(c - 1), V(c + 1), V(c + 2), V(c + 3));
+}
+
+enum SweepFlags : int { SW_EIG = 1, SW_RK = 2, SW_NS = 4, SW_STORE_DVIS = 8 };
+
+// TVD-RK3 stage update of one value (src/TVD-RK3.cpp:57-136, coefficients src/TVD-RK3.h:9-12):
+// u_i is the stage state, u_n the state saved at stage 0, R the right-hand side.
+__device__ __forceinline__ double rk3_update(int stage, double R, double u_i, double u_n, double dt) {
+  double rhs = -R;
+  if (stage == 0) return 1.0 * u_i + 1.0 * rhs * dt;
+  if (stage == 1) return 3.0 / 4.0 * u_n + 1.0 / 4.0 * (rhs * dt + u_i);
+  return 1.0 / 3.0 * u_n + 2.0 / 3.0 * (rhs * dt + u_i);
+}
+
+template <int DIR, int SCH>
+__global__ void __launch_bounds__(kThreads)
+sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
+             int stage, int flags) {
+  constexpr int R = Halo<SCH>::R;
+  constexpr int TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
+  constexpr int NP = TL + 2 * R;
+  constexpr int NV = TL + 6;
+  extern __shared__ double smem[];
+  double *sF = smem;                       // [10][TW][NP]: F+ vars 0..4, F- vars 5..9
+  double *sH = sF + 10 * TW * NP;          // [5][TW][TL+1]: face fluxes
+  const bool ns = (flags & SW_NS) != 0;
+  double *sV = sH + 5 * TW * (TL + 1);     // [4][TW][NV]: viscous fluxes (NS)
+  double *sQ = sV + (ns ? 4 * TW * NV : 0);  // [5][TW][TL]: stage state (zeta sweep)
+  __shared__ double sRed[kThreads / 32];
+
+  const int t = blockIdx.x;
+  const int b = find_block(tm, t);
+  const BlockDev &B = blocks[b];
+  const int n[3] = {B.n[0], B.n[1], B.n[2]};
+  const Geo G = make_geo(DIR, n);
+  int lt = t - tm.tile_start[b];
+  const int nch = (G.L + TL - 1) / TL;
+  const int nwg = (G.nW + TW - 1) / TW;
+  const int ch = lt % nch;
+  lt /= nch;
+  const int wg = lt % nwg;
+  const int o = lt / nwg;
+  const int c0 = ch * TL;
+  const int cl = min(TL, G.L - c0);
+  const int w0 = wg * TW;
+  const int nw = min(TW, G.nW - w0);
+  const long long N = B.N;
+  const int ts = P.ts[DIR];
+  const bool physL = B.face[2 * DIR].type < 0;
+  const bool physR = B.face[2 * DIR + 1].type < 0;
+  const bool eig = (flags & SW_EIG) != 0;
+  unsigned st = 0;
+  double emax = 0.0;
+
+  // ---- phase 1: split fluxes at line positions c0-R .. c0+cl+R-1 ----
+  for (int e = threadIdx.x; e < TW * NP; e += kThreads) {
+    int p, w;
+    if (DIR == 0) { p = e % NP; w = e / NP; } else { w = e % TW; p = e / TW; }
+    double fp[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, fn[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const int g = c0 + p - R;
+    if (w < nw && p < cl + 2 * R) {
+      const int wl = w0 + w;
+      const int sa = (DIR == 1) ? o : wl, sb = (DIR == 1) ? wl : o;
+      double q[5];
+      CellPrim s;
+      if (g >= 0 && g < G.L) {
+        const long long idx = g * G.sL + wl * G.sW + o * G.sO;
+        cell_split(B, stage, idx, DIR, P, fp, fn, s, q, st);
+        if (eig && g >= c0 && g < c0 + cl) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double *m = B.met[d];
+            double ev = eigen_cell(s, __ldg(m + idx), __ldg(m + N + idx), __ldg(m + 2 * N + idx));
+            emax = ev > emax ? ev : emax;
+          }
+        }
+        if (DIR == 2 && g >= c0 && g < c0 + cl) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) sQ[(v * TW + w) * TL + (g - c0)] = q[v];
+        }
+      } else {
+        long long nidx;
+        const int nb = ghost_cell(blocks, B, DIR, g, sa, sb, P.bfs, nidx);
+        if (nb >= 0) {
+          cell_split(blocks[nb], stage, nidx, DIR, P, fp, fn, s, q, st);
+        } else if (g == -1) {
+          const long long eidx = 0 * G.sL + wl * G.sW + o * G.sO;
+          bc_ghost_flux(B, stage, DIR, 0, eidx, P, fp, st);
+        } else if (g == G.L) {
+          const long long eidx = (long long)(G.L - 1) * G.sL + wl * G.sW + o * G.sO;
+          bc_ghost_flux(B, stage, DIR, 1, eidx, P, fn, st);
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      sF[(v * TW + w) * NP + p] = fp[v];
+      sF[((5 + v) * TW + w) * NP + p] = fn[v];
+    }
+  }
+  if (ns) {
+    for (int e = threadIdx.x; e < TW * NV; e += kThreads) {
+      int p, w;
+      if (DIR == 0) { p = e % NV; w = e / NV; } else { w = e % TW; p = e / TW; }
+      double fv[4] = {0.0, 0.0, 0.0, 0.0};
+      const int g = c0 + p - 3;
+      if (w < nw && p < cl + 6) {
+        const int wl = w0 + w;
+        const int sa = (DIR == 1) ? o : wl, sb = (DIR == 1) ? wl : o;
+        const double *vis = nullptr;
+        long long idx = -1, NN = N;
+        if (g >= 0 && g < G.L) {
+          idx = g * G.sL + wl * G.sW + o * G.sO;
+          vis = B.vis;
+        } else {
+          long long nidx;
+          const int nb = ghost_cell(blocks, B, DIR, g, sa, sb, P.bfs, nidx);
+          if (nb >= 0) {
+            idx = nidx;
+            vis = blocks[nb].vis;
+            NN = blocks[nb].N;
+          }
+        }
+        if (vis) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v) fv[v] = __ldg(vis + (DIR * 4 + v) * NN + idx);
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) sV[(v * TW + w) * NV + p] = fv[v];
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 2: faces c0 .. c0+cl ----
+  const bool compat = P.weno5z_compat != 0;
+  for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
+    const int fl = e % (TL + 1), w = e / (TL + 1);
+    if (w >= nw || fl > cl) continue;
+    const int f = c0 + fl;
+#pragma unroll 1
+    for (int v = 0; v < 5; ++v) {
+      const double *rowP = sF + (v * TW + w) * NP + (R - c0);
+      const double *rowN = sF + ((5 + v) * TW + w) * NP + (R - c0);
+      auto Pacc = [rowP](int c) { return rowP[c]; };
+      auto Nacc = [rowN](int c) { return rowN[c]; };
+      double hp = recon_pos<SCH>(f, G.L, ts, physL, physR, compat, Pacc);
+      double hn = recon_neg<SCH>(f, G.L, ts, physL, physR, Nacc);
+      sH[(v * TW + w) * (TL + 1) + fl] = hp + hn;
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 3: cells: flux difference, RHS accumulation, RK stage ----
+  double *__restrict__ rhs = B.rhs;
+  double dt = 0.0;
+  if (flags & SW_RK) {
+    if (stage == 0) {
+      double me = __longlong_as_double((long long)S->max_eig_bits);
+      double dt_local = 1.0 / me;
+      dt = dt_local * P.cfl;
+      if (t == 0 && threadIdx.x == 0) S->dt = dt;
+    } else {
+      dt = S->dt;
+    }
+    if (stage == 2 && t == 0 && threadIdx.x == 0) S->time = S->time + dt;
+  }
+  for (int e = threadIdx.x; e < TW * TL; e += kThreads) {
+    int c, w;
+    if (DIR == 0) { c = e % TL; w = e / TL; } else { w = e % TW; c = e / TW; }
+    if (w >= nw || c >= cl) continue;
+    const int g = c0 + c;
+    const long long idx = g * G.sL + (w0 + w) * G.sW + o * G.sO;
+    double d[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double *h = sH + (v * TW + w) * (TL + 1);
+      d[v] = h[c + 1] - h[c];
+    }
+    double dv[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ns) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const double *row = sV + (v * TW + w) * NV + (3 - c0);
+        auto Vacc = [row](int cc) { return row[cc]; };
+        dv[v] = diff_at(g, G.L, ts, physL, physR, Vacc);
+      }
+    }
+    if (DIR == 0) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) rhs[v * N + idx] = d[v];
+      if (ns) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) B.dvis[v * N + idx] = dv[v];
+      }
+    } else if (DIR == 1) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) rhs[v * N + idx] = rhs[v * N + idx] + d[v];
+      if (ns) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) B.dvis[(4 + v) * N + idx] = dv[v];
+      }
+    } else {
+      double r[5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) r[v] = rhs[v * N + idx] + d[v];
+      if (ns) {
+#pragma unroll
+        for (int v = 1; v < 5; ++v) {
+          r[v] = r[v] - B.dvis[(v - 1) * N + idx];
+          r[v] = r[v] - B.dvis[(4 + v - 1) * N + idx];
+          r[v] = r[v] - dv[v - 1];
+        }
+      }
+      if (flags & SW_RK) {
+        double *__restrict__ qo = B.q[(stage + 1) % 3];
+        const double *__restrict__ qn = B.q[0];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const double ui = sQ[(v * TW + w) * TL + c];
+          const double un = stage == 0 ? 0.0 : qn[v * N + idx];
+          const double x = rk3_update(stage, r[v], ui, un, dt);
+          if (!isfinite(x)) st |= ST_NONFINITE;
+          qo[v * N + idx] = x;
+        }
+      } else {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) rhs[v * N + idx] = r[v];
+      }
+    }
+  }
+
+  if (eig) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      double x = __shfl_xor_sync(0xffffffffu, emax, off);
+      emax = x > emax ? x : emax;
+    }
+    if ((threadIdx.x & 31) == 0) sRed[threadIdx.x >> 5] = emax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = sRed[0];
+      for (int i = 1; i < kThreads / 32; ++i) m = sRed[i] > m ? sRed[i] : m;
+      atomicMax(&S->max_eig_bits, (unsigned long long)__double_as_longlong(m));
+    }
+  }
+  if (st) atomicOr(&S->status, st);
+}
+
+// ---------------------------------------------------------------------------------
+// Navier-Stokes: primitives, then gradients and viscous fluxes per cell.
+// ---------------------------------------------------------------------------------
+constexpr int kCellTile = 256;
+
+__global__ void __launch_bounds__(kCellTile)
+prim_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S, int stage) {
+  const int b = find_block(tm, blockIdx.x);
+  const BlockDev &B = blocks[b];
+  const long long idx = (long long)(blockIdx.x - tm.tile_start[b]) * kCellTile + threadIdx.x;
+  if (idx >= B.N) return;
+  const long long N = B.N;
+  unsigned st = 0;
+  double q[5];
+  CellPrim s;
+  load_q(B.q[stage], N, idx, q);
+  const double jac = __ldg(B.jac + idx);
+  con2prim(q, jac, P.gamma, P.mach, s, st);
+  B.prim[idx] = s.u;
+  B.prim[N + idx] = s.v;
+  B.prim[2 * N + idx] = s.w;
+  B.prim[3 * N + idx] = temperature(s.rho, s.p, P.gamma, P.mach);
+  if (st) atomicOr(&S->status, st);
+}
+
+// Value of primitive component comp at line offset g along direction d of cell (i,j,k).
+__device__ __forceinline__ double prim_along(const BlockDev *__restrict__ blocks, const BlockDev &B,
+                                             int d, int i, int j, int k, int g, int comp, int bfs) {
+  const int L = B.n[d];
+  if (g >= 0 && g < L) {
+    int ii = i, jj = j, kk = k;
+    if (d == 0) ii = g; else if (d == 1) jj = g; else kk = g;
+    const long long idx = ((long long)kk * B.n[1] + jj) * B.n[0] + ii;
+    return __ldg(B.prim + comp * B.N + idx);
+  }
+  const int a = d == 0 ? j : (d == 1 ? k : i);
+  const int bb = d == 0 ? k : (d == 1 ? i : j);
+  long long nidx;
+  const int nb = ghost_cell(blocks, B, d, g, a, bb, bfs, nidx);
+  if (nb < 0) return 0.0;  // never read: one-sided schemes stay inside the block
+  return __ldg(blocks[nb].prim + comp * blocks[nb].N + nidx);
+}
+
+// NaiverStokesData3d::solveGrads + solveViscousFlux (src/NaiverStokes3d.cpp:63-326)
+// with physicsModel::sutherland (src/physicsModel.cpp:199-234).
+__global__ void __launch_bounds__(kCellTile)
+grad_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P) {
+  const int b = find_block(tm, blockIdx.x);
+  const BlockDev &B = blocks[b];
+  const long long idx = (long long)(blockIdx.x - tm.tile_start[b]) * kCellTile + threadIdx.x;
+  if (idx >= B.N) return;
+  const long long N = B.N;
+  const int nx = B.n[0], ny = B.n[1];
+  const int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((long long)nx * ny));
+  const int pos[3] = {i, j, k};
+  double gr[4][3];  // [u,v,w,T][xi,eta,zeta]
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const bool pl = B.face[2 * d].type < 0, pr = B.face[2 * d + 1].type < 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      auto V = [&](int g) { return prim_along(blocks, B, d, i, j, k, g, c, P.bfs); };
+      gr[c][d] = diff_at(pos[d], B.n[d], P.ts[d], pl, pr, V);
+    }
+  }
+  const double jac = __ldg(B.jac + idx);
+  double mx[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) mx[d][c] = __ldg(B.met[d] + c * N + idx);
+  const double xi_x = mx[0][0], xi_y = mx[0][1], xi_z = mx[0][2];
+  const double eta_x = mx[1][0], eta_y = mx[1][1], eta_z = mx[1][2];
+  const double zeta_x = mx[2][0], zeta_y = mx[2][1], zeta_z = mx[2][2];
+
+  double ux = gr[0][0] * xi_x + gr[0][1] * eta_x + gr[0][2] * zeta_x;
+  double uy = gr[0][0] * xi_y + gr[0][1] * eta_y + gr[0][2] * zeta_y;
+  double uz = gr[0][0] * xi_z + gr[0][1] * eta_z + gr[0][2] * zeta_z;
+  double vx = gr[1][0] * xi_x + gr[1][1] * eta_x + gr[1][2] * zeta_x;
+  double vy = gr[1][0] * xi_y + gr[1][1] * eta_y + gr[1][2] * zeta_y;
+  double vz = gr[1][0] * xi_z + gr[1][1] * eta_z + gr[1][2] * zeta_z;
+  double wx = gr[2][0] * xi_x + gr[2][1] * eta_x + gr[2][2] * zeta_x;
+  double wy = gr[2][0] * xi_y + gr[2][1] * eta_y + gr[2][2] * zeta_y;
+  double wz = gr[2][0] * xi_z + gr[2][1] * eta_z + gr[2][2] * zeta_z;
+  double tx = gr[3][0] * xi_x + gr[3][1] * eta_x + gr[3][2] * zeta_x;
+  double ty = gr[3][0] * xi_y + gr[3][1] * eta_y + gr[3][2] * zeta_y;
+  double tz = gr[3][0] * xi_z + gr[3][1] * eta_z + gr[3][2] * zeta_z;
+
+  const double T = __ldg(B.prim + 3 * N + idx);
+  const double nd = P.t_ref / P.t_inf;
+  const double miu0 = (1.0 + nd) / (T + nd) * pow15(T) / P.reynolds;
+  const double coeff0 = miu0 / ((P.gamma - 1.0) * P.mach * P.mach * P.prandtl);
+
+  double grad = ux + vy + wz;
+  double tau_xx = miu0 * (2.0 * ux - 2.0 / 3.0 * grad);
+  double tau_xy = miu0 * (uy + vx - 2.0 / 3.0 * grad);
+  double tau_xz = miu0 * (uz + wx - 2.0 / 3.0 * grad);
+  double tau_yy = miu0 * (2.0 * vy - 2.0 / 3.0 * grad);
+  double tau_yz = miu0 * (vz + wy - 2.0 / 3.0 * grad);
+  double tau_zz = miu0 * (2.0 * wz - 2.0 / 3.0 * grad);
+  double tau_tx = coeff0 * tx;
+  double tau_ty = coeff0 * ty;
+  double tau_tz = coeff0 * tz;
+  const double u = __ldg(B.prim + idx), v = __ldg(B.prim + N + idx), w = __ldg(B.prim + 2 * N + idx);
+  double fv[4] = {tau_xx, tau_xy, tau_xz, u * tau_xx + v * tau_xy + w * tau_xz + tau_tx};
+  double gv[4] = {tau_xy, tau_yy, tau_yz, u * tau_xy + v * tau_yy + w * tau_yz + tau_ty};
+  double hv[4] = {tau_xz, tau_yz, tau_zz, u * tau_xz + v * tau_yz + w * tau_zz + tau_tz};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    B.vis[(0 * 4 + c) * N + idx] = (xi_x * fv[c] + xi_y * gv[c] + xi_z * hv[c]) / jac;
+    B.vis[(1 * 4 + c) * N + idx] = (eta_x * fv[c] + eta_y * gv[c] + eta_z * hv[c]) / jac;
+    B.vis[(2 * 4 + c) * N + idx] = (zeta_x * fv[c] + zeta_y * gv[c] + zeta_z * hv[c]) / jac;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Host-side launchers (called by the C-ABI layer).
+// ---------------------------------------------------------------------------------
+template <int DIR, int SCH>
+inline cudaError_t launch_sweep_t(const Launch &L, int stage, int flags) {
+  const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
+  const size_t smem = sweep_smem_bytes<DIR, SCH>((flags & SW_NS) != 0);
+  sweep_kernel<DIR, SCH><<<ntiles, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[DIR], L.P,
+                                                               L.d_state, stage, flags);
+  return cudaGetLastError();
+}
+
+template <int DIR>
+inline cudaError_t launch_sweep(const Launch &L, int stage, int flags) {
+  switch (L.P.scheme[DIR]) {
+    case SCH_WENO5JS: return launch_sweep_t<DIR, SCH_WENO5JS>(L, stage, flags);
+    case SCH_WENO5Z: return launch_sweep_t<DIR, SCH_WENO5Z>(L, stage, flags);
+    case SCH_WENO7JS: return launch_sweep_t<DIR, SCH_WENO7JS>(L, stage, flags);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// One right-hand-side evaluation at stage `stage`; with rk, also the stage update.
+inline cudaError_t launch_stage(const Launch &L, int stage, bool rk, bool eig) {
+  cudaError_t e;
+  const bool ns = L.P.model == MODEL_NS;
+  if (ns) {
+    const int nt = L.tm_cells.tile_start[L.tm_cells.nblocks];
+    prim_kernel<<<nt, kCellTile, 0, L.stream>>>(L.d_blocks, L.tm_cells, L.P, L.d_state, stage);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    grad_kernel<<<nt, kCellTile, 0, L.stream>>>(L.d_blocks, L.tm_cells, L.P);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  const int nsf = ns ? SW_NS : 0;
+  if ((e = launch_sweep<0>(L, stage, nsf | (eig ? SW_EIG : 0))) != cudaSuccess) return e;
+  if ((e = launch_sweep<1>(L, stage, nsf)) != cudaSuccess) return e;
+  if ((e = launch_sweep<2>(L, stage, nsf | (rk ? SW_RK : 0))) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig) {
+  return launch_stage(L, stage, rk, eig);
+}
+
+template <int DIR, int SCH>
+inline cudaError_t configure_t() {
+  return cudaFuncSetAttribute(sweep_kernel<DIR, SCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sweep_smem_bytes<DIR, SCH>(true));
+}
+
+template <int DIR>
+inline cudaError_t configure_dir() {
+  cudaError_t e;
+  if ((e = configure_t<DIR, SCH_WENO5JS>()) != cudaSuccess) return e;
+  if ((e = configure_t<DIR, SCH_WENO5Z>()) != cudaSuccess) return e;
+  return configure_t<DIR, SCH_WENO7JS>();
+}
+
+cudaError_t configure() {
+  cudaError_t e;
+  if ((e = configure_dir<0>()) != cudaSuccess) return e;
+  if ((e = configure_dir<1>()) != cudaSuccess) return e;
+  return configure_dir<2>();
+}
+
+int tile_count(int dir, const int n[3]) {
+  return dir == 0 ? sweep_tiles<0>(n) : (dir == 1 ? sweep_tiles<1>(n) : sweep_tiles<2>(n));
+}
+
+}  // namespace NUC3D_NS
+}  // namespace nuc3d

@@ -1,0 +1,480 @@
+// nuc3d_abi.cu -- the C ABI (include/nuc3d_gpu.h) over the stage kernels.
+//
+// Owns the per-block device arrays, validates the block topology the way the
+// reference's BC_Topo pairing works (src/boundaryConditions.cpp:25-93,
+// src/MPICommunicator.cpp:27-34), and drives the time loop of block::solve
+// (src/block.cpp:569-594): per step three stages, dt fixed at stage 0 from the
+// global eigenvalue maximum (src/PDEData3d.cpp:152-170), time += dt.  A step is
+// captured once as a CUDA graph and replayed.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "nuc3d_gpu.h"
+
+using namespace nuc3d;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                     \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return fail(NUC3D_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+struct HostBlock {
+  int n[3];
+  long long N;
+  int bc_type[6], bc_id[6];
+  double bcv[6][5];
+  double *q[3] = {nullptr, nullptr, nullptr};
+  double *rhs = nullptr, *jac = nullptr, *met = nullptr, *dxyz = nullptr;
+  double *prim = nullptr, *vis = nullptr, *dvis = nullptr;
+  bool metrics = false;
+};
+
+int parse_scheme(const char *s, int *out) {
+  if (!s) return fail(NUC3D_EINVAL, "null scheme name");
+  if (!std::strcmp(s, "weno5js")) *out = SCH_WENO5JS;
+  else if (!std::strcmp(s, "weno5z")) *out = SCH_WENO5Z;
+  else if (!std::strcmp(s, "weno7js")) *out = SCH_WENO7JS;
+  else if (!std::strcmp(s, "crweno5") || !std::strcmp(s, "hccs"))
+    return fail(NUC3D_ENOTSUP, "scheme '%s' is not implemented by this library", s);
+  else return fail(NUC3D_EINVAL, "unknown reconstruction scheme '%s'", s);
+  return NUC3D_OK;
+}
+
+}  // namespace
+
+struct nuc3d_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool exact = true;
+  SolverParams P{};
+  std::vector<HostBlock> blocks;
+  BlockDev *d_blocks = nullptr;
+  StepState *d_state = nullptr;
+  Launch L{};
+  bool finalized = false;
+  bool use_graph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+
+  cudaError_t stage(int s, bool rk, bool eig) {
+    return exact ? nuc3d::exact::run_stage(L, s, rk, eig) : nuc3d::fast::run_stage(L, s, rk, eig);
+  }
+  cudaError_t one_step() {
+    cudaError_t e = cudaMemsetAsync(&d_state->max_eig_bits, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    for (int s = 0; s < 3; ++s)
+      if ((e = stage(s, true, s == 0)) != cudaSuccess) return e;
+    return cudaSuccess;
+  }
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    gexec = nullptr;
+    graph = nullptr;
+  }
+};
+
+extern "C" {
+
+const char *nuc3d_last_error(void) { return g_err.c_str(); }
+
+int nuc3d_create(const nuc3d_config *cfg, int device, nuc3d_ctx **out) {
+  if (!cfg || !out) return fail(NUC3D_EINVAL, "null argument");
+  *out = nullptr;
+  SolverParams P{};
+  for (int d = 0; d < 3; ++d) {
+    int r = parse_scheme(cfg->scheme_ivs[d], &P.scheme[d]);
+    if (r) return r;
+    const char *v = cfg->scheme_vis[d];
+    if (v && std::strcmp(v, "cd6"))
+      return fail(NUC3D_ENOTSUP, "viscous scheme '%s' is not implemented (cd6 only)", v);
+    P.ts[d] = scheme_tilesize(P.scheme[d]);
+  }
+  // block::initialData: bfsize = max of the three bufferSizes (src/block.cpp:506-507)
+  P.bfs = P.ts[0] > P.ts[1] ? P.ts[0] : P.ts[1];
+  P.bfs = P.bfs > P.ts[2] ? P.bfs : P.ts[2];
+  if (!cfg->riemann) return fail(NUC3D_EINVAL, "null riemann name");
+  if (!std::strcmp(cfg->riemann, "LF")) P.riemann = RIE_LF;
+  else if (!std::strcmp(cfg->riemann, "AUSM")) P.riemann = RIE_AUSM;
+  else if (!std::strcmp(cfg->riemann, "AUSMp")) P.riemann = RIE_AUSMP;
+  else return fail(NUC3D_EINVAL, "unknown Riemann solver '%s'", cfg->riemann);
+  if (!cfg->model) return fail(NUC3D_EINVAL, "null model name");
+  if (!std::strcmp(cfg->model, "Euler3d")) P.model = MODEL_EULER;
+  else if (!std::strcmp(cfg->model, "NavierStokes3d")) P.model = MODEL_NS;
+  else return fail(NUC3D_EINVAL, "unknown model '%s' (Euler3d | NavierStokes3d)", cfg->model);
+  P.reynolds = cfg->reynolds;
+  P.mach = cfg->mach;
+  P.prandtl = cfg->prandtl;
+  P.gamma = cfg->gamma;
+  P.t_ref = cfg->t_ref;
+  P.t_inf = cfg->t_inf;
+  P.t_wall = cfg->t_wall;
+  P.cfl = cfg->cfl;
+  P.weno5z_compat = cfg->weno5z_compat ? 1 : 0;
+  if (!(P.gamma > 1.0) || !(P.mach > 0.0) || !(P.cfl > 0.0))
+    return fail(NUC3D_EINVAL, "gamma > 1, mach > 0 and cfl > 0 are required");
+
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(NUC3D_EINVAL, "device %d not present", device);
+  CUDA_TRY(cudaSetDevice(device));
+  nuc3d_ctx *c = new nuc3d_ctx();
+  c->device = device;
+  c->P = P;
+  c->exact = cfg->exact != 0;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_state, sizeof(StepState));
+  if (e == cudaSuccess) e = cudaMemset(c->d_state, 0, sizeof(StepState));
+  if (e == cudaSuccess) e = c->exact ? nuc3d::exact::configure() : nuc3d::fast::configure();
+  if (e != cudaSuccess) {
+    if (c->d_state) cudaFree(c->d_state);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return fail(NUC3D_ECUDA, "context setup: %s", cudaGetErrorString(e));
+  }
+  c->own_stream = true;
+  *out = c;
+  return NUC3D_OK;
+}
+
+int nuc3d_destroy(nuc3d_ctx *c) {
+  if (!c) return NUC3D_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->drop_graph();
+  for (auto &b : c->blocks) {
+    for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.dxyz, b.prim, b.vis, b.dvis})
+      if (p) cudaFree(p);
+  }
+  if (c->d_blocks) cudaFree(c->d_blocks);
+  if (c->d_state) cudaFree(c->d_state);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return NUC3D_OK;
+}
+
+int nuc3d_block_add(nuc3d_ctx *c, int nx, int ny, int nz, const int bc_type[6], const int bc_id[6],
+                    const double *bc_values, int *block_id) {
+  if (!c || !bc_type || !bc_id) return fail(NUC3D_EINVAL, "null argument");
+  if (c->finalized) return fail(NUC3D_ESTATE, "blocks cannot be added after nuc3d_finalize");
+  if ((int)c->blocks.size() >= kMaxBlocks) return fail(NUC3D_EINVAL, "at most %d blocks", kMaxBlocks);
+  const int n[3] = {nx, ny, nz};
+  for (int d = 0; d < 3; ++d)
+    if (n[d] < 2 * c->P.bfs + 2)
+      return fail(NUC3D_EINVAL, "block dimension %d = %d is below 2*bfsize+2 = %d", d, n[d],
+                  2 * c->P.bfs + 2);
+  HostBlock b;
+  for (int d = 0; d < 3; ++d) b.n[d] = n[d];
+  b.N = (long long)nx * ny * nz;
+  for (int f = 0; f < 6; ++f) {
+    b.bc_type[f] = bc_type[f];
+    b.bc_id[f] = bc_id[f];
+    if (bc_type[f] == -1) {
+      if (bc_id[f] < 0 || bc_id[f] > 3)
+        return fail(NUC3D_EINVAL, "face %d: physical BC id %d not in 0..3", f, bc_id[f]);
+    } else if (bc_type[f] < 0) {
+      return fail(NUC3D_EINVAL, "face %d: type %d (use -1 or a block index)", f, bc_type[f]);
+    }
+    for (int v = 0; v < 5; ++v) b.bcv[f][v] = bc_values ? bc_values[f * 5 + v] : 0.0;
+    if (bc_type[f] == -1 && bc_id[f] == BC_INLET && !bc_values)
+      return fail(NUC3D_EINVAL, "face %d is an inlet but no bc_values were given", f);
+  }
+  cudaSetDevice(c->device);
+  const size_t nb = (size_t)b.N * sizeof(double);
+  cudaError_t e = cudaSuccess;
+  for (int s = 0; s < 3 && e == cudaSuccess; ++s) e = cudaMalloc(&b.q[s], 5 * nb);
+  if (e == cudaSuccess) e = cudaMalloc(&b.rhs, 5 * nb);
+  if (e == cudaSuccess) e = cudaMalloc(&b.jac, nb);
+  if (e == cudaSuccess) e = cudaMalloc(&b.met, 9 * nb);
+  if (c->P.model == MODEL_NS) {
+    if (e == cudaSuccess) e = cudaMalloc(&b.prim, 4 * nb);
+    if (e == cudaSuccess) e = cudaMalloc(&b.vis, 12 * nb);
+    if (e == cudaSuccess) e = cudaMalloc(&b.dvis, 8 * nb);
+  }
+  for (int s = 0; s < 3 && e == cudaSuccess; ++s) e = cudaMemset(b.q[s], 0, 5 * nb);
+  if (e == cudaSuccess) e = cudaMemset(b.rhs, 0, 5 * nb);
+  if (e != cudaSuccess) {
+    for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.prim, b.vis, b.dvis})
+      if (p) cudaFree(p);
+    return fail(NUC3D_ECUDA, "block allocation (%lld cells): %s", b.N, cudaGetErrorString(e));
+  }
+  c->blocks.push_back(b);
+  if (block_id) *block_id = (int)c->blocks.size() - 1;
+  return NUC3D_OK;
+}
+
+int nuc3d_block_set_metrics(nuc3d_ctx *c, int bi, const double *jac, const double *xi_xyz,
+                            const double *eta_xyz, const double *zeta_xyz, const double *dxyz) {
+  if (!c || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad block index");
+  if (!jac || !xi_xyz || !eta_xyz || !zeta_xyz) return fail(NUC3D_EINVAL, "null metric array");
+  HostBlock &b = c->blocks[bi];
+  const size_t nb = (size_t)b.N * sizeof(double);
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaMemcpy(b.jac, jac, nb, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(b.met, xi_xyz, 3 * nb, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(b.met + 3 * b.N, eta_xyz, 3 * nb, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(b.met + 6 * b.N, zeta_xyz, 3 * nb, cudaMemcpyHostToDevice));
+  if (dxyz) {
+    if (!b.dxyz) CUDA_TRY(cudaMalloc(&b.dxyz, 9 * nb));
+    CUDA_TRY(cudaMemcpy(b.dxyz, dxyz, 9 * nb, cudaMemcpyHostToDevice));
+  }
+  b.metrics = true;
+  return NUC3D_OK;
+}
+
+int nuc3d_finalize(nuc3d_ctx *c) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (c->finalized) return fail(NUC3D_ESTATE, "already finalized");
+  const int nbk = (int)c->blocks.size();
+  if (nbk == 0) return fail(NUC3D_ESTATE, "no blocks");
+  const int bfs = c->P.bfs;
+  for (int bi = 0; bi < nbk; ++bi) {
+    const HostBlock &b = c->blocks[bi];
+    if (!b.metrics) return fail(NUC3D_ESTATE, "block %d has no metrics", bi);
+    for (int f = 0; f < 6; ++f) {
+      const int d = f >> 1;
+      if (b.bc_type[f] == -1) {
+        if (b.bc_id[f] == BC_SYMM && !b.dxyz)
+          return fail(NUC3D_EINVAL, "block %d face %d is a symmetry face: dxyz metrics required", bi, f);
+        continue;
+      }
+      const int nbi = b.bc_type[f], nf = b.bc_id[f];
+      if (nbi >= nbk) return fail(NUC3D_EINVAL, "block %d face %d: neighbour %d does not exist", bi, f, nbi);
+      if (nf < 0 || nf > 5) return fail(NUC3D_EINVAL, "block %d face %d: neighbour face %d", bi, f, nf);
+      // The reference exchanges one direction at a time (src/euler3d.cpp:318-330), so a
+      // face can only pair with a face of the same direction.
+      if ((nf >> 1) != d)
+        return fail(NUC3D_EINVAL, "block %d face %d pairs with face %d of another direction", bi, f, nf);
+      const HostBlock &o = c->blocks[nbi];
+      auto area = [](const HostBlock &h, int dd) {
+        return dd == 0 ? (long long)h.n[1] * h.n[2]
+                       : (dd == 1 ? (long long)h.n[2] * h.n[0] : (long long)h.n[0] * h.n[1]);
+      };
+      if (area(b, d) != area(o, d))
+        return fail(NUC3D_EINVAL, "block %d face %d and block %d face %d have different sizes", bi, f,
+                    nbi, nf);
+      if (o.n[d] < bfs) return fail(NUC3D_EINVAL, "block %d is thinner than the ghost width", nbi);
+    }
+  }
+  // device descriptors
+  std::vector<BlockDev> hb(nbk);
+  for (int bi = 0; bi < nbk; ++bi) {
+    const HostBlock &b = c->blocks[bi];
+    BlockDev &d = hb[bi];
+    std::memset(&d, 0, sizeof(d));
+    for (int k = 0; k < 3; ++k) d.n[k] = b.n[k];
+    d.N = b.N;
+    for (int s = 0; s < 3; ++s) d.q[s] = b.q[s];
+    d.rhs = b.rhs;
+    d.jac = b.jac;
+    for (int k = 0; k < 3; ++k) d.met[k] = b.met + 3 * k * b.N;
+    d.dxyz = b.dxyz;
+    d.prim = b.prim;
+    d.vis = b.vis;
+    d.dvis = b.dvis;
+    for (int f = 0; f < 6; ++f) {
+      d.face[f].type = b.bc_type[f];
+      d.face[f].id = b.bc_id[f];
+      for (int v = 0; v < 5; ++v) d.face[f].bcv[v] = b.bcv[f][v];
+    }
+  }
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaMalloc(&c->d_blocks, nbk * sizeof(BlockDev)));
+  CUDA_TRY(cudaMemcpy(c->d_blocks, hb.data(), nbk * sizeof(BlockDev), cudaMemcpyHostToDevice));
+  Launch &L = c->L;
+  L.d_blocks = c->d_blocks;
+  L.d_state = c->d_state;
+  L.P = c->P;
+  L.stream = c->stream;
+  for (int d = 0; d < 3; ++d) {
+    L.tm_dir[d].nblocks = nbk;
+    L.tm_dir[d].tile_start[0] = 0;
+  }
+  L.tm_cells.nblocks = nbk;
+  L.tm_cells.tile_start[0] = 0;
+  for (int bi = 0; bi < nbk; ++bi) {
+    const HostBlock &b = c->blocks[bi];
+    for (int d = 0; d < 3; ++d)
+      L.tm_dir[d].tile_start[bi + 1] = L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, b.n);
+    L.tm_cells.tile_start[bi + 1] = L.tm_cells.tile_start[bi] + (int)((b.N + 255) / 256);
+  }
+  c->finalized = true;
+  return NUC3D_OK;
+}
+
+int nuc3d_block_set_q(nuc3d_ctx *c, int bi, const double *q) {
+  if (!c || !q || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
+  HostBlock &b = c->blocks[bi];
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaMemcpyAsync(b.q[0], q, 5 * (size_t)b.N * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
+  return NUC3D_OK;
+}
+
+int nuc3d_block_get_q(nuc3d_ctx *c, int bi, double *q) {
+  if (!c || !q || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
+  HostBlock &b = c->blocks[bi];
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaMemcpyAsync(q, b.q[0], 5 * (size_t)b.N * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return NUC3D_OK;
+}
+
+int nuc3d_block_q_device(nuc3d_ctx *c, int bi, double **dev_q) {
+  if (!c || !dev_q || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
+  *dev_q = c->blocks[bi].q[0];
+  return NUC3D_OK;
+}
+
+static int copy_out(nuc3d_ctx *c, int bi, double *dst, const double *src, int ncomp) {
+  if (!c || !dst || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
+  if (!src) return fail(NUC3D_ESTATE, "this field is not allocated for the configured model");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(dst, src, (size_t)ncomp * c->blocks[bi].N * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+  return NUC3D_OK;
+}
+
+int nuc3d_block_get_rhs(nuc3d_ctx *c, int bi, double *rhs) {
+  if (!c || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
+  return copy_out(c, bi, rhs, c->blocks[bi].rhs, 5);
+}
+int nuc3d_block_get_prim(nuc3d_ctx *c, int bi, double *prim) {
+  if (!c || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
+  return copy_out(c, bi, prim, c->blocks[bi].prim, 4);
+}
+int nuc3d_block_get_vis(nuc3d_ctx *c, int bi, double *vis) {
+  if (!c || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
+  return copy_out(c, bi, vis, c->blocks[bi].vis, 12);
+}
+
+static int check_status(nuc3d_ctx *c) {
+  StepState s;
+  CUDA_TRY(cudaMemcpy(&s, c->d_state, sizeof(s), cudaMemcpyDeviceToHost));
+  if (s.status & (ST_NEG_PRESSURE | ST_NONFINITE | ST_BAD_LAUNCH))
+    return fail(NUC3D_ENUMERIC, "kernel status 0x%x (negative pressure / non-finite state)", s.status);
+  return NUC3D_OK;
+}
+
+int nuc3d_rhs(nuc3d_ctx *c, double *dt_local) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaMemsetAsync(&c->d_state->max_eig_bits, 0, sizeof(unsigned long long), c->stream));
+  CUDA_TRY(c->stage(0, false, true));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  StepState s;
+  CUDA_TRY(cudaMemcpy(&s, c->d_state, sizeof(s), cudaMemcpyDeviceToHost));
+  if (dt_local) {
+    double me;
+    std::memcpy(&me, &s.max_eig_bits, sizeof(me));
+    *dt_local = 1.0 / me;
+  }
+  return check_status(c);
+}
+
+int nuc3d_step(nuc3d_ctx *c, int nsteps) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  if (nsteps < 0) return fail(NUC3D_EINVAL, "nsteps < 0");
+  cudaSetDevice(c->device);
+  if (c->use_graph && !c->gexec) {
+    CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = c->one_step();
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(NUC3D_ECUDA, "graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    c->graph = g;
+    CUDA_TRY(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    if (c->use_graph) CUDA_TRY(cudaGraphLaunch(c->gexec, c->stream));
+    else CUDA_TRY(c->one_step());
+  }
+  return NUC3D_OK;
+}
+
+int nuc3d_sync(nuc3d_ctx *c) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+int nuc3d_get_time(nuc3d_ctx *c, double *time, double *dt) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  StepState s;
+  CUDA_TRY(cudaMemcpy(&s, c->d_state, sizeof(s), cudaMemcpyDeviceToHost));
+  if (time) *time = s.time;
+  if (dt) *dt = s.dt;
+  return NUC3D_OK;
+}
+
+int nuc3d_set_time(nuc3d_ctx *c, double time) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(&c->d_state->time, &time, sizeof(double), cudaMemcpyHostToDevice));
+  return NUC3D_OK;
+}
+
+int nuc3d_get_status(nuc3d_ctx *c, unsigned *status) {
+  if (!c || !status) return fail(NUC3D_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(status, &c->d_state->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return NUC3D_OK;
+}
+
+int nuc3d_set_stream(nuc3d_ctx *c, void *stream) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->drop_graph();
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+  } else {
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+  }
+  c->L.stream = c->stream;
+  return NUC3D_OK;
+}
+
+int nuc3d_use_graph(nuc3d_ctx *c, int on) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  c->use_graph = on != 0;
+  if (!c->use_graph) c->drop_graph();
+  return NUC3D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,206 @@
+// physics.cuh -- ideal-gas EoS, conservative->primitive, flux splitting, BC point fluxes.
+//
+// Every expression keeps the reference's operand order and grouping, so that the
+// build compiled without FMA contraction (kernels_exact.cu) returns the same bits
+// as the reference compiled for x86-64 SSE2.  Citations are to juncas/NUC3d src/.
+#pragma once
+#include "common.h"
+
+namespace nuc3d {
+namespace NUC3D_NS {
+
+__device__ __forceinline__ double sq(double x) { return x * x; }
+
+// pow(x, 1.5), correctly rounded in all but astronomically rare cases:
+// s = sqrt(x); the FMA residual r = x - s*s is exact; sqrt(x) ~= s + r/(2s);
+// x*s is split exactly (TwoProduct with FMA) and the small terms are added last.
+// The oracle evaluates Sutherland's pow(T, 1.5) (src/physicsModel.cpp:226) with
+// the same sequence of IEEE operations (oracle/pow_cr.c).
+__device__ __forceinline__ double pow15(double x) {
+  if (!(x > 1.0e-300 && x < 1.0e300)) return pow(x, 1.5);
+  double s = sqrt(x);
+  double r = fma(-s, s, x);
+  double e = r / (2.0 * s);
+  double hi = x * s;
+  double lo = fma(x, s, -hi);
+  double t = x * e;
+  return hi + (lo + t);
+}
+
+struct CellPrim {
+  double rho, u, v, w, E, p, alpha;
+  double q4;  // energy component of Q actually used (after the reset of :324-332)
+};
+
+// physicsModel::con2prim (src/physicsModel.cpp:307-356) with EoSIdealGasFWD (:981-1054).
+__device__ __forceinline__ void con2prim(const double q[5], double jac, double gamma, double mach,
+                                         CellPrim &s, unsigned &st) {
+  double rho = q[0] * jac;
+  double u = q[1] / rho * jac;
+  double v = q[2] / rho * jac;
+  double w = q[3] / rho * jac;
+  double E = q[4] * jac;
+  double e0 = E - 0.5 * rho * (u * u + v * v + w * w);
+  s.q4 = q[4];
+  if (e0 < 0.0) {
+    E = (pow(rho, gamma) / ((gamma * mach * mach) * (gamma - 1.0)) + 0.5 * rho * (u * u + v * v + w * w));
+    s.q4 = E / jac;
+    st |= ST_ENERGY_RESET;
+  }
+  double p = (E - 0.5 * rho * (u * u + v * v + w * w)) * (gamma - 1.0);
+  if (p < 0.0) st |= ST_NEG_PRESSURE;
+  s.rho = rho;
+  s.u = u;
+  s.v = v;
+  s.w = w;
+  s.E = E;
+  s.p = p;
+  s.alpha = sqrt(fabs(gamma * p / rho));
+}
+
+// EoSIdealGasgetTemp (src/physicsModel.cpp:1020-1030)
+__device__ __forceinline__ double temperature(double rho, double p, double gamma, double mach) {
+  return gamma * mach * mach * p / rho;
+}
+
+// getMachL/R (src/physicsModel.cpp:803-828); identical for AUSMp (:891-916)
+__device__ __forceinline__ double mach_l(double m) {
+  return fabs(m) < 1.0 ? 0.25 * sq(m + 1.0) + 0.125 * sq(m * m - 1) : 0.50 * (m + fabs(m));
+}
+__device__ __forceinline__ double mach_r(double m) {
+  return fabs(m) < 1.0 ? -0.25 * sq(m - 1.0) - 0.125 * sq(m * m - 1) : 0.50 * (m - fabs(m));
+}
+// getPressureL/R (:830-850)
+__device__ __forceinline__ double pres_l(double m, double p) {
+  return fabs(m) < 1.0 ? p * (m + 1.0) / 2.0 : 0.50 * p * (m + fabs(m)) / m;
+}
+__device__ __forceinline__ double pres_r(double m, double p) {
+  return fabs(m) < 1.0 ? -p * (m - 1.0) / 2.0 : 0.5 * p * (m - fabs(m)) / m;
+}
+// getPressureLp/Rp (:918-938)
+__device__ __forceinline__ double pres_lp(double m, double p) {
+  return fabs(m) < 1.0 ? p * (0.25 * sq(m + 1.0) * (2.0 - m) + 0.1875 * m * sq(m * m - 1.0))
+                       : 0.50 * p * (m + fabs(m)) / m;
+}
+__device__ __forceinline__ double pres_rp(double m, double p) {
+  return fabs(m) < 1.0 ? p * (0.25 * sq(m - 1.0) * (2.0 + m) - 0.1875 * m * sq(m * m - 1.0))
+                       : 0.5 * p * (m - fabs(m)) / m;
+}
+
+// Cell flux splitting along one computational direction with metric (xx, xy, xz):
+// physicsModel::RiemannSolver's per-cell body (src/physicsModel.cpp:557-597) calling
+// RiemannLF (:940-979), RiemannAUSM (:762-801) or RiemannAUSMp (:852-889).
+// Q holds U/J (energy after the reset); fp/fn are F+/F- of (F/J).
+__device__ __forceinline__ void split_cell(int riemann, const double Q[5], const CellPrim &s,
+                                           double xx, double xy, double xz, double jac,
+                                           double fp[5], double fn[5]) {
+  double theta = sqrt(xx * xx + xy * xy + xz * xz);
+  double U0 = (xx * s.u + xy * s.v + xz * s.w);
+  double a0 = s.alpha * theta;
+  double p = s.p;
+  if (riemann == RIE_LF) {
+    double M = fabs(U0) + a0;
+    double f0 = U0 * Q[0];
+    double f1 = U0 * Q[1] + xx * p / jac;
+    double f2 = U0 * Q[2] + xy * p / jac;
+    double f3 = U0 * Q[3] + xz * p / jac;
+    double f4 = U0 * (Q[4] + p / jac);
+    fp[0] = 0.5 * (f0 + M * Q[0]);
+    fp[1] = 0.5 * (f1 + M * Q[1]);
+    fp[2] = 0.5 * (f2 + M * Q[2]);
+    fp[3] = 0.5 * (f3 + M * Q[3]);
+    fp[4] = 0.5 * (f4 + M * Q[4]);
+    fn[0] = 0.5 * (f0 - M * Q[0]);
+    fn[1] = 0.5 * (f1 - M * Q[1]);
+    fn[2] = 0.5 * (f2 - M * Q[2]);
+    fn[3] = 0.5 * (f3 - M * Q[3]);
+    fn[4] = 0.5 * (f4 - M * Q[4]);
+    return;
+  }
+  double m = U0 / a0;
+  double mp = mach_l(m), mn = mach_r(m);
+  double pp, pn;
+  if (riemann == RIE_AUSM) {
+    pp = pres_l(m, p);
+    pn = pres_r(m, p);
+  } else {
+    pp = pres_lp(m, p);
+    pn = pres_rp(m, p);
+  }
+  fp[0] = mp * a0 * Q[0];
+  fp[1] = mp * a0 * Q[1] + xx * pp / jac;
+  fp[2] = mp * a0 * Q[2] + xy * pp / jac;
+  fp[3] = mp * a0 * Q[3] + xz * pp / jac;
+  fp[4] = mp * a0 * Q[4] + mp * a0 * p / jac;
+  fn[0] = mn * a0 * Q[0];
+  fn[1] = mn * a0 * Q[1] + xx * pn / jac;
+  fn[2] = mn * a0 * Q[2] + xy * pn / jac;
+  fn[3] = mn * a0 * Q[3] + xz * pn / jac;
+  fn[4] = mn * a0 * Q[4] + mn * a0 * p / jac;
+}
+
+// |U| + c|grad xi| of one cell along one direction (src/physicsModel.cpp:557-597).
+__device__ __forceinline__ double eigen_cell(const CellPrim &s, double xx, double xy, double xz) {
+  double theta = sqrt(xx * xx + xy * xy + xz * xz);
+  double U0 = (xx * s.u + xy * s.v + xz * s.w);
+  return fabs(U0) + s.alpha * theta;
+}
+
+// physicsModel::solveRiemannPoint{LF,AUSM,AUSMp} (src/physicsModel.cpp:1159-1398):
+// split flux of a primitive state q = (rho,u,v,w,p) at a cell's metric.  side 0
+// returns the left split (fluxl), side 1 the right split (fluxr).
+__device__ __forceinline__ void split_point(int riemann, const double q[5], double jac, double xx,
+                                            double xy, double xz, double gamma, int side,
+                                            double out[5], unsigned &st) {
+  const double rho = q[0], u = q[1], v = q[2], w = q[3], p = q[4];
+  double _rho = rho;
+  double _rhou = rho * u;
+  double _rhov = rho * v;
+  double _rhow = rho * w;
+  double _E = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w);
+  double _p = (_E - 0.5 * rho * (u * u + v * v + w * w)) * (gamma - 1.0);
+  if (_p < 0.0) st |= ST_NEG_PRESSURE;
+  double _alpha = sqrt(fabs(gamma * _p / rho));
+  double theta = sqrt(xx * xx + xy * xy + xz * xz);
+  double alpha = _alpha * theta;
+  double U0 = (xx * u + xy * v + xz * w);
+  double mach = U0 / alpha;
+  if (riemann == RIE_LF) {
+    double M = fabs(U0) + alpha;
+    double f0 = U0 * _rho / jac;
+    double f1 = U0 * _rhou / jac + xx * p / jac;
+    double f2 = U0 * _rhov / jac + xy * p / jac;
+    double f3 = U0 * _rhow / jac + xz * p / jac;
+    double f4 = U0 * (_E / jac + p / jac);
+    if (side == 0) {
+      out[0] = 0.5 * (f0 + M * _rho / jac);
+      out[1] = 0.5 * (f1 + M * _rhou / jac);
+      out[2] = 0.5 * (f2 + M * _rhov / jac);
+      out[3] = 0.5 * (f3 + M * _rhow / jac);
+      out[4] = 0.5 * (f4 + M * _E / jac);
+    } else {
+      out[0] = 0.5 * (f0 - M * _rho / jac);
+      out[1] = 0.5 * (f1 - M * _rhou / jac);
+      out[2] = 0.5 * (f2 - M * _rhov / jac);
+      out[3] = 0.5 * (f3 - M * _rhow / jac);
+      out[4] = 0.5 * (f4 - M * _E / jac);
+    }
+    return;
+  }
+  double mm, pm;
+  if (side == 0) {
+    mm = mach_l(mach);
+    pm = riemann == RIE_AUSM ? pres_l(mach, p) : pres_lp(mach, p);
+  } else {
+    mm = mach_r(mach);
+    pm = riemann == RIE_AUSM ? pres_r(mach, p) : pres_rp(mach, p);
+  }
+  out[0] = mm * alpha * _rho / jac;
+  out[1] = mm * alpha * _rhou / jac + xx * pm / jac;
+  out[2] = mm * alpha * _rhov / jac + xy * pm / jac;
+  out[3] = mm * alpha * _rhow / jac + xz * pm / jac;
+  out[4] = mm * alpha * _E / jac + mm * alpha * p / jac;
+}
+
+}  // namespace NUC3D_NS
+}  // namespace nuc3d

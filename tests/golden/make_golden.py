@@ -1,0 +1,158 @@
+"""Generate the golden fixtures in tests/golden/ by running the NUC3d reference.
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Needs the reference binaries built under oracle/_ref (from the reference sources);
+the fixtures it writes are committed so the tests never need the sources.
+Each fixture <name>.npz holds one case:
+  config (json)   scheme/model/physics/BC description, mesh recipe
+  q0              Q = U/J at t = 0 (5, nz, ny, nx)
+  rhs, dt_local   one right-hand side at q0 (EulerData3D::solve / its NS override)
+  q1, qn          Q after 1 and after `nsteps` TVD-RK3 steps (block::solve)
+  dt, time        per-step dt and accumulated time of those nsteps
+  metrics_*       (only in the first fixture) the reference's metrics, to pin the
+                  host metric computation
+Node coordinates use only + - * / (oracle.refrun.box_nodes), so tests rebuild the
+mesh bit for bit instead of storing it.
+"""
+from __future__ import annotations
+
+import json
+import math
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from oracle import refrun as R  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+TWO_PI = 2.0 * math.pi
+
+
+def case_defs():
+    """Small non-cubic cases covering every scheme, splitting and BC of the hot path."""
+    return [
+        dict(name="tgv_ns_weno5js_lf", model="NavierStokes3d", riemann="LF",
+             schemes=("weno5js",) * 3, shape=(16, 12, 8), lo=(0, 0, 0), hi=(TWO_PI,) * 3,
+             wavy=0.0, faces=["periodic"] * 6, init="tgv",
+             params=dict(Reynolds=1600.0, Mach=0.1, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=5, metrics=True),
+        dict(name="sphere_euler_weno5z_ausm_outlet", model="Euler3d", riemann="AUSM",
+             schemes=("weno5z",) * 3, shape=(12, 12, 12), lo=(0, 0, 0), hi=(1, 1, 1),
+             wavy=0.0, faces=["outlet"] * 6, init="sphere",
+             params=dict(Reynolds=1000.0, Mach=1.0, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=5),
+        dict(name="wavy_euler_weno5js_lf", model="Euler3d", riemann="LF",
+             schemes=("weno5js",) * 3, shape=(16, 8, 12), lo=(0, 0, 0), hi=(2.0, 1.0, 1.5),
+             wavy=0.3, faces=["periodic"] * 6, init="smooth",
+             params=dict(Reynolds=1000.0, Mach=0.5, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=3),
+        dict(name="bc_ns_weno7js_ausmp", model="NavierStokes3d", riemann="AUSMp",
+             schemes=("weno7js",) * 3, shape=(16, 12, 12), lo=(0, 0, 0), hi=(2.0, 1.0, 1.0),
+             wavy=0.2, faces=["inlet", "outlet", "wall", "symm", "periodic", "periodic"],
+             init="channel",
+             params=dict(Reynolds=200.0, Mach=0.5, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.2), nsteps=3),
+        dict(name="mixed_euler_lf_outlet_symm", model="Euler3d", riemann="LF",
+             schemes=("weno5js", "weno5z", "weno7js"), shape=(12, 12, 12), lo=(0, 0, 0),
+             hi=(1.0, 1.0, 1.0), wavy=0.25,
+             faces=["outlet", "outlet", "periodic", "periodic", "symm", "symm"], init="smooth",
+             params=dict(Reynolds=1000.0, Mach=0.8, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=3),
+        dict(name="ns_ausm_weno5z_wall_inlet", model="NavierStokes3d", riemann="AUSM",
+             schemes=("weno5z",) * 3, shape=(12, 12, 16), lo=(0, 0, 0), hi=(1.0, 1.0, 2.0),
+             wavy=0.0, faces=["periodic", "periodic", "wall", "wall", "inlet", "outlet"],
+             init="channel",
+             params=dict(Reynolds=300.0, Mach=0.6, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.1), nsteps=3),
+    ]
+
+
+def inlet_state(p):
+    g, m = p["Gamma"], p["Mach"]
+    return [1.0, 0.5, 0.0, 0.0, 1.0 / (g * m * m)]
+
+
+def initial_prim(kind, xc, yc, zc, p):
+    g, m = p["Gamma"], p["Mach"]
+    if kind == "sphere":
+        return R.spherical_riemann_prim(xc, yc, zc)
+    if kind == "smooth":
+        rho = 1.0 + 0.2 * np.sin(2.0 * math.pi * xc) * np.cos(math.pi * yc)
+        u = 0.3 + 0.1 * np.cos(math.pi * zc)
+        v = 0.1 * np.sin(math.pi * xc)
+        w = -0.05 * np.cos(2.0 * math.pi * yc)
+        pr = 1.0 / (g * m * m) * (1.0 + 0.1 * np.sin(math.pi * zc))
+        return np.stack([rho, u, v, w, pr])
+    if kind == "channel":
+        rho = 1.0 + 0.05 * np.sin(math.pi * xc) * np.sin(math.pi * yc)
+        u = 0.5 * (1.0 + 0.1 * np.cos(math.pi * zc))
+        v = 0.02 * np.sin(2.0 * math.pi * xc)
+        w = 0.01 * np.cos(math.pi * yc)
+        pr = 1.0 / (g * m * m) * (1.0 + 0.02 * np.cos(math.pi * xc))
+        return np.stack([rho, u, v, w, pr])
+    raise ValueError(kind)
+
+
+def build_case(cd):
+    nx, ny, nz = cd["shape"]
+    x, y, z = R.box_nodes(nx, ny, nz, lo=cd["lo"], hi=cd["hi"], wavy=cd["wavy"])
+    inlet = inlet_state(cd["params"])
+    values = [inlet if f == "inlet" else None for f in cd["faces"]]
+    bc = R.bc_lines(cd["faces"], values)
+    case = R.Case(model=cd["model"], riemann=cd["riemann"], schemes=cd["schemes"],
+                  params=cd["params"], nodes=[(x, y, z)], bc_topo=[bc],
+                  benchmark=2 if cd["init"] == "tgv" else 0)
+    return case
+
+
+def generate(cd):
+    case = build_case(cd)
+    init = R.run(case, "init")[0]
+    if cd["init"] != "tgv":
+        xc, yc, zc = (init[f"xyz_center.{i}"] for i in range(3))
+        prim = initial_prim(cd["init"], xc, yc, zc, cd["params"])
+        q0 = R.prim_to_q(prim, init["jac"], cd["params"]["Gamma"])
+        case.start_step = 1
+        case.q0 = [q0]
+    else:
+        q0 = R.stack(init, "Q", 5)
+    rhs = R.run(case, "rhs")[0]
+    s1 = R.run(case, "steps", 1)[0]
+    sn = R.run(case, "steps", cd["nsteps"])[0]
+    out = dict(
+        config=json.dumps({k: v for k, v in cd.items()}),
+        q0=q0, rhs=R.stack(rhs, "RHS", 5), dt_local=rhs["dt_local"],
+        q1=R.stack(s1, "Q", 5), qn=R.stack(sn, "Q", 5), dt=sn["dt"], time=sn["time"],
+    )
+    if cd.get("metrics"):
+        out["metrics_jac"] = init["jac"]
+        for nm in ("xi_xyz", "eta_xyz", "zeta_xyz"):
+            out[f"metrics_{nm}"] = R.stack(init, nm, 3)
+        out["metrics_dxyz"] = np.stack([init[f"{a}.{i}"] for a in ("dx", "dy", "dz")
+                                        for i in range(3)])
+    # stock glibc pow versus the correctly rounded pow of the oracle build
+    libm = R.run(case, "steps", cd["nsteps"], binary="nuc3d_ref_libm_taps")[0] \
+        if (R.REF_BIN_DIR / "nuc3d_ref_libm_taps").exists() else None
+    if libm is not None:
+        qa, qb = R.stack(libm, "Q", 5), out["qn"]
+        out["libm_max_rel_diff"] = np.array([np.max(np.abs(qa - qb)) / np.max(np.abs(qb))])
+    np.savez_compressed(OUT / f"{cd['name']}.npz", **out)
+    return out
+
+
+def main(names=None):
+    for cd in case_defs():
+        if names and cd["name"] not in names:
+            continue
+        o = generate(cd)
+        extra = f" libm_rel_diff={o['libm_max_rel_diff'][0]:.3g}" if "libm_max_rel_diff" in o else ""
+        print(f"{cd['name']}: dt_local={o['dt_local'][0]:.6g} dt={o['dt']}{extra}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

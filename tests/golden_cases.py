@@ -1,0 +1,82 @@
+"""Load the committed golden fixtures and set up the GPU solver for them."""
+from __future__ import annotations
+
+import json
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from oracle import refrun as R
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+FACE_IDS = {"inlet": 0, "outlet": 1, "wall": 2, "symm": 3}
+PERIODIC_NEIGHBOUR_FACE = [1, 0, 3, 2, 5, 4]
+
+
+@dataclass
+class Golden:
+    name: str
+    cfg: dict
+    data: dict
+
+    def __getattr__(self, k):
+        try:
+            return self.data[k]
+        except KeyError as e:
+            raise AttributeError(k) from e
+
+
+def names():
+    return sorted(p.stem for p in GOLDEN.glob("*.npz"))
+
+
+def load(name: str) -> Golden:
+    z = np.load(GOLDEN / f"{name}.npz")
+    data = {k: z[k] for k in z.files}
+    cfg = json.loads(str(data.pop("config")))
+    return Golden(name, cfg, data)
+
+
+def nodes(g: Golden):
+    nx, ny, nz = g.cfg["shape"]
+    return R.box_nodes(nx, ny, nz, lo=g.cfg["lo"], hi=g.cfg["hi"], wavy=g.cfg["wavy"])
+
+
+def inlet_state(p):
+    return [1.0, 0.5, 0.0, 0.0, 1.0 / (p["Gamma"] * p["Mach"] * p["Mach"])]
+
+
+def bc_arrays(g: Golden, self_index: int = 0):
+    types, ids, vals = [], [], np.zeros((6, 5))
+    for f, k in enumerate(g.cfg["faces"]):
+        if k == "periodic":
+            types.append(self_index)
+            ids.append(PERIODIC_NEIGHBOUR_FACE[f])
+        else:
+            types.append(-1)
+            ids.append(FACE_IDS[k])
+            if k == "inlet":
+                vals[f] = inlet_state(g.cfg["params"])
+    return types, ids, vals
+
+
+def nuc3d_config(g: Golden, exact: bool = True):
+    import nuc3d_b200 as nb
+    p = g.cfg["params"]
+    return nb.Config(scheme_ivs=tuple(g.cfg["schemes"]), riemann=g.cfg["riemann"],
+                     model=g.cfg["model"], reynolds=p["Reynolds"], mach=p["Mach"],
+                     prandtl=p["Pt"], gamma=p["Gamma"], t_ref=p["T_ref"], t_inf=p["T_inf"],
+                     t_wall=p["T_wall"], cfl=0.5, exact=exact, weno5z_compat=True)
+
+
+def solver(g: Golden, exact: bool = True):
+    import nuc3d_b200 as nb
+    s = nb.Solver(nuc3d_config(g, exact))
+    nx, ny, nz = g.cfg["shape"]
+    t, i, v = bc_arrays(g)
+    b = s.add_block(nx, ny, nz, t, i, v)
+    s.set_mesh(b, *nodes(g))
+    s.finalize()
+    s.set_q(b, g.q0)
+    return s
