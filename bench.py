@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Throughput of NUC3d's per-block RHS + TVD-RK3 update on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one per GPU): the shock-dominated FP64 Euler case -- a 256^3 block on
+[0,1]^3 with extrapolation (outlet) faces, spherical discontinuity rho,p = 1,10
+inside r < 0.2 and 0.125,0.1 outside, WENO5-Z + AUSM splitting, TVD-RK3 at CFL
+0.5.  The reference has no characteristic projection; splitting is component-wise
+as in src/euler3d.cpp:318-330.  A step = one TVD-RK3 step (3 stages) of the block.
+
+Metric: Mcell-RK3-steps/s = cells x steps / device seconds, summed over GPUs
+(weak scaling: every GPU advances its own block; no data-path collective).
+The timed state (5 x 256^3 doubles = 671 MB per buffer, 4 GB per block) is far
+larger than the 126 MB L2.
+
+--impl reference times the reference's own CPU code (oracle/_ref/nuc3d_ref_taps,
+built from the reference sources) on this machine's host cores, one MPI rank per
+core through the project's shared-memory MPI shim, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SHAPE = (256, 256, 256)
+WORKLOAD = ("spherical Riemann 256^3, FP64 Euler, WENO5-Z (reference :80 stencil), AUSM, "
+            "outlet faces, TVD-RK3 CFL 0.5")
+
+# Algorithmic FP64 operations per cell, counted from the reference's expressions
+# (add/sub/mul/div/sqrt = 1, abs = 0, pow(x,2) = 1).  Derivation in DESIGN.md.
+FLOPS = {
+    "con2prim": 46,        # src/physicsModel.cpp:315-353, :1000-1054
+    "AUSM": 82,            # src/physicsModel.cpp:557-597 + RiemannAUSM :762-850, per direction
+    "LF": 60,              # RiemannLF :940-979, per direction
+    "AUSMp": 94,           # RiemannAUSMp :852-938, per direction
+    "weno5js": 67,         # per face, variable and split: src/weno5js.cpp:75-108
+    "weno5z": 74,          # src/weno5z.cpp:74-109
+    "weno7js": 146,        # src/weno7js.cpp:84-136
+    "combine": 1,          # per face and variable: src/euler3d.cpp:45-49
+    "difference": 1,       # per cell and variable: src/euler3d.cpp:163-169
+    "rhs_add": 1,          # per cell and variable: src/euler3d.cpp:405,419
+    "rk": 14.0 / 3.0,      # per cell and variable, mean of stages 4,5,5: src/TVD-RK3.cpp:57-136
+}
+# HBM bytes a sweep cannot avoid per cell: Q (40) + jac (8) + its direction's metric (24),
+# plus RHS write (xi), RHS read+write (eta), RHS read + Q_n read (stages 1,2) + Q write (zeta).
+SWEEP_BYTES = {0: 72 + 40, 1: 72 + 80, 2: 72 + 40 + 40 * 2.0 / 3.0 + 40}
+
+
+def sweep_flops_per_cell(d: int, scheme: str = "weno5z", riemann: str = "AUSM") -> float:
+    f = FLOPS[riemann] + 10 * FLOPS[scheme] + 5 * FLOPS["combine"] + 5 * FLOPS["difference"]
+    if d == 0:
+        f += FLOPS["con2prim"]
+    else:
+        f += 5 * FLOPS["rhs_add"]
+    if d == 2:
+        f += 5 * FLOPS["rk"]
+    return f
+
+
+# ---------------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.p = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        if self.p is None or self.out is None:
+            return None
+        self.out.flush()
+        rows = [r.split(",") for r in Path(self.out.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "power_w_max": max(pw) if pw else None, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------------
+# the reference on the host cores
+# ---------------------------------------------------------------------------------
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def decompose(shape, nranks):
+    """Split shape into nranks = 2^k blocks by halving the largest extent."""
+    parts = [1, 1, 1]
+    n = nranks
+    while n > 1:
+        ext = [shape[d] // parts[d] for d in range(3)]
+        d = int(np.argmax(ext))
+        if ext[d] % 2 or (ext[d] // 2) % 4 or ext[d] // 2 < 12:
+            break
+        parts[d] *= 2
+        n //= 2
+    return parts
+
+
+def reference_case(shape, nranks):
+    """A refrun.Case of the workload split over nranks blocks (outlet outer faces)."""
+    from oracle import refrun as R
+    from nuc3d_b200 import cases as C
+    parts = decompose(shape, nranks)
+    nr = parts[0] * parts[1] * parts[2]
+    bs = [shape[d] // parts[d] for d in range(3)]
+    xs = [np.arange(shape[d] + 1, dtype=np.float64) / shape[d] for d in range(3)]
+    rank_of = lambda a, b, c: a + parts[0] * (b + parts[1] * c)  # noqa: E731
+    nodes, topo, q0 = [], [], []
+    for c in range(parts[2]):
+        for b in range(parts[1]):
+            for a in range(parts[0]):
+                lo = [a * bs[0], b * bs[1], c * bs[2]]
+                sl = [slice(lo[d], lo[d] + bs[d] + 1) for d in range(3)]
+                Z, Y, X = np.meshgrid(xs[2][sl[2]], xs[1][sl[1]], xs[0][sl[0]], indexing="ij")
+                nodes.append((X, Y, Z))
+                pos = [a, b, c]
+                lines = []
+                for f in range(6):
+                    d, side = f // 2, f % 2
+                    p2 = list(pos)
+                    p2[d] += 1 if side else -1
+                    if 0 <= p2[d] < parts[d]:
+                        lines.append(f"{rank_of(*p2)} {f ^ 1}")
+                    else:
+                        lines.append("-1 1")
+                topo.append(lines)
+                h = [1.0 / shape[d] for d in range(3)]
+                xc = [(lo[d] + np.arange(bs[d]) + 0.5) * h[d] for d in range(3)]
+                Zc, Yc, Xc = np.meshgrid(xc[2], xc[1], xc[0], indexing="ij")
+                prim = R.spherical_riemann_prim(Xc, Yc, Zc)
+                jac = np.full(Xc.shape, 1.0 / (h[0] * h[1] * h[2]))
+                q0.append(C.prim_to_q(prim, jac, 1.4))
+    case = R.Case(model="Euler3d", riemann="AUSM", schemes=("weno5z",) * 3,
+                  params={"Reynolds": 1000.0, "Mach": 1.0, "Pt": 0.72, "Gamma": 1.4,
+                          "T_ref": 110.4, "T_inf": 288.0, "T_wall": 1.0},
+                  nodes=nodes, bc_topo=topo, q0=q0, start_step=1)
+    return case, nr
+
+
+def run_reference(shape, steps, warmup, timeout=1800):
+    """Reference block::solve time on the host cores: (Mcell-steps/s, cores, sample)."""
+    from oracle import refrun as R
+    cores = host_cores()
+    nranks = 1
+    while nranks * 2 <= min(cores, 256):
+        nranks *= 2
+    case, nr = reference_case(shape, nranks)
+    out = R.run(case, "time", steps, warmup, timeout=timeout)[0]
+    rec = json.loads(out.strip().splitlines()[-1])
+    cells = shape[0] * shape[1] * shape[2]
+    value = cells * steps / rec["solve_seconds"] / 1e6
+    sample = (f"{steps} timed + {warmup} warm-up TVD-RK3 steps of the {shape[0]}x{shape[1]}x"
+              f"{shape[2]} workload split into {nr} blocks, one reference rank (process) per core; "
+              f"time = sum over steps of max over ranks of block::solve wall time")
+    return value, nr, sample, rec["solve_seconds"]
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    shape = SHAPE
+    cells = shape[0] * shape[1] * shape[2]
+    # bound the run: ~0.15 Mcell-steps/s per core for this scheme on one core
+    est = cells / (0.15e6 * max(1, min(host_cores(), 256))) * (args.steps + args.warmup)
+    if est > 300.0:
+        shape = (128, 128, 128)
+        cells = shape[0] ** 3
+    value, nr, sample, secs = run_reference(shape, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": "Mcell-RK3-steps/s", "value": value,
+        "unit": "Mcell-RK3-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": cells, "parallelism": f"{nr} MPI ranks on CPU"},
+        "cpu_baseline": {"value": value, "unit": "Mcell-RK3-steps/s", "cores": nr,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "Mcell-RK3-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------
+def ours(args):
+    import torch
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    cfg = nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="Euler3d", mach=1.0,
+                    gamma=1.4, cfl=0.5, exact=args.exact, weno5z_compat=True)
+    q0, m = C.spherical_riemann(SHAPE)
+    cells = int(np.prod(SHAPE))
+    s = nb.Solver(cfg, device=local)
+    b = s.add_block(*SHAPE, *C.outlet_faces())
+    s.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
+    s.finalize()
+    stream = torch.cuda.Stream(device=dev)
+    s.set_stream(stream.cuda_stream)
+    s.set_q(b, q0)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        s.sync()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timing ----
+    s.step(args.warmup)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            s.step(args.steps, sync=False)
+            ev1.record(stream)
+        ev1.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    s.sync()
+    status = s.status()
+    value = world * cells * args.steps / (ms * 1e-3) / 1e6
+
+    # ---- end to end through the public API with pinned host buffers ----
+    host_in = torch.empty(5 * cells, dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty(5 * cells, dtype=torch.float64, pin_memory=True)
+    host_in.numpy()[:] = s.get_q(b).reshape(-1)
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(2):  # warm-up of the copy path
+        s.set_q_ptr(b, host_in.data_ptr())
+        s.step(1, sync=False)
+        s.get_q_ptr(b, host_out.data_ptr())
+    barrier()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for _ in range(e2e_steps):
+        s.set_q_ptr(b, host_in.data_ptr())
+        s.step(1, sync=False)
+        s.get_q_ptr(b, host_out.data_ptr())
+    ev3.record(stream)
+    ev3.synchronize()
+    e2e_ms = max_over_ranks(ev2.elapsed_time(ev3))
+    e2e_value = world * cells * e2e_steps / (e2e_ms * 1e-3) / 1e6
+
+    # ---- roofline of the dominant kernel ----
+    s.set_q(b, q0)
+    per = {d: s.profile_sweep(d, reps=5) for d in range(3)}
+    dom = max(per, key=per.get)
+    flops = sweep_flops_per_cell(dom) * cells
+    achieved = flops / (per[dom] * 1e-3) / 1e12
+    peak = nb.fp64_peak_tflops(local)
+    hbm_achieved = SWEEP_BYTES[dom] * cells / (per[dom] * 1e-3) / 1e9
+    try:
+        hbm_peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]
+        hbm_src = "MEASURED_PEAKS.json"
+    except Exception:
+        hbm_peak, hbm_src = 6650.0, "fallback"
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        s.close()
+        return 0
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            v, nr, sample, _ = run_reference(SHAPE, 1, 1)
+            cpu = {"value": v, "unit": "Mcell-RK3-steps/s", "cores": nr, "kind": "reference",
+                   "sample": sample}
+        except Exception as e:  # the baseline is a report, never a reason to fail the bench
+            cpu = {"value": None, "unit": "Mcell-RK3-steps/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}".splitlines()[0][:200]}
+
+    line = {
+        "metric": "Mcell-RK3-steps/s", "value": value, "unit": "Mcell-RK3-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells_per_gpu": cells,
+                   "arith": "reference-order (no FMA)" if args.exact else "fast (FMA, 1 div/face)",
+                   "l2": "no flush: 3 state buffers of 671 MB + RHS + metrics = 4 GB > 126 MB L2",
+                   "parallelism": f"replicas x{world} (one independent block per GPU)",
+                   "status_bits": status},
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_value, "unit": "Mcell-RK3-steps/s",
+                "h2d_bytes_per_step": 5 * cells * 8, "d2h_bytes_per_step": 5 * cells * 8,
+                "steps": e2e_steps},
+        "gpu_launches": 9 * args.steps,
+        "roofline": {
+            "bound": "fp64", "kernel": f"sweep_kernel<{dom}> ({'xi eta zeta'.split()[dom]})",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "measured live: libnuc3d_probe DFMA microbenchmark",
+            "flops_per_cell": sweep_flops_per_cell(dom), "ms_per_launch": per[dom],
+            "ms_per_launch_all": per,
+            "traffic": None,
+            "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": hbm_achieved / hbm_peak, "peak_source": hbm_src,
+                    "bytes_per_cell": SWEEP_BYTES[dom]},
+        },
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    s.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--exact", action="store_true", help="reference-order arithmetic")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -125,6 +125,11 @@ int nuc3d_set_stream(nuc3d_ctx *ctx, void *stream);
 /* 1: replay the three stages of a step as one CUDA graph (default); 0: launch directly. */
 int nuc3d_use_graph(nuc3d_ctx *ctx, int on);
 
+/* Profiling: launch the dir-sweep kernel (0 xi, 1 eta, 2 zeta; right-hand side
+   only, at the current state) `reps` times back to back on the context's stream and
+   return the mean device time per launch in milliseconds (CUDA events). */
+int nuc3d_profile_sweep(nuc3d_ctx *ctx, int dir, int reps, double *ms_per_launch);
+
 /* Debug taps: NS primitives (u, v, w, T: 4N) and contravariant viscous fluxes
    ([dir][var 1..4]: 12N) of the last evaluation. */
 int nuc3d_block_get_prim(nuc3d_ctx *ctx, int block, double *prim);

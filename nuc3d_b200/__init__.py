@@ -31,8 +31,22 @@ EXPORTED = (
     "nuc3d_block_set_metrics", "nuc3d_finalize", "nuc3d_block_set_q", "nuc3d_block_get_q",
     "nuc3d_block_q_device", "nuc3d_rhs", "nuc3d_block_get_rhs", "nuc3d_step", "nuc3d_sync",
     "nuc3d_get_time", "nuc3d_set_time", "nuc3d_get_status", "nuc3d_set_stream",
-    "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis",
+    "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis", "nuc3d_profile_sweep",
 )
+
+
+def fp64_peak_tflops(device: int = 0, reps: int = 20) -> float:
+    """Measured FP64 FMA throughput of the device (libnuc3d_probe.so microbenchmark)."""
+    p = _LIB_PATH.with_name("libnuc3d_probe.so")
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with `python -m nuc3d_b200.build`")
+    lib = ctypes.CDLL(str(p))
+    lib.nuc3d_probe_fp64_tflops.restype = ctypes.c_double
+    lib.nuc3d_probe_fp64_tflops.argtypes = [ctypes.c_int, ctypes.c_int]
+    v = lib.nuc3d_probe_fp64_tflops(device, reps)
+    if v < 0:
+        raise RuntimeError(f"fp64 probe failed ({v})")
+    return v
 
 
 class Nuc3dError(RuntimeError):
@@ -88,6 +102,7 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_use_graph.argtypes = [P, I]
     lib.nuc3d_block_get_prim.argtypes = [P, I, PD]
     lib.nuc3d_block_get_vis.argtypes = [P, I, PD]
+    lib.nuc3d_profile_sweep.argtypes = [P, I, I, PD]
     for name in EXPORTED:
         if name != "nuc3d_last_error":
             getattr(lib, name).restype = ctypes.c_int
@@ -266,6 +281,12 @@ class Solver:
         s = ctypes.c_uint()
         _check(self.lib.nuc3d_get_status(self._ctx, ctypes.byref(s)))
         return s.value
+
+    def profile_sweep(self, direction: int, reps: int = 10) -> float:
+        """Mean device milliseconds of one launch of the direction sweep kernel."""
+        ms = ctypes.c_double()
+        _check(self.lib.nuc3d_profile_sweep(self._ctx, direction, reps, ctypes.byref(ms)))
+        return ms.value
 
     def use_graph(self, on: bool) -> None:
         _check(self.lib.nuc3d_use_graph(self._ctx, int(bool(on))))

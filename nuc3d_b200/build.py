@@ -19,6 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libnuc3d_b200.so"
+PROBE_LIB = PKG / "libnuc3d_probe.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"),
@@ -73,6 +74,11 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         cmd = [cc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static", "-lrt",
                "-ldl", "-lpthread"]
         subprocess.run(cmd, check=True)
+    probe_src = CSRC / "probe.cu"
+    if force or _stale(PROBE_LIB, [probe_src, Path(__file__)]):
+        subprocess.run([cc, *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+                        str(probe_src), "-o", str(PROBE_LIB), "-lcudart_static", "-lrt", "-ldl",
+                        "-lpthread"], check=True)
     return LIB
 
 

@@ -95,11 +95,13 @@ struct Launch {
 // tile_count(): CTAs of the dir-sweep over one block of n cells.
 namespace exact {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 cudaError_t configure();
 int tile_count(int dir, const int n[3]);
 }
 namespace fast {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 cudaError_t configure();
 int tile_count(int dir, const int n[3]);
 }

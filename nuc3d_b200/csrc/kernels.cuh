@@ -674,6 +674,13 @@ cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig) {
   return launch_stage(L, stage, rk, eig);
 }
 
+cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags) {
+  const int f = flags | (L.P.model == MODEL_NS ? SW_NS : 0);
+  if (dir == 0) return launch_sweep<0>(L, stage, f);
+  if (dir == 1) return launch_sweep<1>(L, stage, f);
+  return launch_sweep<2>(L, stage, f & ~SW_RK);
+}
+
 template <int DIR, int SCH>
 inline cudaError_t configure_t() {
   return cudaFuncSetAttribute(sweep_kernel<DIR, SCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,

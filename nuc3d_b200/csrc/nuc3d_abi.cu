@@ -470,6 +470,29 @@ int nuc3d_set_stream(nuc3d_ctx *c, void *stream) {
   return NUC3D_OK;
 }
 
+int nuc3d_profile_sweep(nuc3d_ctx *c, int dir, int reps, double *ms) {
+  if (!c || !ms || dir < 0 || dir > 2 || reps < 1) return fail(NUC3D_EINVAL, "bad argument");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  cudaSetDevice(c->device);
+  auto sweep = [&]() {
+    return c->exact ? nuc3d::exact::run_sweep(c->L, dir, 0, 0) : nuc3d::fast::run_sweep(c->L, dir, 0, 0);
+  };
+  CUDA_TRY(sweep());  // warm-up
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  CUDA_TRY(cudaEventRecord(e0, c->stream));
+  for (int r = 0; r < reps; ++r) CUDA_TRY(sweep());
+  CUDA_TRY(cudaEventRecord(e1, c->stream));
+  CUDA_TRY(cudaEventSynchronize(e1));
+  float t = 0.0f;
+  CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = (double)t / reps;
+  return check_status(c);
+}
+
 int nuc3d_use_graph(nuc3d_ctx *c, int on) {
   if (!c) return fail(NUC3D_EINVAL, "null context");
   c->use_graph = on != 0;

@@ -1,0 +1,59 @@
+// probe.cu -- FP64 peak of the device, measured with a dependent-FMA microbenchmark.
+//
+// The roofline denominators on this GPU pool cover HBM copy bandwidth and bf16
+// tensor throughput only; the NUC3d path is plain FP64 (no tensor cores), so its
+// compute roof is measured here: every thread runs 8 independent DFMA chains,
+// enough CTAs to fill all SMs several times over, timed with CUDA events.
+// Exported from libnuc3d_probe.so (not part of the solver ABI).
+#include <cuda_runtime.h>
+
+namespace {
+
+constexpr int kChains = 8;
+
+__global__ void __launch_bounds__(256) dfma_loop(double *out, int iters, double b, double c) {
+  double a[kChains];
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) a[k] = threadIdx.x * 1e-3 + k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) a[k] = fma(a[k], b, c);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) s += a[k];
+  if (s == 1234.5678) out[blockIdx.x] = s;  // never true; keeps the chains alive
+}
+
+}  // namespace
+
+extern "C" {
+
+// Returns sustained FP64 TFLOP/s (FMA = 2 flops) over `reps` launches, or a negative
+// CUDA error code.
+double nuc3d_probe_fp64_tflops(int device, int reps) {
+  if (cudaSetDevice(device) != cudaSuccess) return -1.0;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  double *out = nullptr;
+  if (cudaMalloc(&out, 1 << 20) != cudaSuccess) return -2.0;
+  const int blocks = sms * 16, threads = 256, iters = 1 << 14;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  dfma_loop<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);  // warm-up
+  cudaEventRecord(e0);
+  for (int r = 0; r < reps; ++r) dfma_loop<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+  cudaEventRecord(e1);
+  cudaError_t err = cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (err != cudaSuccess) return -3.0;
+  const double flops = 2.0 * kChains * (double)iters * threads * blocks * reps;
+  return flops / (ms * 1e-3) / 1e12;
+}
+
+}  // extern "C"

@@ -99,8 +99,10 @@ def write_case(case: Case, rundir: Path) -> None:
         nz0, ny0, nx0 = x.shape
         with open(rundir / f"mesh/mesh_{r}.x", "w") as f:
             f.write(f"{nx0} {ny0} {nz0}\n")
+        with open(rundir / f"mesh/mesh_{r}.x", "a") as f:
             for a in (x, y, z):
-                f.write("\n".join(repr(float(v)) for v in a.ravel()))
+                # %.17g round-trips every double exactly
+                np.ascontiguousarray(a).ravel().tofile(f, sep="\n", format="%.17g")
                 f.write("\n")
         (rundir / f"bc_topo/BC_Topo_{r}.in").write_text("\n".join(case.bc_topo[r]) + "\n")
         if case.start_step > 0:
