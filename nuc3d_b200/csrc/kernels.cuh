@@ -24,16 +24,20 @@
 namespace nuc3d {
 namespace NUC3D_NS {
 
-constexpr int kThreads = 256;
-
-// Tile of one sweep CTA: TW lines side by side, TL cells along each line.
-// xi lines are contiguous in memory; eta/zeta tiles put TW consecutive i in a row.
-template <int DIR> struct Tile;
-template <> struct Tile<0> { static constexpr int TW = 4, TL = 64; };
-template <> struct Tile<1> { static constexpr int TW = 8, TL = 32; };
-template <> struct Tile<2> { static constexpr int TW = 8, TL = 32; };
+// Tile of one sweep CTA: TW lines side by side, TL cells along each line.  xi lines
+// are contiguous in memory; eta/zeta tiles put TW consecutive i in a row (one 32-byte
+// sector).  kThreads = TW*TL + 32 makes every phase a single round: TW*(TL+2R) <= 288
+// split fluxes, TW*(TL+1) faces, TW*TL cells, so no warp idles at a barrier waiting
+// for a one-lane tail.
+constexpr int kTW = 4, kTL = 64;
+constexpr int kThreads = kTW * kTL + 32;
+template <int DIR> struct Tile { static constexpr int TW = kTW, TL = kTL; };
 
 template <int SCH> struct Halo { static constexpr int R = (SCH == SCH_WENO7JS) ? 4 : 3; };
+
+// Row strides of the shared-memory tiles, padded so that the TW rows of one warp
+// access fall in different bank halves (stride = 8 mod 16 doubles).
+__host__ __device__ constexpr int pad_row(int n) { return ((n + 7) / 16) * 16 + 8; }
 
 struct Geo {
   int L, nW, nO;
@@ -63,9 +67,9 @@ __host__ __device__ inline int sweep_tiles(const int n[3]) {
 template <int DIR, int SCH>
 __host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
   constexpr int R = Halo<SCH>::R, TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
-  size_t n = (size_t)10 * TW * (TL + 2 * R) + (size_t)5 * TW * (TL + 1);
-  if (ns) n += (size_t)4 * TW * (TL + 6);
-  if (DIR == 2) n += (size_t)5 * TW * TL;
+  size_t n = (size_t)10 * TW * pad_row(TL + 2 * R) + (size_t)5 * TW * pad_row(TL + 1);
+  if (ns) n += (size_t)4 * TW * pad_row(TL + 6);
+  if (DIR == 2) n += (size_t)5 * TW * pad_row(TL);
   return n * sizeof(double);
 }
 
@@ -286,14 +290,15 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
              int stage, int flags) {
   constexpr int R = Halo<SCH>::R;
   constexpr int TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
-  constexpr int NP = TL + 2 * R;
-  constexpr int NV = TL + 6;
+  constexpr int NP = TL + 2 * R, SP = pad_row(NP);  // positions, row stride
+  constexpr int NV = TL + 6, SV = pad_row(NV);
+  constexpr int SH = pad_row(TL + 1), SQ = pad_row(TL);
   extern __shared__ double smem[];
-  double *sF = smem;                       // [10][TW][NP]: F+ vars 0..4, F- vars 5..9
-  double *sH = sF + 10 * TW * NP;          // [5][TW][TL+1]: face fluxes
+  double *sF = smem;                       // [10][TW][SP]: F+ vars 0..4, F- vars 5..9
+  double *sH = sF + 10 * TW * SP;          // [5][TW][SH]: face fluxes
   const bool ns = (flags & SW_NS) != 0;
-  double *sV = sH + 5 * TW * (TL + 1);     // [4][TW][NV]: viscous fluxes (NS)
-  double *sQ = sV + (ns ? 4 * TW * NV : 0);  // [5][TW][TL]: stage state (zeta sweep)
+  double *sV = sH + 5 * TW * SH;           // [4][TW][SV]: viscous fluxes (NS)
+  double *sQ = sV + (ns ? 4 * TW * SV : 0);  // [5][TW][SQ]: stage state (zeta sweep)
   __shared__ double sRed[kThreads / 32];
 
   const int t = blockIdx.x;
@@ -344,7 +349,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
         }
         if (DIR == 2 && g >= c0 && g < c0 + cl) {
 #pragma unroll
-          for (int v = 0; v < 5; ++v) sQ[(v * TW + w) * TL + (g - c0)] = q[v];
+          for (int v = 0; v < 5; ++v) sQ[(v * TW + w) * SQ + (g - c0)] = q[v];
         }
       } else {
         long long nidx;
@@ -362,8 +367,8 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     }
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      sF[(v * TW + w) * NP + p] = fp[v];
-      sF[((5 + v) * TW + w) * NP + p] = fn[v];
+      sF[(v * TW + w) * SP + p] = fp[v];
+      sF[((5 + v) * TW + w) * SP + p] = fn[v];
     }
   }
   if (ns) {
@@ -395,7 +400,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
         }
       }
 #pragma unroll
-      for (int v = 0; v < 4; ++v) sV[(v * TW + w) * NV + p] = fv[v];
+      for (int v = 0; v < 4; ++v) sV[(v * TW + w) * SV + p] = fv[v];
     }
   }
   __syncthreads();
@@ -408,13 +413,13 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     const int f = c0 + fl;
 #pragma unroll 1
     for (int v = 0; v < 5; ++v) {
-      const double *rowP = sF + (v * TW + w) * NP + (R - c0);
-      const double *rowN = sF + ((5 + v) * TW + w) * NP + (R - c0);
+      const double *rowP = sF + (v * TW + w) * SP + (R - c0);
+      const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - c0);
       auto Pacc = [rowP](int c) { return rowP[c]; };
       auto Nacc = [rowN](int c) { return rowN[c]; };
       double hp = recon_pos<SCH>(f, G.L, ts, physL, physR, compat, Pacc);
       double hn = recon_neg<SCH>(f, G.L, ts, physL, physR, Nacc);
-      sH[(v * TW + w) * (TL + 1) + fl] = hp + hn;
+      sH[(v * TW + w) * SH + fl] = hp + hn;
     }
   }
   __syncthreads();
@@ -442,14 +447,14 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     double d[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      const double *h = sH + (v * TW + w) * (TL + 1);
+      const double *h = sH + (v * TW + w) * SH;
       d[v] = h[c + 1] - h[c];
     }
     double dv[4] = {0.0, 0.0, 0.0, 0.0};
     if (ns) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        const double *row = sV + (v * TW + w) * NV + (3 - c0);
+        const double *row = sV + (v * TW + w) * SV + (3 - c0);
         auto Vacc = [row](int cc) { return row[cc]; };
         dv[v] = diff_at(g, G.L, ts, physL, physR, Vacc);
       }
@@ -485,7 +490,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
         const double *__restrict__ qn = B.q[0];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const double ui = sQ[(v * TW + w) * TL + c];
+          const double ui = sQ[(v * TW + w) * SQ + c];
           const double un = stage == 0 ? 0.0 : qn[v * N + idx];
           const double x = rk3_update(stage, r[v], ui, un, dt);
           if (!isfinite(x)) st |= ST_NONFINITE;
