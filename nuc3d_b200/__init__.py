@@ -20,7 +20,11 @@ import numpy as np
 
 from .metrics import metrics_from_nodes  # noqa: F401  (host-side block::getJacobians)
 
-_LIB_PATH = Path(__file__).resolve().parent / "libnuc3d_b200.so"
+import os
+
+# NUC3D_LIB selects another build of the library (e.g. a variant compiled with
+# different tile options); by default the in-tree build is used.
+_LIB_PATH = Path(os.environ.get("NUC3D_LIB") or Path(__file__).resolve().parent / "libnuc3d_b200.so")
 
 NUC3D_OK, NUC3D_EINVAL, NUC3D_ECUDA, NUC3D_ESTATE, NUC3D_ENUMERIC, NUC3D_ENOTSUP = range(6)
 ST_NEG_PRESSURE, ST_ENERGY_RESET, ST_NONFINITE = 1, 2, 4

@@ -45,8 +45,16 @@ def _stale(out: Path, deps) -> bool:
     return any(Path(d).stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, defines=(), out: Path | None = None,
+          build_dir: Path | None = None) -> Path:
+    """Compile the library; `defines` (e.g. ["NUC3D_SWEEP_MINB=3"]) select tile options,
+    `out`/`build_dir` put a variant build elsewhere."""
+    global BUILD, LIB
+    if out is not None:
+        LIB = Path(out)
+    if build_dir is not None:
+        BUILD = Path(build_dir)
+    BUILD.mkdir(parents=True, exist_ok=True)
     headers = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "nuc3d_gpu.h"]
     cc = nvcc()
     procs, objs = [], []
@@ -55,7 +63,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         obj = BUILD / (src.stem + ".o")
         objs.append(obj)
         if force or _stale(obj, [src, *headers, Path(__file__)]):
-            cmd = [cc, *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
+            cmd = [cc, *ARCH, *COMMON, *extra, *[f"-D{d}" for d in defines], "-c", str(src),
+                   "-o", str(obj)]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd), flush=True)
@@ -75,7 +84,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
                "-ldl", "-lpthread"]
         subprocess.run(cmd, check=True)
     probe_src = CSRC / "probe.cu"
-    if force or _stale(PROBE_LIB, [probe_src, Path(__file__)]):
+    if out is None and (force or _stale(PROBE_LIB, [probe_src, Path(__file__)])):
         subprocess.run([cc, *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
                         str(probe_src), "-o", str(PROBE_LIB), "-lcudart_static", "-lrt", "-ldl",
                         "-lpthread"], check=True)

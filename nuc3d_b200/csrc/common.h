@@ -49,7 +49,20 @@ struct BlockDev {
   double *prim;          // NS: u, v, w, T (4*N)
   double *vis;           // NS: contravariant viscous fluxes, [dir][var 1..4] (12*N)
   double *dvis;          // NS exact mode: d(Fv)/dxi and d(Gv)/deta, vars 1..4 (8*N)
+  double *ghost;         // split flux of the ghost next to each physical face: at
+                         // ghost + goff[f], 5 components of A_f*B_f slab cells (F+ on
+                         // left faces, F- on right faces)
+  long long goff[6];     // -1 for neighbour faces
   FaceDev face[6];
+};
+
+// Physical faces of all blocks, laid end to end for the BC ghost pass.
+constexpr int kMaxFaceJobs = 6 * 512;
+struct FaceJobs {
+  int njobs;
+  int block[kMaxFaceJobs];
+  unsigned char face[kMaxFaceJobs];
+  int start[kMaxFaceJobs + 1];  // prefix sums of 256-cell tiles
 };
 
 struct SolverParams {
@@ -85,6 +98,8 @@ struct Launch {
   SolverParams P;
   TileMap tm_dir[3];
   TileMap tm_cells;
+  const FaceJobs *d_jobs;  // device copy
+  int bc_tiles;            // CTAs of the BC ghost pass (0: no physical faces)
   cudaStream_t stream;
 };
 

@@ -29,6 +29,15 @@ namespace NUC3D_NS {
 // sector).  kThreads = TW*TL + 32 makes every phase a single round: TW*(TL+2R) <= 288
 // split fluxes, TW*(TL+1) faces, TW*TL cells, so no warp idles at a barrier waiting
 // for a one-lane tail.
+#ifndef NUC3D_SEQ_SPLITS
+#define NUC3D_SEQ_SPLITS 0  // 1: the ten face reconstructions strictly one at a time
+#endif
+#ifndef NUC3D_SPLIT_ITEMS
+#define NUC3D_SPLIT_ITEMS 0  // 1: F+ and F- faces reconstructed by different threads
+#endif
+#ifndef NUC3D_SWEEP_MINB
+#define NUC3D_SWEEP_MINB 4  // resident sweep CTAs per SM the register budget is cut for (measured best)
+#endif
 constexpr int kTW = 4, kTL = 64;
 constexpr int kThreads = kTW * kTL + 32;
 template <int DIR> struct Tile { static constexpr int TW = kTW, TL = kTL; };
@@ -70,6 +79,9 @@ __host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
   size_t n = (size_t)10 * TW * pad_row(TL + 2 * R) + (size_t)5 * TW * pad_row(TL + 1);
   if (ns) n += (size_t)4 * TW * pad_row(TL + 6);
   if (DIR == 2) n += (size_t)5 * TW * pad_row(TL);
+#if NUC3D_SPLIT_ITEMS
+  n += (size_t)5 * TW * pad_row(TL + 1);
+#endif
   return n * sizeof(double);
 }
 
@@ -285,7 +297,7 @@ __device__ __forceinline__ double rk3_update(int stage, double R, double u_i, do
 }
 
 template <int DIR, int SCH>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
 sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
              int stage, int flags) {
   constexpr int R = Halo<SCH>::R;
@@ -356,12 +368,19 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
         const int nb = ghost_cell(blocks, B, DIR, g, sa, sb, P.bfs, nidx);
         if (nb >= 0) {
           cell_split(blocks[nb], stage, nidx, DIR, P, fp, fn, s, q, st);
-        } else if (g == -1) {
-          const long long eidx = 0 * G.sL + wl * G.sW + o * G.sO;
-          bc_ghost_flux(B, stage, DIR, 0, eidx, P, fp, st);
-        } else if (g == G.L) {
-          const long long eidx = (long long)(G.L - 1) * G.sL + wl * G.sW + o * G.sO;
-          bc_ghost_flux(B, stage, DIR, 1, eidx, P, fn, st);
+        } else if (g == -1 || g == G.L) {
+          // ghost next to a physical face, filled by bc_ghost_kernel this stage
+          const int f = 2 * DIR + (g < 0 ? 0 : 1);
+          const int A = DIR == 0 ? n[1] : (DIR == 1 ? n[2] : n[0]);
+          const long long area = (long long)A * (DIR == 0 ? n[2] : (DIR == 1 ? n[0] : n[1]));
+          const double *gh = B.ghost + B.goff[f] + (sa + (long long)A * sb);
+          if (g < 0) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) fp[v] = __ldg(gh + v * area);
+          } else {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) fn[v] = __ldg(gh + v * area);
+          }
         }
       }
     }
@@ -407,10 +426,47 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
 
   // ---- phase 2: faces c0 .. c0+cl ----
   const bool compat = P.weno5z_compat != 0;
+#if NUC3D_SPLIT_ITEMS
+  // one work item = (face, split): the positive and negative reconstructions of a
+  // face run on different threads; sH holds F+ faces, sHn the F- faces.
+  double *sHn = sQ + (DIR == 2 ? 5 * TW * SQ : 0);
+  for (int e = threadIdx.x; e < 2 * TW * (TL + 1); e += kThreads) {
+    const int side = e / (TW * (TL + 1));
+    const int r = e - side * (TW * (TL + 1));
+    const int fl = r % (TL + 1), w = r / (TL + 1);
+    if (w >= nw || fl > cl) continue;
+    const int f = c0 + fl;
+#pragma unroll 1
+    for (int v = 0; v < 5; ++v) {
+      if (side == 0) {
+        const double *rowP = sF + (v * TW + w) * SP + (R - c0);
+        auto Pacc = [rowP](int c) { return rowP[c]; };
+        sH[(v * TW + w) * SH + fl] = recon_pos<SCH>(f, G.L, ts, physL, physR, compat, Pacc);
+      } else {
+        const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - c0);
+        auto Nacc = [rowN](int c) { return rowN[c]; };
+        sHn[(v * TW + w) * SH + fl] = recon_neg<SCH>(f, G.L, ts, physL, physR, Nacc);
+      }
+    }
+  }
+#else
   for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
     const int fl = e % (TL + 1), w = e / (TL + 1);
     if (w >= nw || fl > cl) continue;
     const int f = c0 + fl;
+#if NUC3D_SEQ_SPLITS
+    // the ten reconstructions one after the other (fewer live registers)
+#pragma unroll 1
+    for (int k = 0; k < 10; ++k) {
+      const int v = k >> 1;
+      const double *row = sF + ((k & 1 ? 5 + v : v) * TW + w) * SP + (R - c0);
+      auto Acc = [row](int c) { return row[c]; };
+      double h = (k & 1) ? recon_neg<SCH>(f, G.L, ts, physL, physR, Acc)
+                         : recon_pos<SCH>(f, G.L, ts, physL, physR, compat, Acc);
+      double *dst = sH + (v * TW + w) * SH + fl;
+      if (k & 1) *dst = *dst + h; else *dst = h;
+    }
+#else
 #pragma unroll 1
     for (int v = 0; v < 5; ++v) {
       const double *rowP = sF + (v * TW + w) * SP + (R - c0);
@@ -421,7 +477,9 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       double hn = recon_neg<SCH>(f, G.L, ts, physL, physR, Nacc);
       sH[(v * TW + w) * SH + fl] = hp + hn;
     }
+#endif
   }
+#endif
   __syncthreads();
 
   // ---- phase 3: cells: flux difference, RHS accumulation, RK stage ----
@@ -448,7 +506,12 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       const double *h = sH + (v * TW + w) * SH;
+#if NUC3D_SPLIT_ITEMS
+      const double *hn = sQ + (DIR == 2 ? 5 * TW * SQ : 0) + (v * TW + w) * SH;
+      d[v] = (h[c + 1] + hn[c + 1]) - (h[c] + hn[c]);
+#else
       d[v] = h[c + 1] - h[c];
+#endif
     }
     double dv[4] = {0.0, 0.0, 0.0, 0.0};
     if (ns) {
@@ -517,6 +580,43 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       atomicMax(&S->max_eig_bits, (unsigned long long)__double_as_longlong(m));
     }
   }
+  if (st) atomicOr(&S->status, st);
+}
+
+// ---------------------------------------------------------------------------------
+// Physical-face ghost fluxes: the reference's setBC (src/boundaryConditions.cpp:95-108)
+// fills the ghost slabs before its sweeps; here one thread per face cell evaluates
+// the slot next to the face (the only one the exterior reconstruction reads).
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+bc_ghost_kernel(const BlockDev *__restrict__ blocks, const FaceJobs *__restrict__ jobs,
+                SolverParams P, StepState *S, int stage) {
+  int lo = 0, hi = jobs->njobs - 1;
+  const int t = blockIdx.x;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (jobs->start[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  const BlockDev &B = blocks[jobs->block[lo]];
+  const int f = jobs->face[lo], d = f >> 1, side = f & 1;
+  const int A = d == 0 ? B.n[1] : (d == 1 ? B.n[2] : B.n[0]);
+  const int Bn = d == 0 ? B.n[2] : (d == 1 ? B.n[0] : B.n[1]);
+  const long long r = (long long)(t - jobs->start[lo]) * 256 + threadIdx.x;
+  if (r >= (long long)A * Bn) return;
+  const int a = (int)(r % A), b = (int)(r / A);
+  int i, j, k;
+  const int pos = side ? B.n[d] - 1 : 0;
+  if (d == 0) { i = pos; j = a; k = b; }
+  else if (d == 1) { i = b; j = pos; k = a; }
+  else { i = a; j = b; k = pos; }
+  const long long eidx = ((long long)k * B.n[1] + j) * B.n[0] + i;
+  unsigned st = 0;
+  double out[5];
+  bc_ghost_flux(B, stage, d, side, eidx, P, out, st);
+  double *gh = B.ghost + B.goff[f] + r;
+  const long long area = (long long)A * Bn;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) gh[v * area] = out[v];
   if (st) atomicOr(&S->status, st);
 }
 
@@ -661,6 +761,10 @@ inline cudaError_t launch_sweep(const Launch &L, int stage, int flags) {
 inline cudaError_t launch_stage(const Launch &L, int stage, bool rk, bool eig) {
   cudaError_t e;
   const bool ns = L.P.model == MODEL_NS;
+  if (L.bc_tiles > 0) {
+    bc_ghost_kernel<<<L.bc_tiles, 256, 0, L.stream>>>(L.d_blocks, L.d_jobs, L.P, L.d_state, stage);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (ns) {
     const int nt = L.tm_cells.tile_start[L.tm_cells.nblocks];
     prim_kernel<<<nt, kCellTile, 0, L.stream>>>(L.d_blocks, L.tm_cells, L.P, L.d_state, stage);
@@ -681,6 +785,11 @@ cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig) {
 
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags) {
   const int f = flags | (L.P.model == MODEL_NS ? SW_NS : 0);
+  if (L.bc_tiles > 0) {
+    bc_ghost_kernel<<<L.bc_tiles, 256, 0, L.stream>>>(L.d_blocks, L.d_jobs, L.P, L.d_state, stage);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   if (dir == 0) return launch_sweep<0>(L, stage, f);
   if (dir == 1) return launch_sweep<1>(L, stage, f);
   return launch_sweep<2>(L, stage, f & ~SW_RK);

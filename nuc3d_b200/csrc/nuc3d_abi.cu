@@ -44,7 +44,8 @@ struct HostBlock {
   double bcv[6][5];
   double *q[3] = {nullptr, nullptr, nullptr};
   double *rhs = nullptr, *jac = nullptr, *met = nullptr, *dxyz = nullptr;
-  double *prim = nullptr, *vis = nullptr, *dvis = nullptr;
+  double *prim = nullptr, *vis = nullptr, *dvis = nullptr, *ghost = nullptr;
+  long long goff[6] = {-1, -1, -1, -1, -1, -1};
   bool metrics = false;
 };
 
@@ -69,6 +70,7 @@ struct nuc3d_ctx {
   SolverParams P{};
   std::vector<HostBlock> blocks;
   BlockDev *d_blocks = nullptr;
+  FaceJobs *d_jobs = nullptr;
   StepState *d_state = nullptr;
   Launch L{};
   bool finalized = false;
@@ -163,10 +165,12 @@ int nuc3d_destroy(nuc3d_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->drop_graph();
   for (auto &b : c->blocks) {
-    for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.dxyz, b.prim, b.vis, b.dvis})
+    for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.dxyz, b.prim, b.vis, b.dvis,
+                   b.ghost})
       if (p) cudaFree(p);
   }
   if (c->d_blocks) cudaFree(c->d_blocks);
+  if (c->d_jobs) cudaFree(c->d_jobs);
   if (c->d_state) cudaFree(c->d_state);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -211,10 +215,21 @@ int nuc3d_block_add(nuc3d_ctx *c, int nx, int ny, int nz, const int bc_type[6], 
     if (e == cudaSuccess) e = cudaMalloc(&b.vis, 12 * nb);
     if (e == cudaSuccess) e = cudaMalloc(&b.dvis, 8 * nb);
   }
+  {
+    long long off = 0;
+    for (int f = 0; f < 6; ++f) {
+      if (bc_type[f] != -1) continue;
+      const int d = f >> 1;
+      const long long area = d == 0 ? (long long)ny * nz : (d == 1 ? (long long)nz * nx : (long long)nx * ny);
+      b.goff[f] = off;
+      off += 5 * area;
+    }
+    if (off > 0 && e == cudaSuccess) e = cudaMalloc(&b.ghost, off * sizeof(double));
+  }
   for (int s = 0; s < 3 && e == cudaSuccess; ++s) e = cudaMemset(b.q[s], 0, 5 * nb);
   if (e == cudaSuccess) e = cudaMemset(b.rhs, 0, 5 * nb);
   if (e != cudaSuccess) {
-    for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.prim, b.vis, b.dvis})
+    for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.prim, b.vis, b.dvis, b.ghost})
       if (p) cudaFree(p);
     return fail(NUC3D_ECUDA, "block allocation (%lld cells): %s", b.N, cudaGetErrorString(e));
   }
@@ -292,6 +307,8 @@ int nuc3d_finalize(nuc3d_ctx *c) {
     d.prim = b.prim;
     d.vis = b.vis;
     d.dvis = b.dvis;
+    d.ghost = b.ghost;
+    for (int f = 0; f < 6; ++f) d.goff[f] = b.goff[f];
     for (int f = 0; f < 6; ++f) {
       d.face[f].type = b.bc_type[f];
       d.face[f].id = b.bc_id[f];
@@ -318,6 +335,27 @@ int nuc3d_finalize(nuc3d_ctx *c) {
       L.tm_dir[d].tile_start[bi + 1] = L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, b.n);
     L.tm_cells.tile_start[bi + 1] = L.tm_cells.tile_start[bi] + (int)((b.N + 255) / 256);
   }
+  // physical faces for the BC ghost pass
+  std::vector<FaceJobs> jv(1);
+  FaceJobs &J = jv[0];
+  std::memset(&J, 0, sizeof(J));
+  for (int bi = 0; bi < nbk; ++bi) {
+    const HostBlock &b = c->blocks[bi];
+    for (int f = 0; f < 6; ++f) {
+      if (b.bc_type[f] != -1) continue;
+      const int d = f >> 1;
+      const long long area = d == 0 ? (long long)b.n[1] * b.n[2]
+                                    : (d == 1 ? (long long)b.n[2] * b.n[0] : (long long)b.n[0] * b.n[1]);
+      J.block[J.njobs] = bi;
+      J.face[J.njobs] = (unsigned char)f;
+      J.start[J.njobs + 1] = J.start[J.njobs] + (int)((area + 255) / 256);
+      ++J.njobs;
+    }
+  }
+  L.bc_tiles = J.start[J.njobs];
+  CUDA_TRY(cudaMalloc(&c->d_jobs, sizeof(FaceJobs)));
+  CUDA_TRY(cudaMemcpy(c->d_jobs, &J, sizeof(FaceJobs), cudaMemcpyHostToDevice));
+  L.d_jobs = c->d_jobs;
   c->finalized = true;
   return NUC3D_OK;
 }
