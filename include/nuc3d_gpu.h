@@ -135,6 +135,30 @@ int nuc3d_profile_sweep(nuc3d_ctx *ctx, int dir, int reps, double *ms_per_launch
 int nuc3d_block_get_prim(nuc3d_ctx *ctx, int block, double *prim);
 int nuc3d_block_get_vis(nuc3d_ctx *ctx, int block, double *vis);
 
+/* ---- Allocation-free right-hand side -------------------------------------------
+   No counterpart in the reference: it exists for callers that cannot allocate device
+   memory where they evaluate the right-hand side (inside a CUDA stream capture that
+   must not allocate, under a host framework that owns all device memory, in loops
+   where an allocation would stall).  One Euler3d block: all array arguments are
+   DEVICE pointers owned by the caller (q, metrics as in nuc3d_block_set_metrics, and
+   the output rhs, 5N); bc_type[f] is -1 (physical) or 0 (the block is its own
+   neighbour, i.e. periodic).  It calls no cudaMalloc/cudaFree: its working memory
+   (block descriptor, step state, face list, 40 bytes per cell of every physical face)
+   is a static device array of NUC3D_NOALLOC_SCRATCH_BYTES that every GPU loading the
+   library keeps until the process exits; larger blocks are rejected with NUC3D_EINVAL.
+   The first call on a device looks up that array's device address and sets kernel
+   attributes, so make the first call before any stream capture.  All calls share the
+   array: calls that overlap on the GPU (different streams, or threads without
+   ordering) race and must be serialised by the caller.  With dt_local non-NULL the
+   call waits for the stream and returns 1/max eigenvalue; with NULL it is
+   asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream). */
+#define NUC3D_NOALLOC_SCRATCH_BYTES (8u << 20)
+int nuc3d_rhs_noalloc(const nuc3d_config *cfg, int device, int nx, int ny, int nz,
+                      const int bc_type[6], const int bc_id[6], const double *bc_values,
+                      const double *q, const double *jac, const double *xi_xyz,
+                      const double *eta_xyz, const double *zeta_xyz, const double *dxyz,
+                      double *rhs, double *dt_local, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

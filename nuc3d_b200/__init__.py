@@ -36,6 +36,7 @@ EXPORTED = (
     "nuc3d_block_q_device", "nuc3d_rhs", "nuc3d_block_get_rhs", "nuc3d_step", "nuc3d_sync",
     "nuc3d_get_time", "nuc3d_set_time", "nuc3d_get_status", "nuc3d_set_stream",
     "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis", "nuc3d_profile_sweep",
+    "nuc3d_rhs_noalloc",
 )
 
 
@@ -107,6 +108,9 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_block_get_prim.argtypes = [P, I, PD]
     lib.nuc3d_block_get_vis.argtypes = [P, I, PD]
     lib.nuc3d_profile_sweep.argtypes = [P, I, I, PD]
+    PI = ctypes.POINTER(I)
+    lib.nuc3d_rhs_noalloc.argtypes = [ctypes.POINTER(_Cfg), I, I, I, I, PI, PI, PD, P, P, P, P,
+                                      P, P, P, PD, P]
     for name in EXPORTED:
         if name != "nuc3d_last_error":
             getattr(lib, name).restype = ctypes.c_int

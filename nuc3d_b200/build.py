@@ -28,6 +28,7 @@ UNITS = {
     "kernels_exact.cu": ["-fmad=false"],
     "kernels_fast.cu": ["-fmad=true"],
     "nuc3d_abi.cu": [],
+    "nuc3d_noalloc.cu": [],
 }
 
 

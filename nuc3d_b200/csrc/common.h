@@ -106,6 +106,9 @@ struct Launch {
 // One right-hand-side evaluation of every block at RK stage `stage`
 // (state q[stage]); rk: also apply the TVD-RK3 update; eig: reduce the
 // eigenvalue maximum that fixes dt.  Defined once per arithmetic mode.
+// Message returned by nuc3d_last_error() for the calling thread.
+void set_error_message(const char *msg);
+
 // configure(): one-time kernel attributes (dynamic shared memory opt-in).
 // tile_count(): CTAs of the dir-sweep over one block of n cells.
 namespace exact {

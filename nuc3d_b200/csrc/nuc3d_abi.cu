@@ -62,6 +62,8 @@ int parse_scheme(const char *s, int *out) {
 
 }  // namespace
 
+void nuc3d::set_error_message(const char *msg) { g_err = msg; }
+
 struct nuc3d_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
