@@ -55,7 +55,7 @@ typedef struct nuc3d_ctx nuc3d_ctx;
 
 typedef struct {
   /* Method.in: scheme_{x,y,z}_ivs and scheme_{x,y,z}_vis (src/fieldOperator.cpp:20-33).
-     ivs: "weno5js" | "weno5z" | "weno7js"; vis: "cd6". */
+     ivs: "weno5js" | "weno5z" | "weno7js" | "crweno5" | "hccs"; vis: "cd6". */
   const char *scheme_ivs[3];
   const char *scheme_vis[3];
   /* PhysModel.in positional entries (src/physicsModel.cpp:65-69):

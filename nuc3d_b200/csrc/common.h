@@ -53,6 +53,8 @@ struct BlockDev {
                          // ghost + goff[f], 5 components of A_f*B_f slab cells (F+ on
                          // left faces, F- on right faces)
   long long goff[6];     // -1 for neighbour faces
+  double *fh;            // compact schemes: face fluxes [sys][line][face] of one direction
+  double *rows;          // compact schemes: tridiagonal rows [row][4][sys*lines + line]
   FaceDev face[6];
 };
 
@@ -97,6 +99,7 @@ struct Launch {
   StepState *d_state;
   SolverParams P;
   TileMap tm_dir[3];
+  TileMap tm_sys[3];       // compact schemes: 256-system tiles per direction
   TileMap tm_cells;
   const FaceJobs *d_jobs;  // device copy
   int bc_tiles;            // CTAs of the BC ghost pass (0: no physical faces)

@@ -29,12 +29,6 @@ namespace NUC3D_NS {
 // sector).  kThreads = TW*TL + 32 makes every phase a single round: TW*(TL+2R) <= 288
 // split fluxes, TW*(TL+1) faces, TW*TL cells, so no warp idles at a barrier waiting
 // for a one-lane tail.
-#ifndef NUC3D_SEQ_SPLITS
-#define NUC3D_SEQ_SPLITS 0  // 1: the ten face reconstructions strictly one at a time
-#endif
-#ifndef NUC3D_SPLIT_ITEMS
-#define NUC3D_SPLIT_ITEMS 0  // 1: F+ and F- faces reconstructed by different threads
-#endif
 #ifndef NUC3D_SWEEP_MINB
 #define NUC3D_SWEEP_MINB 4  // resident sweep CTAs per SM the register budget is cut for (measured best)
 #endif
@@ -42,7 +36,9 @@ constexpr int kTW = 4, kTL = 64;
 constexpr int kThreads = kTW * kTL + 32;
 template <int DIR> struct Tile { static constexpr int TW = kTW, TL = kTL; };
 
-template <int SCH> struct Halo { static constexpr int R = (SCH == SCH_WENO7JS) ? 4 : 3; };
+template <int SCH> struct Halo {
+  static constexpr int R = (SCH == SCH_WENO7JS || SCH == SCH_HCCS) ? 4 : 3;
+};
 
 // Row strides of the shared-memory tiles, padded so that the TW rows of one warp
 // access fall in different bank halves (stride = 8 mod 16 doubles).
@@ -79,9 +75,6 @@ __host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
   size_t n = (size_t)10 * TW * pad_row(TL + 2 * R) + (size_t)5 * TW * pad_row(TL + 1);
   if (ns) n += (size_t)4 * TW * pad_row(TL + 6);
   if (DIR == 2) n += (size_t)5 * TW * pad_row(TL);
-#if NUC3D_SPLIT_ITEMS
-  n += (size_t)5 * TW * pad_row(TL + 1);
-#endif
   return n * sizeof(double);
 }
 
@@ -223,9 +216,9 @@ __device__ __forceinline__ double recon_pos(int f, int L, int ts, bool physL, bo
       default: return weno5js(P(0), P(1), P(2), P(3), P(4));
     }
   }
-  if (SCH == SCH_WENO7JS) {
+  if (SCH == SCH_WENO7JS || SCH == SCH_HCCS) {
     double s[7] = {P(f - 4), P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), P(f + 2)};
-    return weno7js(s);
+    return SCH == SCH_HCCS ? weno7z(s) : weno7js(s);
   } else if (SCH == SCH_WENO5Z) {
     return weno5z(P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), compat && f >= ts && f <= L - ts);
   } else {
@@ -251,9 +244,9 @@ __device__ __forceinline__ double recon_neg(int f, int L, int ts, bool physL, bo
       default: return weno5js(Nf(5), Nf(4), Nf(3), Nf(2), Nf(1));
     }
   }
-  if (SCH == SCH_WENO7JS) {
+  if (SCH == SCH_WENO7JS || SCH == SCH_HCCS) {
     double s[7] = {Nf(f + 3), Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), Nf(f - 3)};
-    return weno7js(s);
+    return SCH == SCH_HCCS ? weno7z(s) : weno7js(s);
   } else if (SCH == SCH_WENO5Z) {
     return weno5z(Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), false);
   } else {
@@ -296,72 +289,89 @@ __device__ __forceinline__ double rk3_update(int stage, double R, double u_i, do
   return 1.0 / 3.0 * u_n + 2.0 / 3.0 * (rhs * dt + u_i);
 }
 
-template <int DIR, int SCH>
-__global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
-sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
-             int stage, int flags) {
-  constexpr int R = Halo<SCH>::R;
-  constexpr int TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
-  constexpr int NP = TL + 2 * R, SP = pad_row(NP);  // positions, row stride
-  constexpr int NV = TL + 6, SV = pad_row(NV);
-  constexpr int SH = pad_row(TL + 1), SQ = pad_row(TL);
-  extern __shared__ double smem[];
-  double *sF = smem;                       // [10][TW][SP]: F+ vars 0..4, F- vars 5..9
-  double *sH = sF + 10 * TW * SP;          // [5][TW][SH]: face fluxes
-  const bool ns = (flags & SW_NS) != 0;
-  double *sV = sH + 5 * TW * SH;           // [4][TW][SV]: viscous fluxes (NS)
-  double *sQ = sV + (ns ? 4 * TW * SV : 0);  // [5][TW][SQ]: stage state (zeta sweep)
-  __shared__ double sRed[kThreads / 32];
+// Geometry of one sweep tile (a CTA's share of one block's lines).
+struct TileCtx {
+  int t, b;
+  const BlockDev *B;
+  Geo G;
+  int n[3];
+  int c0, cl, w0, nw, o;  // first cell and cell count along the lines, first lane, lanes, outer index
+  long long N;
+  int ts;
+  bool physL, physR;
+};
 
-  const int t = blockIdx.x;
-  const int b = find_block(tm, t);
-  const BlockDev &B = blocks[b];
-  const int n[3] = {B.n[0], B.n[1], B.n[2]};
-  const Geo G = make_geo(DIR, n);
-  int lt = t - tm.tile_start[b];
-  const int nch = (G.L + TL - 1) / TL;
-  const int nwg = (G.nW + TW - 1) / TW;
+template <int DIR>
+__device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ blocks, const TileMap &tm,
+                                               const SolverParams &P) {
+  constexpr int TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
+  TileCtx T;
+  T.t = blockIdx.x;
+  T.b = find_block(tm, T.t);
+  T.B = &blocks[T.b];
+  for (int d = 0; d < 3; ++d) T.n[d] = T.B->n[d];
+  T.G = make_geo(DIR, T.n);
+  int lt = T.t - tm.tile_start[T.b];
+  const int nch = (T.G.L + TL - 1) / TL;
+  const int nwg = (T.G.nW + TW - 1) / TW;
   const int ch = lt % nch;
   lt /= nch;
   const int wg = lt % nwg;
-  const int o = lt / nwg;
-  const int c0 = ch * TL;
-  const int cl = min(TL, G.L - c0);
-  const int w0 = wg * TW;
-  const int nw = min(TW, G.nW - w0);
-  const long long N = B.N;
-  const int ts = P.ts[DIR];
-  const bool physL = B.face[2 * DIR].type < 0;
-  const bool physR = B.face[2 * DIR + 1].type < 0;
-  const bool eig = (flags & SW_EIG) != 0;
-  unsigned st = 0;
-  double emax = 0.0;
+  T.o = lt / nwg;
+  T.c0 = ch * TL;
+  T.cl = min(TL, T.G.L - T.c0);
+  T.w0 = wg * TW;
+  T.nw = min(TW, T.G.nW - T.w0);
+  T.N = T.B->N;
+  T.ts = P.ts[DIR];
+  T.physL = T.B->face[2 * DIR].type < 0;
+  T.physR = T.B->face[2 * DIR + 1].type < 0;
+  return T;
+}
 
-  // ---- phase 1: split fluxes at line positions c0-R .. c0+cl+R-1 ----
+// Shared-memory row strides of a sweep tile.
+template <int DIR, int SCH> struct TileSmem {
+  static constexpr int R = Halo<SCH>::R, TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
+  static constexpr int NP = TL + 2 * R, SP = pad_row(NP);
+  static constexpr int NV = TL + 6, SV = pad_row(NV);
+  static constexpr int SH = pad_row(TL + 1), SQ = pad_row(TL);
+};
+
+// Phase 1: split fluxes F+/F- of the tile's line positions c0-R .. c0+cl+R-1 into sF
+// ([10][TW][SP]); own cells of the zeta tile also leave their state in sQ; eig reduces
+// max(|U|+c|grad xi|) over the three directions.
+template <int DIR, int SCH>
+__device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks, const TileCtx &T,
+                                            const SolverParams &P, int stage, bool eig, double *sF,
+                                            double *sQ, unsigned &st, double &emax) {
+  using M = TileSmem<DIR, SCH>;
+  constexpr int R = M::R, TW = M::TW, NP = M::NP, SP = M::SP, SQ = M::SQ;
+  const BlockDev &B = *T.B;
+  const Geo &G = T.G;
   for (int e = threadIdx.x; e < TW * NP; e += kThreads) {
     int p, w;
     if (DIR == 0) { p = e % NP; w = e / NP; } else { w = e % TW; p = e / TW; }
     double fp[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, fn[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const int g = c0 + p - R;
-    if (w < nw && p < cl + 2 * R) {
-      const int wl = w0 + w;
-      const int sa = (DIR == 1) ? o : wl, sb = (DIR == 1) ? wl : o;
+    const int g = T.c0 + p - R;
+    if (w < T.nw && p < T.cl + 2 * R) {
+      const int wl = T.w0 + w;
+      const int sa = (DIR == 1) ? T.o : wl, sb = (DIR == 1) ? wl : T.o;
       double q[5];
       CellPrim s;
       if (g >= 0 && g < G.L) {
-        const long long idx = g * G.sL + wl * G.sW + o * G.sO;
+        const long long idx = g * G.sL + wl * G.sW + T.o * G.sO;
         cell_split(B, stage, idx, DIR, P, fp, fn, s, q, st);
-        if (eig && g >= c0 && g < c0 + cl) {
+        if (eig && g >= T.c0 && g < T.c0 + T.cl) {
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
             const double *m = B.met[d];
-            double ev = eigen_cell(s, __ldg(m + idx), __ldg(m + N + idx), __ldg(m + 2 * N + idx));
+            double ev = eigen_cell(s, __ldg(m + idx), __ldg(m + T.N + idx), __ldg(m + 2 * T.N + idx));
             emax = ev > emax ? ev : emax;
           }
         }
-        if (DIR == 2 && g >= c0 && g < c0 + cl) {
+        if (DIR == 2 && sQ && g >= T.c0 && g < T.c0 + T.cl) {
 #pragma unroll
-          for (int v = 0; v < 5; ++v) sQ[(v * TW + w) * SQ + (g - c0)] = q[v];
+          for (int v = 0; v < 5; ++v) sQ[(v * TW + w) * SQ + (g - T.c0)] = q[v];
         }
       } else {
         long long nidx;
@@ -371,8 +381,8 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
         } else if (g == -1 || g == G.L) {
           // ghost next to a physical face, filled by bc_ghost_kernel this stage
           const int f = 2 * DIR + (g < 0 ? 0 : 1);
-          const int A = DIR == 0 ? n[1] : (DIR == 1 ? n[2] : n[0]);
-          const long long area = (long long)A * (DIR == 0 ? n[2] : (DIR == 1 ? n[0] : n[1]));
+          const int A = DIR == 0 ? T.n[1] : (DIR == 1 ? T.n[2] : T.n[0]);
+          const long long area = (long long)A * (DIR == 0 ? T.n[2] : (DIR == 1 ? T.n[0] : T.n[1]));
           const double *gh = B.ghost + B.goff[f] + (sa + (long long)A * sb);
           if (g < 0) {
 #pragma unroll
@@ -390,99 +400,60 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       sF[((5 + v) * TW + w) * SP + p] = fn[v];
     }
   }
-  if (ns) {
-    for (int e = threadIdx.x; e < TW * NV; e += kThreads) {
-      int p, w;
-      if (DIR == 0) { p = e % NV; w = e / NV; } else { w = e % TW; p = e / TW; }
-      double fv[4] = {0.0, 0.0, 0.0, 0.0};
-      const int g = c0 + p - 3;
-      if (w < nw && p < cl + 6) {
-        const int wl = w0 + w;
-        const int sa = (DIR == 1) ? o : wl, sb = (DIR == 1) ? wl : o;
-        const double *vis = nullptr;
-        long long idx = -1, NN = N;
-        if (g >= 0 && g < G.L) {
-          idx = g * G.sL + wl * G.sW + o * G.sO;
-          vis = B.vis;
-        } else {
-          long long nidx;
-          const int nb = ghost_cell(blocks, B, DIR, g, sa, sb, P.bfs, nidx);
-          if (nb >= 0) {
-            idx = nidx;
-            vis = blocks[nb].vis;
-            NN = blocks[nb].N;
-          }
-        }
-        if (vis) {
-#pragma unroll
-          for (int v = 0; v < 4; ++v) fv[v] = __ldg(vis + (DIR * 4 + v) * NN + idx);
-        }
-      }
-#pragma unroll
-      for (int v = 0; v < 4; ++v) sV[(v * TW + w) * SV + p] = fv[v];
-    }
-  }
-  __syncthreads();
+}
 
-  // ---- phase 2: faces c0 .. c0+cl ----
-  const bool compat = P.weno5z_compat != 0;
-#if NUC3D_SPLIT_ITEMS
-  // one work item = (face, split): the positive and negative reconstructions of a
-  // face run on different threads; sH holds F+ faces, sHn the F- faces.
-  double *sHn = sQ + (DIR == 2 ? 5 * TW * SQ : 0);
-  for (int e = threadIdx.x; e < 2 * TW * (TL + 1); e += kThreads) {
-    const int side = e / (TW * (TL + 1));
-    const int r = e - side * (TW * (TL + 1));
-    const int fl = r % (TL + 1), w = r / (TL + 1);
-    if (w >= nw || fl > cl) continue;
-    const int f = c0 + fl;
-#pragma unroll 1
-    for (int v = 0; v < 5; ++v) {
-      if (side == 0) {
-        const double *rowP = sF + (v * TW + w) * SP + (R - c0);
-        auto Pacc = [rowP](int c) { return rowP[c]; };
-        sH[(v * TW + w) * SH + fl] = recon_pos<SCH>(f, G.L, ts, physL, physR, compat, Pacc);
+// Viscous fluxes of the tile's line positions c0-3 .. c0+cl+2 into sV ([4][TW][SV]).
+template <int DIR, int SCH>
+__device__ __forceinline__ void phase_vis(const BlockDev *__restrict__ blocks, const TileCtx &T,
+                                          const SolverParams &P, double *sV) {
+  using M = TileSmem<DIR, SCH>;
+  constexpr int TW = M::TW, NV = M::NV, SV = M::SV;
+  const BlockDev &B = *T.B;
+  const Geo &G = T.G;
+  for (int e = threadIdx.x; e < TW * NV; e += kThreads) {
+    int p, w;
+    if (DIR == 0) { p = e % NV; w = e / NV; } else { w = e % TW; p = e / TW; }
+    double fv[4] = {0.0, 0.0, 0.0, 0.0};
+    const int g = T.c0 + p - 3;
+    if (w < T.nw && p < T.cl + 6) {
+      const int wl = T.w0 + w;
+      const int sa = (DIR == 1) ? T.o : wl, sb = (DIR == 1) ? wl : T.o;
+      const double *vis = nullptr;
+      long long idx = -1, NN = T.N;
+      if (g >= 0 && g < G.L) {
+        idx = g * G.sL + wl * G.sW + T.o * G.sO;
+        vis = B.vis;
       } else {
-        const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - c0);
-        auto Nacc = [rowN](int c) { return rowN[c]; };
-        sHn[(v * TW + w) * SH + fl] = recon_neg<SCH>(f, G.L, ts, physL, physR, Nacc);
+        long long nidx;
+        const int nb = ghost_cell(blocks, B, DIR, g, sa, sb, P.bfs, nidx);
+        if (nb >= 0) {
+          idx = nidx;
+          vis = blocks[nb].vis;
+          NN = blocks[nb].N;
+        }
+      }
+      if (vis) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) fv[v] = __ldg(vis + (DIR * 4 + v) * NN + idx);
       }
     }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) sV[(v * TW + w) * SV + p] = fv[v];
   }
-#else
-  for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
-    const int fl = e % (TL + 1), w = e / (TL + 1);
-    if (w >= nw || fl > cl) continue;
-    const int f = c0 + fl;
-#if NUC3D_SEQ_SPLITS
-    // the ten reconstructions one after the other (fewer live registers)
-#pragma unroll 1
-    for (int k = 0; k < 10; ++k) {
-      const int v = k >> 1;
-      const double *row = sF + ((k & 1 ? 5 + v : v) * TW + w) * SP + (R - c0);
-      auto Acc = [row](int c) { return row[c]; };
-      double h = (k & 1) ? recon_neg<SCH>(f, G.L, ts, physL, physR, Acc)
-                         : recon_pos<SCH>(f, G.L, ts, physL, physR, compat, Acc);
-      double *dst = sH + (v * TW + w) * SH + fl;
-      if (k & 1) *dst = *dst + h; else *dst = h;
-    }
-#else
-#pragma unroll 1
-    for (int v = 0; v < 5; ++v) {
-      const double *rowP = sF + (v * TW + w) * SP + (R - c0);
-      const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - c0);
-      auto Pacc = [rowP](int c) { return rowP[c]; };
-      auto Nacc = [rowN](int c) { return rowN[c]; };
-      double hp = recon_pos<SCH>(f, G.L, ts, physL, physR, compat, Pacc);
-      double hn = recon_neg<SCH>(f, G.L, ts, physL, physR, Nacc);
-      sH[(v * TW + w) * SH + fl] = hp + hn;
-    }
-#endif
-  }
-#endif
-  __syncthreads();
+}
 
-  // ---- phase 3: cells: flux difference, RHS accumulation, RK stage ----
+// Phase 3: per cell, dF from the face fluxes in sH, RHS accumulation (src/euler3d.cpp:368-427,
+// src/NaiverStokes3d.cpp:401-513), and on the zeta sweep the TVD-RK3 stage.
+template <int DIR, int SCH>
+__device__ __forceinline__ void phase_cells(const TileCtx &T, const SolverParams &P, StepState *S,
+                                            int stage, int flags, const double *sH, const double *sV,
+                                            const double *sQ, unsigned &st) {
+  using M = TileSmem<DIR, SCH>;
+  constexpr int TW = M::TW, TL = M::TL, SV = M::SV, SH = M::SH, SQ = M::SQ;
+  const BlockDev &B = *T.B;
+  const Geo &G = T.G;
+  const long long N = T.N;
+  const bool ns = (flags & SW_NS) != 0;
   double *__restrict__ rhs = B.rhs;
   double dt = 0.0;
   if (flags & SW_RK) {
@@ -490,36 +461,31 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       double me = __longlong_as_double((long long)S->max_eig_bits);
       double dt_local = 1.0 / me;
       dt = dt_local * P.cfl;
-      if (t == 0 && threadIdx.x == 0) S->dt = dt;
+      if (T.t == 0 && threadIdx.x == 0) S->dt = dt;
     } else {
       dt = S->dt;
     }
-    if (stage == 2 && t == 0 && threadIdx.x == 0) S->time = S->time + dt;
+    if (stage == 2 && T.t == 0 && threadIdx.x == 0) S->time = S->time + dt;
   }
   for (int e = threadIdx.x; e < TW * TL; e += kThreads) {
     int c, w;
     if (DIR == 0) { c = e % TL; w = e / TL; } else { w = e % TW; c = e / TW; }
-    if (w >= nw || c >= cl) continue;
-    const int g = c0 + c;
-    const long long idx = g * G.sL + (w0 + w) * G.sW + o * G.sO;
+    if (w >= T.nw || c >= T.cl) continue;
+    const int g = T.c0 + c;
+    const long long idx = g * G.sL + (T.w0 + w) * G.sW + T.o * G.sO;
     double d[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       const double *h = sH + (v * TW + w) * SH;
-#if NUC3D_SPLIT_ITEMS
-      const double *hn = sQ + (DIR == 2 ? 5 * TW * SQ : 0) + (v * TW + w) * SH;
-      d[v] = (h[c + 1] + hn[c + 1]) - (h[c] + hn[c]);
-#else
       d[v] = h[c + 1] - h[c];
-#endif
     }
     double dv[4] = {0.0, 0.0, 0.0, 0.0};
     if (ns) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        const double *row = sV + (v * TW + w) * SV + (3 - c0);
+        const double *row = sV + (v * TW + w) * SV + (3 - T.c0);
         auto Vacc = [row](int cc) { return row[cc]; };
-        dv[v] = diff_at(g, G.L, ts, physL, physR, Vacc);
+        dv[v] = diff_at(g, G.L, T.ts, T.physL, T.physR, Vacc);
       }
     }
     if (DIR == 0) {
@@ -565,21 +531,230 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       }
     }
   }
+}
 
-  if (eig) {
+__device__ __forceinline__ void reduce_eig(double emax, double *sRed, StepState *S) {
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      double x = __shfl_xor_sync(0xffffffffu, emax, off);
-      emax = x > emax ? x : emax;
-    }
-    if ((threadIdx.x & 31) == 0) sRed[threadIdx.x >> 5] = emax;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double m = sRed[0];
-      for (int i = 1; i < kThreads / 32; ++i) m = sRed[i] > m ? sRed[i] : m;
-      atomicMax(&S->max_eig_bits, (unsigned long long)__double_as_longlong(m));
+  for (int off = 16; off > 0; off >>= 1) {
+    double x = __shfl_xor_sync(0xffffffffu, emax, off);
+    emax = x > emax ? x : emax;
+  }
+  if ((threadIdx.x & 31) == 0) sRed[threadIdx.x >> 5] = emax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = sRed[0];
+    for (int i = 1; i < kThreads / 32; ++i) m = sRed[i] > m ? sRed[i] : m;
+    atomicMax(&S->max_eig_bits, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// Explicit-scheme sweep: phases split -> faces -> cells in one CTA.
+template <int DIR, int SCH>
+__global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
+sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
+             int stage, int flags) {
+  using M = TileSmem<DIR, SCH>;
+  constexpr int R = M::R, TW = M::TW, TL = M::TL, SP = M::SP, SV = M::SV, SH = M::SH;
+  extern __shared__ double smem[];
+  double *sF = smem;                        // [10][TW][SP]: F+ vars 0..4, F- vars 5..9
+  double *sH = sF + 10 * TW * SP;           // [5][TW][SH]: face fluxes
+  const bool ns = (flags & SW_NS) != 0;
+  double *sV = sH + 5 * TW * SH;            // [4][TW][SV]: viscous fluxes (NS)
+  double *sQ = sV + (ns ? 4 * TW * SV : 0); // [5][TW][SQ]: stage state (zeta sweep)
+  __shared__ double sRed[kThreads / 32];
+
+  const TileCtx T = decode_tile<DIR>(blocks, tm, P);
+  const bool eig = (flags & SW_EIG) != 0;
+  unsigned st = 0;
+  double emax = 0.0;
+  phase_split<DIR, SCH>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st, emax);
+  if (ns) phase_vis<DIR, SCH>(blocks, T, P, sV);
+  __syncthreads();
+
+  // ---- faces c0 .. c0+cl: the ten reconstructions of each face ----
+  const bool compat = P.weno5z_compat != 0;
+  for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
+    const int fl = e % (TL + 1), w = e / (TL + 1);
+    if (w >= T.nw || fl > T.cl) continue;
+    const int f = T.c0 + fl;
+#pragma unroll 1
+    for (int v = 0; v < 5; ++v) {
+      const double *rowP = sF + (v * TW + w) * SP + (R - T.c0);
+      const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - T.c0);
+      auto Pacc = [rowP](int c) { return rowP[c]; };
+      auto Nacc = [rowN](int c) { return rowN[c]; };
+      double hp = recon_pos<SCH>(f, T.G.L, T.ts, T.physL, T.physR, compat, Pacc);
+      double hn = recon_neg<SCH>(f, T.G.L, T.ts, T.physL, T.physR, Nacc);
+      sH[(v * TW + w) * SH + fl] = hp + hn;
     }
   }
+  __syncthreads();
+  phase_cells<DIR, SCH>(T, P, S, stage, flags, sH, sV, sQ, st);
+  if (eig) reduce_eig(emax, sRed, S);
+  if (st) atomicOr(&S->status, st);
+}
+
+// ---------------------------------------------------------------------------------
+// Compact schemes (crweno5, hccs): the reference solves, per line, variable and split,
+// a tridiagonal system over faces ts .. n-ts (src/crweno5.cpp:44-401, src/hccs.cpp:45-493)
+// with explicit end rows and explicit block-edge faces.  Three kernels per direction:
+//   compact_rows_kernel   split fluxes (phase 1 of the sweep), then per face either the
+//                         explicit value (into fh) or the tridiagonal row (a, b, c, d)
+//   compact_thomas_kernel one thread per system: the reference's Thomas elimination and
+//                         back substitution (src/crweno5.cpp:207-218), into fh
+//   compact_finish_kernel faces from fh, then phase 3 (difference, RHS, RK)
+// Layouts per block and direction (nl lines = nW*nO, system s = sys*nl + line, sys =
+// 2*variable + split): fh[(sys*nl + line)*(L+1) + face]; rows[(r*4 + k)*(10*nl) + s].
+// ---------------------------------------------------------------------------------
+template <int SCH>
+__device__ __forceinline__ void compact_row(const double f[5], double &lo, double &di, double &up,
+                                            double &rhs) {
+  if (SCH == SCH_CRWENO5) crweno5_row(f, lo, di, up, rhs);
+  else hccs_row(f, lo, di, up, rhs);
+}
+
+template <int DIR, int SCH>
+__global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
+compact_rows_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
+                    int stage, int flags) {
+  using M = TileSmem<DIR, SCH>;
+  constexpr int R = M::R, TW = M::TW, TL = M::TL, SP = M::SP;
+  extern __shared__ double smem[];
+  double *sF = smem;
+  __shared__ double sRed[kThreads / 32];
+  const TileCtx T = decode_tile<DIR>(blocks, tm, P);
+  const bool eig = (flags & SW_EIG) != 0;
+  unsigned st = 0;
+  double emax = 0.0;
+  phase_split<DIR, SCH>(blocks, T, P, stage, eig, sF, nullptr, st, emax);
+  __syncthreads();
+  const BlockDev &B = *T.B;
+  const int L = T.G.L, ts = T.ts, m = L - 2 * ts + 1;
+  const long long nl = (long long)T.G.nW * T.G.nO;
+  const long long S10 = 10 * nl;
+  for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
+    const int fl = e % (TL + 1), w = e / (TL + 1);
+    if (w >= T.nw || fl > T.cl) continue;
+    const int f = T.c0 + fl;
+    const long long line = (T.w0 + w) + (long long)T.G.nW * T.o;
+#pragma unroll 1
+    for (int sys = 0; sys < 10; ++sys) {
+      const int v = sys >> 1, side = sys & 1;
+      const double *row = sF + ((side ? 5 + v : v) * TW + w) * SP + (R - T.c0);
+      auto A = [row](int c) { return row[c]; };
+      const long long sidx = sys * nl + line;
+      if (f < ts || f > L - ts) {
+        const double h = side ? recon_neg<SCH>(f, L, ts, T.physL, T.physR, A)
+                              : recon_pos<SCH>(f, L, ts, T.physL, T.physR, false, A);
+        B.fh[sidx * (L + 1) + f] = h;
+        continue;
+      }
+      const int r = f - ts;
+      double a, b, c, d;
+      if (r == 0 || r == m - 1) {
+        // explicit end rows: WENO5-JS (crweno5) or WENO7-Z (hccs)
+        a = 0.0; b = 1.0; c = 0.0;
+        d = side ? recon_neg<SCH>(f, L, ts, false, false, A)
+                 : recon_pos<SCH>(f, L, ts, false, false, false, A);
+      } else {
+        double s5[5];
+        if (side) { s5[0] = A(f + 2); s5[1] = A(f + 1); s5[2] = A(f); s5[3] = A(f - 1); s5[4] = A(f - 2); }
+        else { s5[0] = A(f - 3); s5[1] = A(f - 2); s5[2] = A(f - 1); s5[3] = A(f); s5[4] = A(f + 1); }
+        double lo, di, up;
+        compact_row<SCH>(s5, lo, di, up, d);
+        b = di;
+        if (side) { a = up; c = lo; } else { a = lo; c = up; }
+      }
+      double *rw = B.rows + (long long)r * 4 * S10 + sidx;
+      rw[0] = a;
+      rw[S10] = b;
+      rw[2 * S10] = c;
+      rw[3 * S10] = d;
+    }
+  }
+  if (eig) reduce_eig(emax, sRed, S);
+  if (st) atomicOr(&S->status, st);
+}
+
+// One thread per (line, variable, split) system of one direction.
+template <int DIR>
+__global__ void __launch_bounds__(256)
+compact_thomas_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P) {
+  const int b = find_block(tm, blockIdx.x);
+  const BlockDev &B = blocks[b];
+  const int n[3] = {B.n[0], B.n[1], B.n[2]};
+  const Geo G = make_geo(DIR, n);
+  const long long nl = (long long)G.nW * G.nO, S10 = 10 * nl;
+  const long long s = (long long)(blockIdx.x - tm.tile_start[b]) * 256 + threadIdx.x;
+  if (s >= S10) return;
+  const int L = G.L, ts = P.ts[DIR], m = L - 2 * ts + 1;
+  double *rw = B.rows + s;
+  double cp = rw[2 * S10], dp = rw[3 * S10];
+  for (int r = 1; r < m; ++r) {
+    double *x = rw + (long long)r * 4 * S10;
+    const double a = x[0], bb = x[S10], c = x[2 * S10], d = x[3 * S10];
+    const double den = bb - cp * a;
+    cp = c / den;
+    dp = (d - dp * a) / den;
+    x[2 * S10] = cp;
+    x[3 * S10] = dp;
+  }
+  double *fh = B.fh + s * (L + 1) + ts;
+  double xv = dp;
+  fh[m - 1] = xv;
+  for (int r = m - 2; r >= 0; --r) {
+    const double *x = rw + (long long)r * 4 * S10;
+    xv = x[3 * S10] - x[2 * S10] * xv;
+    fh[r] = xv;
+  }
+}
+
+template <int DIR, int SCH>
+__global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
+compact_finish_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
+                      int stage, int flags) {
+  using M = TileSmem<DIR, SCH>;
+  constexpr int TW = M::TW, TL = M::TL, SV = M::SV, SH = M::SH, SQ = M::SQ;
+  extern __shared__ double smem[];
+  double *sH = smem;
+  double *sV = sH + 5 * TW * SH;
+  const bool ns = (flags & SW_NS) != 0;
+  double *sQ = sV + (ns ? 4 * TW * SV : 0);
+  const TileCtx T = decode_tile<DIR>(blocks, tm, P);
+  const BlockDev &B = *T.B;
+  unsigned st = 0;
+  if (DIR == 2 && (flags & SW_RK)) {
+    // stage state of the tile's own cells (with the energy reset), as phase 1 leaves it
+    for (int e = threadIdx.x; e < TW * TL; e += kThreads) {
+      int c, w;
+      w = e % TW; c = e / TW;
+      if (w >= T.nw || c >= T.cl) continue;
+      const long long idx = (T.c0 + c) * T.G.sL + (T.w0 + w) * T.G.sW + T.o * T.G.sO;
+      double q[5];
+      CellPrim s;
+      load_q(B.q[stage], T.N, idx, q);
+      con2prim(q, __ldg(B.jac + idx), P.gamma, P.mach, s, st);
+      q[4] = s.q4;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) sQ[(v * TW + w) * SQ + c] = q[v];
+    }
+  }
+  if (ns) phase_vis<DIR, SCH>(blocks, T, P, sV);
+  const int L = T.G.L;
+  const long long nl = (long long)T.G.nW * T.G.nO;
+  for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
+    const int fl = e % (TL + 1), w = e / (TL + 1);
+    if (w >= T.nw || fl > T.cl) continue;
+    const long long line = (T.w0 + w) + (long long)T.G.nW * T.o;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double hp = B.fh[((2 * v) * nl + line) * (L + 1) + T.c0 + fl];
+      const double hn = B.fh[((2 * v + 1) * nl + line) * (L + 1) + T.c0 + fl];
+      sH[(v * TW + w) * SH + fl] = hp + hn;
+    }
+  }
+  __syncthreads();
+  phase_cells<DIR, SCH>(T, P, S, stage, flags, sH, sV, sQ, st);
   if (st) atomicOr(&S->status, st);
 }
 
@@ -747,12 +922,45 @@ inline cudaError_t launch_sweep_t(const Launch &L, int stage, int flags) {
   return cudaGetLastError();
 }
 
+template <int DIR, int SCH>
+__host__ __device__ inline size_t compact_rows_smem_bytes() {
+  using M = TileSmem<DIR, SCH>;
+  return (size_t)10 * M::TW * M::SP * sizeof(double);
+}
+template <int DIR, int SCH>
+__host__ __device__ inline size_t compact_finish_smem_bytes(bool ns) {
+  using M = TileSmem<DIR, SCH>;
+  size_t n = (size_t)5 * M::TW * M::SH;
+  if (ns) n += (size_t)4 * M::TW * M::SV;
+  if (DIR == 2) n += (size_t)5 * M::TW * M::SQ;
+  return n * sizeof(double);
+}
+
+template <int DIR, int SCH>
+inline cudaError_t launch_compact_t(const Launch &L, int stage, int flags) {
+  const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
+  compact_rows_kernel<DIR, SCH><<<ntiles, kThreads, compact_rows_smem_bytes<DIR, SCH>(), L.stream>>>(
+      L.d_blocks, L.tm_dir[DIR], L.P, L.d_state, stage, flags & SW_EIG);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int nsys = L.tm_sys[DIR].tile_start[L.tm_sys[DIR].nblocks];
+  compact_thomas_kernel<DIR><<<nsys, 256, 0, L.stream>>>(L.d_blocks, L.tm_sys[DIR], L.P);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  compact_finish_kernel<DIR, SCH><<<ntiles, kThreads,
+                                    compact_finish_smem_bytes<DIR, SCH>((flags & SW_NS) != 0),
+                                    L.stream>>>(L.d_blocks, L.tm_dir[DIR], L.P, L.d_state, stage,
+                                                flags & ~SW_EIG);
+  return cudaGetLastError();
+}
+
 template <int DIR>
 inline cudaError_t launch_sweep(const Launch &L, int stage, int flags) {
   switch (L.P.scheme[DIR]) {
     case SCH_WENO5JS: return launch_sweep_t<DIR, SCH_WENO5JS>(L, stage, flags);
     case SCH_WENO5Z: return launch_sweep_t<DIR, SCH_WENO5Z>(L, stage, flags);
     case SCH_WENO7JS: return launch_sweep_t<DIR, SCH_WENO7JS>(L, stage, flags);
+    case SCH_CRWENO5: return launch_compact_t<DIR, SCH_CRWENO5>(L, stage, flags);
+    case SCH_HCCS: return launch_compact_t<DIR, SCH_HCCS>(L, stage, flags);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -801,11 +1009,24 @@ inline cudaError_t configure_t() {
                               (int)sweep_smem_bytes<DIR, SCH>(true));
 }
 
+template <int DIR, int SCH>
+inline cudaError_t configure_compact_t() {
+  cudaError_t e = cudaFuncSetAttribute(compact_rows_kernel<DIR, SCH>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)compact_rows_smem_bytes<DIR, SCH>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(compact_finish_kernel<DIR, SCH>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)compact_finish_smem_bytes<DIR, SCH>(true));
+}
+
 template <int DIR>
 inline cudaError_t configure_dir() {
   cudaError_t e;
   if ((e = configure_t<DIR, SCH_WENO5JS>()) != cudaSuccess) return e;
   if ((e = configure_t<DIR, SCH_WENO5Z>()) != cudaSuccess) return e;
+  if ((e = configure_compact_t<DIR, SCH_CRWENO5>()) != cudaSuccess) return e;
+  if ((e = configure_compact_t<DIR, SCH_HCCS>()) != cudaSuccess) return e;
   return configure_t<DIR, SCH_WENO7JS>();
 }
 

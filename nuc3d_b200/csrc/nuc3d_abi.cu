@@ -6,6 +6,7 @@
 // (src/block.cpp:569-594): per step three stages, dt fixed at stage 0 from the
 // global eigenvalue maximum (src/PDEData3d.cpp:152-170), time += dt.  A step is
 // captured once as a CUDA graph and replayed.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -45,6 +46,7 @@ struct HostBlock {
   double *q[3] = {nullptr, nullptr, nullptr};
   double *rhs = nullptr, *jac = nullptr, *met = nullptr, *dxyz = nullptr;
   double *prim = nullptr, *vis = nullptr, *dvis = nullptr, *ghost = nullptr;
+  double *fh = nullptr, *rows = nullptr;  // compact schemes
   long long goff[6] = {-1, -1, -1, -1, -1, -1};
   bool metrics = false;
 };
@@ -54,8 +56,8 @@ int parse_scheme(const char *s, int *out) {
   if (!std::strcmp(s, "weno5js")) *out = SCH_WENO5JS;
   else if (!std::strcmp(s, "weno5z")) *out = SCH_WENO5Z;
   else if (!std::strcmp(s, "weno7js")) *out = SCH_WENO7JS;
-  else if (!std::strcmp(s, "crweno5") || !std::strcmp(s, "hccs"))
-    return fail(NUC3D_ENOTSUP, "scheme '%s' is not implemented by this library", s);
+  else if (!std::strcmp(s, "crweno5")) *out = SCH_CRWENO5;
+  else if (!std::strcmp(s, "hccs")) *out = SCH_HCCS;
   else return fail(NUC3D_EINVAL, "unknown reconstruction scheme '%s'", s);
   return NUC3D_OK;
 }
@@ -168,7 +170,7 @@ int nuc3d_destroy(nuc3d_ctx *c) {
   c->drop_graph();
   for (auto &b : c->blocks) {
     for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.dxyz, b.prim, b.vis, b.dvis,
-                   b.ghost})
+                   b.ghost, b.fh, b.rows})
       if (p) cudaFree(p);
   }
   if (c->d_blocks) cudaFree(c->d_blocks);
@@ -228,10 +230,27 @@ int nuc3d_block_add(nuc3d_ctx *c, int nx, int ny, int nz, const int bc_type[6], 
     }
     if (off > 0 && e == cudaSuccess) e = cudaMalloc(&b.ghost, off * sizeof(double));
   }
+  {
+    // compact schemes: face fluxes of all systems of one direction and their tridiagonal
+    // rows, sized for the largest compact direction of the block (directions run one
+    // after the other)
+    long long fh_n = 0, rows_n = 0;
+    for (int d = 0; d < 3; ++d) {
+      const int sc = c->P.scheme[d];
+      if (sc != SCH_CRWENO5 && sc != SCH_HCCS) continue;
+      const long long nl = (long long)b.N / n[d];
+      const long long m = n[d] - 2 * c->P.ts[d] + 1;
+      fh_n = std::max(fh_n, 10 * nl * (n[d] + 1));
+      rows_n = std::max(rows_n, 4 * m * 10 * nl);
+    }
+    if (fh_n > 0 && e == cudaSuccess) e = cudaMalloc(&b.fh, fh_n * sizeof(double));
+    if (rows_n > 0 && e == cudaSuccess) e = cudaMalloc(&b.rows, rows_n * sizeof(double));
+  }
   for (int s = 0; s < 3 && e == cudaSuccess; ++s) e = cudaMemset(b.q[s], 0, 5 * nb);
   if (e == cudaSuccess) e = cudaMemset(b.rhs, 0, 5 * nb);
   if (e != cudaSuccess) {
-    for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.prim, b.vis, b.dvis, b.ghost})
+    for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.prim, b.vis, b.dvis, b.ghost,
+                   b.fh, b.rows})
       if (p) cudaFree(p);
     return fail(NUC3D_ECUDA, "block allocation (%lld cells): %s", b.N, cudaGetErrorString(e));
   }
@@ -310,6 +329,8 @@ int nuc3d_finalize(nuc3d_ctx *c) {
     d.vis = b.vis;
     d.dvis = b.dvis;
     d.ghost = b.ghost;
+    d.fh = b.fh;
+    d.rows = b.rows;
     for (int f = 0; f < 6; ++f) d.goff[f] = b.goff[f];
     for (int f = 0; f < 6; ++f) {
       d.face[f].type = b.bc_type[f];
@@ -328,13 +349,18 @@ int nuc3d_finalize(nuc3d_ctx *c) {
   for (int d = 0; d < 3; ++d) {
     L.tm_dir[d].nblocks = nbk;
     L.tm_dir[d].tile_start[0] = 0;
+    L.tm_sys[d].nblocks = nbk;
+    L.tm_sys[d].tile_start[0] = 0;
   }
   L.tm_cells.nblocks = nbk;
   L.tm_cells.tile_start[0] = 0;
   for (int bi = 0; bi < nbk; ++bi) {
     const HostBlock &b = c->blocks[bi];
-    for (int d = 0; d < 3; ++d)
+    for (int d = 0; d < 3; ++d) {
       L.tm_dir[d].tile_start[bi + 1] = L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, b.n);
+      const long long nsys = 10 * (b.N / b.n[d]);
+      L.tm_sys[d].tile_start[bi + 1] = L.tm_sys[d].tile_start[bi] + (int)((nsys + 255) / 256);
+    }
     L.tm_cells.tile_start[bi + 1] = L.tm_cells.tile_start[bi] + (int)((b.N + 255) / 256);
   }
   // physical faces for the BC ghost pass

@@ -126,6 +126,79 @@ __device__ __forceinline__ double weno7js(const double f[7]) {
 #endif
 }
 
+// WENO7-Z: the 7th-order stencils of weno7js with Z weights, tau7 = |is0 - is3|,
+// eps 1e-40 -- hccs's block-edge faces and explicit end rows (src/hccs.cpp:92-142,516-990).
+__device__ __forceinline__ double weno7z(const double f[7]) {
+  double is0 = f[0] * (547.0 * f[0] - 3882.0 * f[1] + 4642.0 * f[2] - 1854.0 * f[3]) +
+               f[1] * (7043.0 * f[1] - 17246.0 * f[2] + 7042.0 * f[3]) +
+               f[2] * (11003.0 * f[2] - 9402.0 * f[3]) + 2107.0 * f[3] * f[3];
+  double is1 = f[1] * (267.0 * f[1] - 1642.0 * f[2] + 1602.0 * f[3] - 494.0 * f[4]) +
+               f[2] * (2843.0 * f[2] - 5966.0 * f[3] + 1922.0 * f[4]) +
+               f[3] * (3443.0 * f[3] - 2522.0 * f[4]) + 547.0 * f[4] * f[4];
+  double is2 = f[2] * (547.0 * f[2] - 2522.0 * f[3] + 1922.0 * f[4] - 494.0 * f[5]) +
+               f[3] * (3443.0 * f[3] - 5966.0 * f[4] + 1602.0 * f[5]) +
+               f[4] * (2843.0 * f[4] - 1642.0 * f[5]) + 267.0 * f[5] * f[5];
+  double is3 = f[3] * (2107.0 * f[3] - 9402.0 * f[4] + 7042.0 * f[5] - 1854.0 * f[6]) +
+               f[4] * (11003.0 * f[4] - 17246.0 * f[5] + 4642.0 * f[6]) +
+               f[5] * (7043.0 * f[5] - 3882.0 * f[6]) + 547.0 * f[6] * f[6];
+  double q0 = kA7[0][0] * f[0] + kA7[0][1] * f[1] + kA7[0][2] * f[2] + kA7[0][3] * f[3];
+  double q1 = kA7[1][0] * f[1] + kA7[1][1] * f[2] + kA7[1][2] * f[3] + kA7[1][3] * f[4];
+  double q2 = kA7[2][0] * f[2] + kA7[2][1] * f[3] + kA7[2][2] * f[4] + kA7[2][3] * f[5];
+  double q3 = kA7[3][0] * f[3] + kA7[3][1] * f[4] + kA7[3][2] * f[5] + kA7[3][3] * f[6];
+  const double ss = 1.0e-40;
+  double tau7 = fabs(is0 - is3);
+  double a0 = kC7[0] * (1.0 + sq(tau7 / (ss + is0)));
+  double a1 = kC7[1] * (1.0 + sq(tau7 / (ss + is1)));
+  double a2 = kC7[2] * (1.0 + sq(tau7 / (ss + is2)));
+  double a3 = kC7[3] * (1.0 + sq(tau7 / (ss + is3)));
+  double s = a0 + a1 + a2 + a3;
+  double w0 = a0 / s, w1 = a1 / s, w2 = a2 / s, w3 = a3 / s;
+  return w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3;
+}
+
+// Interior row of the CRWENO5 tridiagonal system on an oriented 5-cell stencil f[0..4]
+// (src/crweno5.cpp:130-161 for F+, :310-340 for F-): JS indicators, weights
+// 0.2/0.5/0.3, eps 1e-6.  lo multiplies the unknown on the upwind side (a of F+, c of
+// F-), up the one on the downwind side.
+__device__ constexpr double kCR5[3] = {0.2, 0.5, 0.3};
+__device__ __forceinline__ void crweno5_row(const double f[5], double &lo, double &di, double &up,
+                                            double &rhs) {
+  W5 r = w5_parts(f[0], f[1], f[2], f[3], f[4], false);
+  const double ss = 1.0e-6;
+  double a0 = kCR5[0] / sq(ss + r.is0);
+  double a1 = kCR5[1] / sq(ss + r.is1);
+  double a2 = kCR5[2] / sq(ss + r.is2);
+  double s = a0 + a1 + a2;
+  double w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
+  lo = 2.0 / 3.0 * w0 + 1.0 / 3.0 * w1;
+  di = 1.0 / 3.0 * w0 + 2.0 / 3.0 * (w1 + w2);
+  up = 1.0 / 3.0 * w2;
+  rhs = 1.0 / 6.0 * w0 * f[1] + (5.0 * (w0 + w1) + w2) * f[2] / 6.0 + (w1 + 5.0 * w2) * f[3] / 6.0;
+}
+
+// Interior row of the hybrid compact scheme (src/hccs.cpp:145-188 for F+, :371-414
+// for F-): CRWENO5-Z weights (eps 1e-40), blended with the 7th-order compact central row
+// (2/7, 4/7, 1/7 | q7) by theta = 1/(1 + (sum alpha - 1)^2).
+__device__ __forceinline__ void hccs_row(const double f[5], double &lo, double &di, double &up,
+                                         double &rhs) {
+  W5 r = w5_parts(f[0], f[1], f[2], f[3], f[4], false);
+  const double ss = 1.0e-40;
+  double q7 = (-f[0] + 19.0 * f[1] + 239.0 * f[2] + 159.0 * f[3] + 4.0 * f[4]) / 420.0;
+  double tau = fabs(r.is2 - r.is0);
+  double a0 = kCR5[0] * (1.0 + sq(tau / (r.is0 + ss)));
+  double a1 = kCR5[1] * (1.0 + sq(tau / (r.is1 + ss)));
+  double a2 = kCR5[2] * (1.0 + sq(tau / (r.is2 + ss)));
+  double s = a0 + a1 + a2;
+  double w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
+  double theta = 1.0 / (1.0 + sq(s - 1.0));
+  lo = (2.0 / 3.0 * w0 + 1.0 / 3.0 * w1) * (1.0 - theta) + 2.0 / 7.0 * theta;
+  di = (1.0 / 3.0 * w0 + 2.0 / 3.0 * (w1 + w2)) * (1.0 - theta) + 4.0 / 7.0 * theta;
+  up = (1.0 / 3.0 * w2) * (1.0 - theta) + 1.0 / 7.0 * theta;
+  rhs = (1.0 / 6.0 * w0 * f[1] + (5.0 * (w0 + w1) + w2) * f[2] / 6.0 + (w1 + 5.0 * w2) * f[3] / 6.0) *
+            (1.0 - theta) +
+        q7 * theta;
+}
+
 // Reduced-order schemes on faces next to a physical boundary
 // (ReconstructionboundaryScheme, src/reconstructionBoundaryScheme.cpp:315-463).
 __device__ __forceinline__ double rb_second(double f0, double f1) { return 0.5 * (f0 + f1); }

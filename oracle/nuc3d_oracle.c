@@ -28,7 +28,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-enum { S_WENO5JS = 0, S_WENO5Z = 1, S_WENO7JS = 2 };
+enum { S_WENO5JS = 0, S_WENO5Z = 1, S_WENO7JS = 2, S_CRWENO5 = 3, S_HCCS = 4 };
 enum { R_LF = 0, R_AUSM = 1, R_AUSMP = 2 };
 
 typedef struct {
@@ -95,8 +95,11 @@ static double weno5(const double *f, int z, int bug) {
   return a0 / s * q0 + a1 / s * q1 + a2 / s * q2;
 }
 
-/* WENO7-JS on f[0..6], src/weno7js.cpp:84-136 */
-static double weno7(const double *f) {
+/* WENO7-JS on f[0..6], src/weno7js.cpp:84-136; z: the WENO7-Z weights of hccs
+   (tau7 = |is0 - is3|, src/hccs.cpp:125-137) */
+static double weno7zs(const double *f, int z);
+static double weno7(const double *f) { return weno7zs(f, 0); }
+static double weno7zs(const double *f, int z) {
   double is[4];
   is[0] = f[0] * (547.0 * f[0] - 3882.0 * f[1] + 4642.0 * f[2] - 1854.0 * f[3]) +
           f[1] * (7043.0 * f[1] - 17246.0 * f[2] + 7042.0 * f[3]) +
@@ -111,12 +114,51 @@ static double weno7(const double *f) {
           f[4] * (11003.0 * f[4] - 17246.0 * f[5] + 4642.0 * f[6]) +
           f[5] * (7043.0 * f[5] - 3882.0 * f[6]) + 547.0 * f[6] * f[6];
   double q[4], a[4];
+  double tau7 = fabs(is[0] - is[3]);
   for (int k = 0; k < 4; ++k) {
     q[k] = A7[k][0] * f[k] + A7[k][1] * f[k + 1] + A7[k][2] * f[k + 2] + A7[k][3] * f[k + 3];
-    a[k] = C7[k] / sq(1.0e-40 + is[k]);
+    a[k] = z ? C7[k] * (1.0 + sq(tau7 / (1.0e-40 + is[k]))) : C7[k] / sq(1.0e-40 + is[k]);
   }
   double s = a[0] + a[1] + a[2] + a[3];
   return a[0] / s * q[0] + a[1] / s * q[1] + a[2] / s * q[2] + a[3] / s * q[3];
+}
+
+/* Interior tridiagonal row on an oriented stencil f[0..4]: lo multiplies the upwind
+   neighbour, up the downwind one.  crweno5: src/crweno5.cpp:130-161 (JS weights
+   0.2/0.5/0.3, eps 1e-6); hccs: src/hccs.cpp:145-188 (Z weights eps 1e-40, blended with
+   the compact central row 2/7 4/7 1/7 | q7 by theta). */
+static const double CR5[3] = {0.2, 0.5, 0.3};
+static void compact_row(int hccs, const double *f, double *lo, double *di, double *up, double *rhs) {
+  double is0 = G0 * sq(f[0] - 2.0 * f[1] + f[2]) + G1 * sq(f[0] - 4.0 * f[1] + 3.0 * f[2]);
+  double is1 = G0 * sq(f[1] - 2.0 * f[2] + f[3]) + G1 * sq(f[1] - f[3]);
+  double is2 = G0 * sq(f[2] - 2.0 * f[3] + f[4]) + G1 * sq(3.0 * f[2] - 4.0 * f[3] + f[4]);
+  double a0, a1, a2;
+  if (hccs) {
+    double tau = fabs(is2 - is0);
+    a0 = CR5[0] * (1.0 + sq(tau / (is0 + 1.0e-40)));
+    a1 = CR5[1] * (1.0 + sq(tau / (is1 + 1.0e-40)));
+    a2 = CR5[2] * (1.0 + sq(tau / (is2 + 1.0e-40)));
+  } else {
+    a0 = CR5[0] / sq(1.0e-6 + is0);
+    a1 = CR5[1] / sq(1.0e-6 + is1);
+    a2 = CR5[2] / sq(1.0e-6 + is2);
+  }
+  double sum = a0 + a1 + a2;
+  double w0 = a0 / sum, w1 = a1 / sum, w2 = a2 / sum;
+  double l = 2.0 / 3.0 * w0 + 1.0 / 3.0 * w1;
+  double dd = 1.0 / 3.0 * w0 + 2.0 / 3.0 * (w1 + w2);
+  double u = 1.0 / 3.0 * w2;
+  double r = 1.0 / 6.0 * w0 * f[1] + (5.0 * (w0 + w1) + w2) * f[2] / 6.0 + (w1 + 5.0 * w2) * f[3] / 6.0;
+  if (hccs) {
+    double q7 = (-f[0] + 19.0 * f[1] + 239.0 * f[2] + 159.0 * f[3] + 4.0 * f[4]) / 420.0;
+    double th = 1.0 / (1.0 + sq(sum - 1.0));
+    l = (2.0 / 3.0 * w0 + 1.0 / 3.0 * w1) * (1.0 - th) + 2.0 / 7.0 * th;
+    dd = (1.0 / 3.0 * w0 + 2.0 / 3.0 * (w1 + w2)) * (1.0 - th) + 4.0 / 7.0 * th;
+    u = (1.0 / 3.0 * w2) * (1.0 - th) + 1.0 / 7.0 * th;
+    r = (1.0 / 6.0 * w0 * f[1] + (5.0 * (w0 + w1) + w2) * f[2] / 6.0 + (w1 + 5.0 * w2) * f[3] / 6.0) *
+            (1.0 - th) + q7 * th;
+  }
+  *lo = l; *di = dd; *up = u; *rhs = r;
 }
 
 /* ReconstructionboundaryScheme point schemes, src/reconstructionBoundaryScheme.cpp:315-463 */
@@ -383,63 +425,101 @@ static void line_ext(const oc_config *c, work_t *W, int bfs, int bi, int d, int 
   }
 }
 
+/* explicit face value of one split at face f: BL/BR or inner stencil of the scheme
+   (compact schemes use WENO5-JS / WENO7-Z there), or the exterior point schemes */
+static double face_explicit(const oc_config *c, int d, int side, int f, int L, int ts, int physL,
+                            int physR, int bfs, const double *e) {
+#define P(cc) e[(cc) + bfs]
+  int sch = c->scheme[d];
+  int exL = physL && f < ts, exR = physR && f > L - ts;
+  if (side == 0) {
+    if (exR) {
+      int m = L - f;
+      if (m == 0) return P(L - 1);
+      if (m == 1) return rb2(P(L - 2), P(L - 1));
+      if (m == 2) return rb3(P(L - 4), P(L - 3), P(L - 2));
+      double s[5] = {P(L - 6), P(L - 5), P(L - 4), P(L - 3), P(L - 2)};
+      return weno5(s, 0, 0);
+    }
+    if (exL) {
+      if (f == 0) return e[bfs - 1];
+      if (f == 1) return rb2(P(0), P(1));
+      if (f == 2) return rb3(P(0), P(1), P(2));
+      double s[5] = {P(0), P(1), P(2), P(3), P(4)};
+      return weno5(s, 0, 0);
+    }
+    if (sch == S_WENO7JS || sch == S_HCCS) {
+      double s[7];
+      for (int k = 0; k < 7; ++k) s[k] = P(f - 4 + k);
+      return weno7zs(s, sch == S_HCCS);
+    }
+    double s[5];
+    for (int k = 0; k < 5; ++k) s[k] = P(f - 3 + k);
+    int z = sch == S_WENO5Z;
+    return weno5(s, z, z && c->compat && f >= ts && f <= L - ts);
+  }
+  if (exR) {
+    int m = L - f;
+    if (m == 0) return e[L + bfs];
+    if (m == 1) return rb2(P(L - 1), P(L - 2));
+    if (m == 2) return rb3(P(L - 1), P(L - 2), P(L - 3));
+    double s[5] = {P(L - 1), P(L - 2), P(L - 3), P(L - 4), P(L - 5)};
+    return weno5(s, 0, 0);
+  }
+  if (exL) {
+    if (f == 0) return P(0);
+    if (f == 1) return rb2(P(1), P(0));
+    if (f == 2) return rb3(P(3), P(2), P(1));
+    double s[5] = {P(5), P(4), P(3), P(2), P(1)};
+    return weno5(s, 0, 0);
+  }
+  if (sch == S_WENO7JS || sch == S_HCCS) {
+    double s[7];
+    for (int k = 0; k < 7; ++k) s[k] = P(f + 3 - k);
+    return weno7zs(s, sch == S_HCCS);
+  }
+  double s[5];
+  for (int k = 0; k < 5; ++k) s[k] = P(f + 2 - k);
+  return weno5(s, sch == S_WENO5Z, 0);
+#undef P
+}
+
 /* face values of one line: positive and negative reconstruction (upwind +1 / -1) */
 static void line_faces(const oc_config *c, const oc_block *b, int d, int bfs, const double *eP,
                        const double *eN, double *face) {
-  int L = b->n[d], ts = (c->scheme[d] == S_WENO7JS) ? 4 : 3;
+  int L = b->n[d], sch = c->scheme[d];
+  int ts = (sch == S_WENO7JS || sch == S_HCCS) ? 4 : 3;
   int physL = b->bc_type[2 * d] < 0, physR = b->bc_type[2 * d + 1] < 0;
-#define P(cc) eP[(cc) + bfs]
-#define NN(cc) eN[(cc) + bfs]
-  for (int f = 0; f <= L; ++f) {
-    double hp, hn;
-    int exL = physL && f < ts, exR = physR && f > L - ts;
-    /* ---- F+ ---- */
-    if (exR) {
-      int m = L - f;
-      if (m == 0) hp = P(L - 1);
-      else if (m == 1) hp = rb2(P(L - 2), P(L - 1));
-      else if (m == 2) hp = rb3(P(L - 4), P(L - 3), P(L - 2));
-      else { double s[5] = {P(L - 6), P(L - 5), P(L - 4), P(L - 3), P(L - 2)}; hp = weno5(s, 0, 0); }
-    } else if (exL) {
-      if (f == 0) hp = eP[bfs - 1];
-      else if (f == 1) hp = rb2(P(0), P(1));
-      else if (f == 2) hp = rb3(P(0), P(1), P(2));
-      else { double s[5] = {P(0), P(1), P(2), P(3), P(4)}; hp = weno5(s, 0, 0); }
-    } else if (c->scheme[d] == S_WENO7JS) {
-      double s[7];
-      for (int k = 0; k < 7; ++k) s[k] = P(f - 4 + k);
-      hp = weno7(s);
-    } else {
-      double s[5];
-      for (int k = 0; k < 5; ++k) s[k] = P(f - 3 + k);
-      int z = c->scheme[d] == S_WENO5Z;
-      hp = weno5(s, z, z && c->compat && f >= ts && f <= L - ts);
+  int compact = sch == S_CRWENO5 || sch == S_HCCS;
+  static double hs[2][4096], ra[4096], rb[4096], rc[4096], rd[4096];
+  for (int side = 0; side < 2; ++side) {
+    const double *e = side ? eN : eP;
+    for (int f = 0; f <= L; ++f)
+      if (!compact || f < ts || f > L - ts) hs[side][f] = face_explicit(c, d, side, f, L, ts, physL, physR, bfs, e);
+    if (!compact) continue;
+    /* tridiagonal system over faces ts .. L-ts (src/crweno5.cpp:82-218) */
+    int m = L - 2 * ts + 1;
+    for (int r = 0; r < m; ++r) {
+      int f = ts + r;
+      if (r == 0 || r == m - 1) {
+        ra[r] = 0.0; rb[r] = 1.0; rc[r] = 0.0;
+        rd[r] = face_explicit(c, d, side, f, L, ts, 0, 0, bfs, e);
+      } else {
+        double s5[5], lo, di, up;
+        for (int k = 0; k < 5; ++k) s5[k] = side ? e[f + 2 - k + bfs] : e[f - 3 + k + bfs];
+        compact_row(sch == S_HCCS, s5, &lo, &di, &up, &rd[r]);
+        rb[r] = di;
+        if (side) { ra[r] = up; rc[r] = lo; } else { ra[r] = lo; rc[r] = up; }
+      }
     }
-    /* ---- F- ---- */
-    if (exR) {
-      int m = L - f;
-      if (m == 0) hn = eN[L + bfs];
-      else if (m == 1) hn = rb2(NN(L - 1), NN(L - 2));
-      else if (m == 2) hn = rb3(NN(L - 1), NN(L - 2), NN(L - 3));
-      else { double s[5] = {NN(L - 1), NN(L - 2), NN(L - 3), NN(L - 4), NN(L - 5)}; hn = weno5(s, 0, 0); }
-    } else if (exL) {
-      if (f == 0) hn = NN(0);
-      else if (f == 1) hn = rb2(NN(1), NN(0));
-      else if (f == 2) hn = rb3(NN(3), NN(2), NN(1));
-      else { double s[5] = {NN(5), NN(4), NN(3), NN(2), NN(1)}; hn = weno5(s, 0, 0); }
-    } else if (c->scheme[d] == S_WENO7JS) {
-      double s[7];
-      for (int k = 0; k < 7; ++k) s[k] = NN(f + 3 - k);
-      hn = weno7(s);
-    } else {
-      double s[5];
-      for (int k = 0; k < 5; ++k) s[k] = NN(f + 2 - k);
-      hn = weno5(s, c->scheme[d] == S_WENO5Z, 0);
+    for (int i = 1; i < m; ++i) {
+      rc[i] = rc[i] / (rb[i] - rc[i - 1] * ra[i]);
+      rd[i] = (rd[i] - rd[i - 1] * ra[i]) / (rb[i] - rc[i - 1] * ra[i]);
     }
-    face[f] = hp + hn;
+    hs[side][ts + m - 1] = rd[m - 1];
+    for (int i = m - 2; i >= 0; --i) hs[side][ts + i] = rd[i] - rc[i] * hs[side][ts + i + 1];
   }
-#undef P
-#undef NN
+  for (int f = 0; f <= L; ++f) face[f] = hs[0][f] + hs[1][f];
 }
 
 /* derivative of an extended line (ghosts at [-bfs, 0) and [L, L+bfs)) at position pos */
@@ -520,7 +600,7 @@ static void pass_inviscid(const oc_config *c, work_t *W, int nb, int bfs, double
 
 static void pass_viscous(const oc_config *c, work_t *W, int nb, int bfs, double *ext) {
   int ts[3];
-  for (int d = 0; d < 3; ++d) ts[d] = (c->scheme[d] == S_WENO7JS) ? 4 : 3;
+  for (int d = 0; d < 3; ++d) ts[d] = (c->scheme[d] == S_WENO7JS || c->scheme[d] == S_HCCS) ? 4 : 3;
   /* gradients of u, v, w, T along xi, eta, zeta (src/NaiverStokes3d.cpp:63-168) */
   for (int bi = 0; bi < nb; ++bi) {
     oc_block *b = W[bi].b;
@@ -609,7 +689,7 @@ static void pass_viscous(const oc_config *c, work_t *W, int nb, int bfs, double 
 static int eval_rhs(const oc_config *c, int nb, oc_block *blocks, work_t *W, double *dt_local) {
   int bfs = 3;
   for (int d = 0; d < 3; ++d)
-    if (c->scheme[d] == S_WENO7JS) bfs = 4;
+    if (c->scheme[d] == S_WENO7JS || c->scheme[d] == S_HCCS) bfs = 4;
   int maxL = 0;
   for (int bi = 0; bi < nb; ++bi)
     for (int d = 0; d < 3; ++d)

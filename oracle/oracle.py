@@ -12,7 +12,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_ref" / "liboracle.so"
-SCHEMES = {"weno5js": 0, "weno5z": 1, "weno7js": 2}
+SCHEMES = {"weno5js": 0, "weno5z": 1, "weno7js": 2, "crweno5": 3, "hccs": 4}
 RIEMANN = {"LF": 0, "AUSM": 1, "AUSMp": 2}
 MODELS = {"Euler3d": 0, "NavierStokes3d": 1}
 

@@ -69,6 +69,23 @@ def case_defs():
              init="channel",
              params=dict(Reynolds=300.0, Mach=0.6, Pt=0.72, Gamma=1.4, T_ref=110.4,
                          T_inf=288.0, T_wall=1.1), nsteps=3),
+        dict(name="crweno5_euler_lf_periodic", model="Euler3d", riemann="LF",
+             schemes=("crweno5",) * 3, shape=(16, 12, 12), lo=(0, 0, 0), hi=(2.0, 1.0, 1.0),
+             wavy=0.2, faces=["periodic"] * 6, init="smooth",
+             params=dict(Reynolds=1000.0, Mach=0.5, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=3),
+        dict(name="hccs_ns_ausm_bc", model="NavierStokes3d", riemann="AUSM",
+             schemes=("hccs",) * 3, shape=(16, 12, 12), lo=(0, 0, 0), hi=(2.0, 1.0, 1.0),
+             wavy=0.15, faces=["inlet", "outlet", "wall", "symm", "periodic", "periodic"],
+             init="channel",
+             params=dict(Reynolds=200.0, Mach=0.5, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.2), nsteps=3),
+        dict(name="mixed_compact_ausmp", model="Euler3d", riemann="AUSMp",
+             schemes=("crweno5", "hccs", "weno5z"), shape=(12, 16, 12), lo=(0, 0, 0),
+             hi=(1.0, 1.5, 1.0), wavy=0.2,
+             faces=["periodic", "periodic", "outlet", "outlet", "symm", "symm"], init="smooth",
+             params=dict(Reynolds=1000.0, Mach=0.8, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=3),
     ]
 
 
