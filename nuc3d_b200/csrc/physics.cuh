@@ -36,9 +36,18 @@ struct CellPrim {
 __device__ __forceinline__ void con2prim(const double q[5], double jac, double gamma, double mach,
                                          CellPrim &s, unsigned &st) {
   double rho = q[0] * jac;
+#if NUC3D_FAST
+  // one reciprocal instead of three divisions; alpha from the same reciprocal below
+  const double rinv = 1.0 / rho;
+  const double fj = rinv * jac;
+  double u = q[1] * fj;
+  double v = q[2] * fj;
+  double w = q[3] * fj;
+#else
   double u = q[1] / rho * jac;
   double v = q[2] / rho * jac;
   double w = q[3] / rho * jac;
+#endif
   double E = q[4] * jac;
   double e0 = E - 0.5 * rho * (u * u + v * v + w * w);
   s.q4 = q[4];
@@ -55,7 +64,11 @@ __device__ __forceinline__ void con2prim(const double q[5], double jac, double g
   s.w = w;
   s.E = E;
   s.p = p;
+#if NUC3D_FAST
+  s.alpha = sqrt(fabs(gamma * p * rinv));
+#else
   s.alpha = sqrt(fabs(gamma * p / rho));
+#endif
 }
 
 // EoSIdealGasgetTemp (src/physicsModel.cpp:1020-1030)
@@ -98,13 +111,24 @@ __device__ __forceinline__ void split_cell(int riemann, const double Q[5], const
   double U0 = (xx * s.u + xy * s.v + xz * s.w);
   double a0 = s.alpha * theta;
   double p = s.p;
+#if NUC3D_FAST
+  // p/J once: every pressure term of the split divides by the same Jacobian
+  const double pj = p / jac;
+#endif
   if (riemann == RIE_LF) {
     double M = fabs(U0) + a0;
     double f0 = U0 * Q[0];
+#if NUC3D_FAST
+    double f1 = U0 * Q[1] + xx * pj;
+    double f2 = U0 * Q[2] + xy * pj;
+    double f3 = U0 * Q[3] + xz * pj;
+    double f4 = U0 * (Q[4] + pj);
+#else
     double f1 = U0 * Q[1] + xx * p / jac;
     double f2 = U0 * Q[2] + xy * p / jac;
     double f3 = U0 * Q[3] + xz * p / jac;
     double f4 = U0 * (Q[4] + p / jac);
+#endif
     fp[0] = 0.5 * (f0 + M * Q[0]);
     fp[1] = 0.5 * (f1 + M * Q[1]);
     fp[2] = 0.5 * (f2 + M * Q[2]);
@@ -120,6 +144,30 @@ __device__ __forceinline__ void split_cell(int riemann, const double Q[5], const
   double m = U0 / a0;
   double mp = mach_l(m), mn = mach_r(m);
   double pp, pn;
+#if NUC3D_FAST
+  // split pressures as fractions of p/J: pp/J = p/J * (pp/p); supersonic (pp/p) is 1 or 0
+  if (riemann == RIE_AUSM) {
+    pp = fabs(m) < 1.0 ? pj * (m + 1.0) * 0.5 : (m > 0.0 ? pj : 0.0);
+    pn = fabs(m) < 1.0 ? -pj * (m - 1.0) * 0.5 : (m < 0.0 ? pj : 0.0);
+  } else {
+    pp = fabs(m) < 1.0 ? pj * (0.25 * sq(m + 1.0) * (2.0 - m) + 0.1875 * m * sq(m * m - 1.0))
+                       : (m > 0.0 ? pj : 0.0);
+    pn = fabs(m) < 1.0 ? pj * (0.25 * sq(m - 1.0) * (2.0 + m) - 0.1875 * m * sq(m * m - 1.0))
+                       : (m < 0.0 ? pj : 0.0);
+  }
+  const double ma = mp * a0, na = mn * a0;
+  fp[0] = ma * Q[0];
+  fp[1] = ma * Q[1] + xx * pp;
+  fp[2] = ma * Q[2] + xy * pp;
+  fp[3] = ma * Q[3] + xz * pp;
+  fp[4] = ma * Q[4] + ma * pj;
+  fn[0] = na * Q[0];
+  fn[1] = na * Q[1] + xx * pn;
+  fn[2] = na * Q[2] + xy * pn;
+  fn[3] = na * Q[3] + xz * pn;
+  fn[4] = na * Q[4] + na * pj;
+  return;
+#endif
   if (riemann == RIE_AUSM) {
     pp = pres_l(m, p);
     pn = pres_r(m, p);
