@@ -193,6 +193,33 @@ __device__ __forceinline__ void bc_ghost_flux(const BlockDev &B, int stage, int 
   split_point(P.riemann, qb, jac, xx, xy, xz, P.gamma, side, out, st);
 }
 
+// Interior reconstructions (no physical face within the scheme's reach): the uniform
+// stencil of the line extended by ghost cells.  compat selects the weno5z stencil of
+// src/weno5z.cpp:80 (interior positive faces only).
+template <int SCH, class Acc>
+__device__ __forceinline__ double recon_pos_in(int f, bool compat, Acc P) {
+  if (SCH == SCH_WENO7JS || SCH == SCH_HCCS) {
+    double s[7] = {P(f - 4), P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), P(f + 2)};
+    return SCH == SCH_HCCS ? weno7z(s) : weno7js(s);
+  } else if (SCH == SCH_WENO5Z) {
+    return weno5z(P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), compat);
+  } else {
+    return weno5js(P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1));
+  }
+}
+
+template <int SCH, class Acc>
+__device__ __forceinline__ double recon_neg_in(int f, Acc Nf) {
+  if (SCH == SCH_WENO7JS || SCH == SCH_HCCS) {
+    double s[7] = {Nf(f + 3), Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), Nf(f - 3)};
+    return SCH == SCH_HCCS ? weno7z(s) : weno7js(s);
+  } else if (SCH == SCH_WENO5Z) {
+    return weno5z(Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), false);
+  } else {
+    return weno5js(Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2));
+  }
+}
+
 // Reconstructed F+ at face f from the split fluxes P(c) of cells c (line coordinates).
 // Faces next to a physical face use ReconstructionboundaryScheme
 // (src/reconstructionBoundaryScheme.cpp:52-313); the right side is tested first
@@ -216,14 +243,7 @@ __device__ __forceinline__ double recon_pos(int f, int L, int ts, bool physL, bo
       default: return weno5js(P(0), P(1), P(2), P(3), P(4));
     }
   }
-  if (SCH == SCH_WENO7JS || SCH == SCH_HCCS) {
-    double s[7] = {P(f - 4), P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), P(f + 2)};
-    return SCH == SCH_HCCS ? weno7z(s) : weno7js(s);
-  } else if (SCH == SCH_WENO5Z) {
-    return weno5z(P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), compat && f >= ts && f <= L - ts);
-  } else {
-    return weno5js(P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1));
-  }
+  return recon_pos_in<SCH>(f, compat && f >= ts && f <= L - ts, P);
 }
 
 template <int SCH, class Acc>
@@ -244,14 +264,7 @@ __device__ __forceinline__ double recon_neg(int f, int L, int ts, bool physL, bo
       default: return weno5js(Nf(5), Nf(4), Nf(3), Nf(2), Nf(1));
     }
   }
-  if (SCH == SCH_WENO7JS || SCH == SCH_HCCS) {
-    double s[7] = {Nf(f + 3), Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), Nf(f - 3)};
-    return SCH == SCH_HCCS ? weno7z(s) : weno7js(s);
-  } else if (SCH == SCH_WENO5Z) {
-    return weno5z(Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), false);
-  } else {
-    return weno5js(Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2));
-  }
+  return recon_neg_in<SCH>(f, Nf);
 }
 
 // d/dxi of a cell-centred field at line position c: boundaryScheme within ts cells
@@ -577,15 +590,29 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     const int fl = e % (TL + 1), w = e / (TL + 1);
     if (w >= T.nw || fl > T.cl) continue;
     const int f = T.c0 + fl;
+    // one test per face: faces within ts of a physical face take the boundary schemes
+    const bool edge = (T.physR && f > T.G.L - T.ts) || (T.physL && f < T.ts);
+    if (!edge) {
+      const bool cz = compat && f >= T.ts && f <= T.G.L - T.ts;
 #pragma unroll 1
-    for (int v = 0; v < 5; ++v) {
-      const double *rowP = sF + (v * TW + w) * SP + (R - T.c0);
-      const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - T.c0);
-      auto Pacc = [rowP](int c) { return rowP[c]; };
-      auto Nacc = [rowN](int c) { return rowN[c]; };
-      double hp = recon_pos<SCH>(f, T.G.L, T.ts, T.physL, T.physR, compat, Pacc);
-      double hn = recon_neg<SCH>(f, T.G.L, T.ts, T.physL, T.physR, Nacc);
-      sH[(v * TW + w) * SH + fl] = hp + hn;
+      for (int v = 0; v < 5; ++v) {
+        const double *rowP = sF + (v * TW + w) * SP + (R + fl);
+        const double *rowN = sF + ((5 + v) * TW + w) * SP + (R + fl);
+        auto Pacc = [rowP](int c) { return rowP[c]; };
+        auto Nacc = [rowN](int c) { return rowN[c]; };
+        sH[(v * TW + w) * SH + fl] = recon_pos_in<SCH>(0, cz, Pacc) + recon_neg_in<SCH>(0, Nacc);
+      }
+    } else {
+#pragma unroll 1
+      for (int v = 0; v < 5; ++v) {
+        const double *rowP = sF + (v * TW + w) * SP + (R - T.c0);
+        const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - T.c0);
+        auto Pacc = [rowP](int c) { return rowP[c]; };
+        auto Nacc = [rowN](int c) { return rowN[c]; };
+        double hp = recon_pos<SCH>(f, T.G.L, T.ts, T.physL, T.physR, compat, Pacc);
+        double hn = recon_neg<SCH>(f, T.G.L, T.ts, T.physL, T.physR, Nacc);
+        sH[(v * TW + w) * SH + fl] = hp + hn;
+      }
     }
   }
   __syncthreads();

@@ -11,6 +11,25 @@ namespace NUC3D_NS {
 
 __device__ __forceinline__ double sq(double x) { return x * x; }
 
+// a / b.  The reference-order build divides with IEEE division.  The throughput build
+// uses a branch-free quotient for finite, normal b: the PTX reciprocal approximation
+// x0 ~ 1/b (relative error e0), one Newton-Raphson step x1 = x0 + x0 (1 - b x0)
+// (error e0^2), q = a x1, then Markstein's residual correction q + (a - b q) x1, whose
+// relative error is of order e0^4 plus the final rounding (P. Markstein, IBM J. Res.
+// Dev. 34(1), 1990).  Zero, infinite or NaN b gives a non-finite result, which the
+// state checks report as they do for IEEE division.
+__device__ __forceinline__ double qdiv(double a, double b) {
+#if NUC3D_FAST
+  double x;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(b));
+  x = fma(x, fma(-b, x, 1.0), x);
+  const double q = a * x;
+  return fma(fma(-b, q, a), x, q);
+#else
+  return a / b;
+#endif
+}
+
 // pow(x, 1.5), correctly rounded in all but astronomically rare cases:
 // s = sqrt(x); the FMA residual r = x - s*s is exact; sqrt(x) ~= s + r/(2s);
 // x*s is split exactly (TwoProduct with FMA) and the small terms are added last.
@@ -38,7 +57,7 @@ __device__ __forceinline__ void con2prim(const double q[5], double jac, double g
   double rho = q[0] * jac;
 #if NUC3D_FAST
   // one reciprocal instead of three divisions; alpha from the same reciprocal below
-  const double rinv = 1.0 / rho;
+  const double rinv = qdiv(1.0, rho);
   const double fj = rinv * jac;
   double u = q[1] * fj;
   double v = q[2] * fj;
@@ -113,7 +132,7 @@ __device__ __forceinline__ void split_cell(int riemann, const double Q[5], const
   double p = s.p;
 #if NUC3D_FAST
   // p/J once: every pressure term of the split divides by the same Jacobian
-  const double pj = p / jac;
+  const double pj = qdiv(p, jac);
 #endif
   if (riemann == RIE_LF) {
     double M = fabs(U0) + a0;
@@ -141,7 +160,7 @@ __device__ __forceinline__ void split_cell(int riemann, const double Q[5], const
     fn[4] = 0.5 * (f4 - M * Q[4]);
     return;
   }
-  double m = U0 / a0;
+  double m = qdiv(U0, a0);
   double mp = mach_l(m), mn = mach_r(m);
   double pp, pn;
 #if NUC3D_FAST

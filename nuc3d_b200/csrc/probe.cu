@@ -1,11 +1,16 @@
-// probe.cu -- FP64 peak of the device, measured with a dependent-FMA microbenchmark.
-//
-// The roofline denominators on this GPU pool cover HBM copy bandwidth and bf16
-// tensor throughput only; the NUC3d path is plain FP64 (no tensor cores), so its
-// compute roof is measured here: every thread runs 8 independent DFMA chains,
-// enough CTAs to fill all SMs several times over, timed with CUDA events.
-// Exported from libnuc3d_probe.so (not part of the solver ABI).
+// probe.cu -- device measurements that are not part of the solver ABI
+// (exported from libnuc3d_probe.so):
+//   nuc3d_probe_fp64_tflops  FP64 peak, measured with a dependent-FMA microbenchmark.
+//     The NUC3d path is plain FP64 (no tensor cores), so its compute roof is measured
+//     here: every thread runs 8 independent DFMA chains, enough CTAs to fill all SMs
+//     several times over, timed with CUDA events.
+//   nuc3d_probe_qdiv         the throughput build's division next to IEEE division on
+//     the same operands, for the accuracy test of the former.
 #include <cuda_runtime.h>
+
+#define NUC3D_NS fast
+#define NUC3D_FAST 1
+#include "physics.cuh"
 
 namespace {
 
@@ -25,9 +30,36 @@ __global__ void __launch_bounds__(256) dfma_loop(double *out, int iters, double 
   if (s == 1234.5678) out[blockIdx.x] = s;  // never true; keeps the chains alive
 }
 
+__global__ void qdiv_pairs(const double *a, const double *b, double *q_fast, double *q_ieee,
+                           long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    q_fast[i] = nuc3d::fast::qdiv(a[i], b[i]);
+    q_ieee[i] = a[i] / b[i];
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+// q_fast[i] = the throughput build's a[i] / b[i], q_ieee[i] = IEEE a[i] / b[i]; host arrays
+// of n doubles.  Returns 0 or a CUDA error code.
+int nuc3d_probe_qdiv(int device, const double *a, const double *b, double *q_fast, double *q_ieee,
+                     long long n) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return (int)e;
+  double *d = nullptr;
+  const size_t bytes = (size_t)n * sizeof(double);
+  if ((e = cudaMalloc(&d, 4 * bytes)) != cudaSuccess) return (int)e;
+  cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice);
+  cudaMemcpy(d + n, b, bytes, cudaMemcpyHostToDevice);
+  qdiv_pairs<<<1184, 256>>>(d, d + n, d + 2 * n, d + 3 * n, n);
+  cudaMemcpy(q_fast, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+  e = cudaMemcpy(q_ieee, d + 3 * n, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return (int)e;
+}
 
 // Returns sustained FP64 TFLOP/s (FMA = 2 flops) over `reps` launches, or a negative
 // CUDA error code.

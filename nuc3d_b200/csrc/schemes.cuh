@@ -56,7 +56,7 @@ __device__ __forceinline__ double weno5js(double f0, double f1, double f2, doubl
   // one division: omega_k = c_k P_k / sum_j c_j P_j with P_k = prod_{j!=k} (ss+is_j)^2
   double b0 = sq(ss + r.is0), b1 = sq(ss + r.is1), b2 = sq(ss + r.is2);
   double a0 = kC5[0] * (b1 * b2), a1 = kC5[1] * (b0 * b2), a2 = kC5[2] * (b0 * b1);
-  return (a0 * r.q0 + a1 * r.q1 + a2 * r.q2) / (a0 + a1 + a2);
+  return qdiv(a0 * r.q0 + a1 * r.q1 + a2 * r.q2, a0 + a1 + a2);
 #else
   double a0 = kC5[0] / sq(ss + r.is0);
   double a1 = kC5[1] / sq(ss + r.is1);
@@ -79,7 +79,7 @@ __device__ __forceinline__ double weno5z(double f0, double f1, double f2, double
   double d0 = sq(r.is0 + ss), d1 = sq(r.is1 + ss), d2 = sq(r.is2 + ss);
   double n0 = kC5[0] * (d0 + t2), n1 = kC5[1] * (d1 + t2), n2 = kC5[2] * (d2 + t2);
   double a0 = n0 * (d1 * d2), a1 = n1 * (d0 * d2), a2 = n2 * (d0 * d1);
-  return (a0 * r.q0 + a1 * r.q1 + a2 * r.q2) / (a0 + a1 + a2);
+  return qdiv(a0 * r.q0 + a1 * r.q1 + a2 * r.q2, a0 + a1 + a2);
 #else
   double a0 = kC5[0] * (1.0 + sq(tau / (r.is0 + ss)));
   double a1 = kC5[1] * (1.0 + sq(tau / (r.is1 + ss)));
@@ -114,7 +114,7 @@ __device__ __forceinline__ double weno7js(const double f[7]) {
   double b01 = b0 * b1, b23 = b2 * b3;
   double a0 = kC7[0] * (b1 * b23), a1 = kC7[1] * (b0 * b23), a2 = kC7[2] * (b01 * b3),
          a3 = kC7[3] * (b01 * b2);
-  return (a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3) / (a0 + a1 + a2 + a3);
+  return qdiv(a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3, a0 + a1 + a2 + a3);
 #else
   double a0 = kC7[0] / sq(ss + is0);
   double a1 = kC7[1] / sq(ss + is1);

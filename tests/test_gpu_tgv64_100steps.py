@@ -3,9 +3,17 @@ CFL 0.5, Re 1600, Ma 0.1) against the reference itself.
 
 The reference runs here as 8 MPI ranks (2x2x2 blocks of 32^3, the project's shared-memory
 MPI shim); its multi-rank result equals its single-block result bit for bit for explicit
-WENO schemes.  The GPU runs the single 64^3 block.  Criteria: reference-order build bitwise
-equal; throughput build within 1e-10 relative max-norm; conserved totals of the periodic
-box unchanged to round-off.
+WENO schemes.  The GPU runs the single 64^3 block.  Criterion for the reference-order build:
+bitwise equal.
+
+The throughput build cannot be held to a fixed tolerance at CFL 0.5: this discretisation
+amplifies the (pi, pi, pi) checkerboard mode of the grid by about 4.6x per step, so a
+1e-15 relative perturbation of the initial state alone, stepped in the reference's own
+arithmetic, ends 100 steps at a few 1e-2 relative difference (the mode saturates).  Its
+criteria are therefore (a) no further from the reference than that perturbed reference-order
+run, (b) conserved totals of the periodic box unchanged to round-off, and (c) at CFL 0.2,
+where the mode is damped and perturbations stay at round-off, within 1e-12 of the
+reference-order build after the same 100 steps.
 """
 import math
 
@@ -53,13 +61,15 @@ def _reference():
 
 @pytest.fixture(scope="module")
 def reference():
+    if not (R.REF_BIN_DIR / "nuc3d_ref_taps").exists():
+        pytest.skip("reference binaries not built (make -C oracle ref)")
     return _reference()
 
 
-def _gpu(nodes, q0, exact):
+def _gpu(nodes, q0, exact, cfl=0.5):
     import nuc3d_b200 as nb
     cfg = nb.Config(scheme_ivs=("weno5js",) * 3, riemann="LF", model="NavierStokes3d",
-                    reynolds=1600.0, mach=0.1, prandtl=0.72, exact=exact)
+                    reynolds=1600.0, mach=0.1, prandtl=0.72, exact=exact, cfl=cfl)
     s = nb.Solver(cfg)
     b = s.add_block(N, N, N, [0] * 6, [1, 0, 3, 2, 5, 4])
     s.set_mesh(b, *nodes)
@@ -79,15 +89,34 @@ def test_tgv64_100_steps_bitwise(reference):
     assert np.array_equal(q, qref), float(np.max(np.abs(q - qref)) / np.max(np.abs(qref)))
 
 
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
 @pytest.mark.gpu
 @pytest.mark.slow
-def test_tgv64_100_steps_fast_within_1e10(reference):
+def test_tgv64_100_steps_fast_within_input_sensitivity(reference):
     nodes, q0, qref, dts, times = reference
     q, t, dt = _gpu(nodes, q0, exact=False)
-    rel = float(np.max(np.abs(q - qref)) / np.max(np.abs(qref)))
-    assert rel <= 1e-10, rel
+    rng = np.random.default_rng(20261203)
+    q0p = q0 * (1.0 + 1e-15 * rng.standard_normal(q0.shape))
+    qp, _, _ = _gpu(nodes, q0p, exact=True)
+    rel_fast, rel_pert = _rel(q, qref), _rel(qp, qref)
+    assert rel_pert > 1e-6, rel_pert          # the checkerboard mode did grow
+    assert rel_fast <= 4.0 * rel_pert, (rel_fast, rel_pert)
+    assert abs(t - times[-1]) <= 1e-6 * times[-1], (t, times[-1])
     # conserved totals of the periodic box (mass, momentum, energy)
     for v in range(5):
         s0, s1 = q0[v].sum(), q[v].sum()
         scale = np.abs(q0[v]).sum()
         assert abs(s1 - s0) <= 1e-12 * scale, (v, s0, s1)
+
+
+@pytest.mark.gpu
+@pytest.mark.slow
+def test_tgv64_100_steps_fast_stable_cfl(reference):
+    nodes, q0, _, _, _ = reference
+    qe, te, _ = _gpu(nodes, q0, exact=True, cfl=0.2)
+    qf, tf, _ = _gpu(nodes, q0, exact=False, cfl=0.2)
+    assert _rel(qf, qe) <= 1e-12, _rel(qf, qe)
+    assert abs(tf - te) <= 1e-13 * te
