@@ -56,7 +56,24 @@ struct BlockDev {
   double *fh;            // compact schemes: face fluxes [sys][line][face] of one direction
   double *rows;          // compact schemes: tridiagonal rows [row][4][sys*lines + line]
   FaceDev face[6];
+  // Per direction d, ceil(2^40 / k) for k = tile chunks per line and k = line groups:
+  // the sweep kernels divide tile indices by multiply-and-shift (set_tile_divisors).
+  unsigned long long tdiv[3][2];
 };
+
+// Sweep tiles: kTileW lines x kTileL cells along one direction.
+constexpr int kTileW = 4, kTileL = 64;
+
+// Fills BlockDev::tdiv from n[].  q = (x * tdiv) >> 40 equals x / k exactly for
+// x < 2^24 (the tile count of a block of fewer than 2^32 cells) and k < 2^16.
+inline void set_tile_divisors(BlockDev &b) {
+  for (int d = 0; d < 3; ++d) {
+    const unsigned long long L = (unsigned long long)b.n[d];
+    const unsigned long long nW = (unsigned long long)(d == 0 ? b.n[1] : b.n[0]);
+    const unsigned long long k[2] = {(L + kTileL - 1) / kTileL, (nW + kTileW - 1) / kTileW};
+    for (int j = 0; j < 2; ++j) b.tdiv[d][j] = ((1ull << 40) + k[j] - 1) / k[j];
+  }
+}
 
 // Physical faces of all blocks, laid end to end for the BC ghost pass.
 constexpr int kMaxFaceJobs = 6 * 512;

@@ -32,7 +32,7 @@ namespace NUC3D_NS {
 #ifndef NUC3D_SWEEP_MINB
 #define NUC3D_SWEEP_MINB 4  // resident sweep CTAs per SM the register budget is cut for (measured best)
 #endif
-constexpr int kTW = 4, kTL = 64;
+constexpr int kTW = kTileW, kTL = kTileL;
 constexpr int kThreads = kTW * kTL + 32;
 template <int DIR> struct Tile { static constexpr int TW = kTW, TL = kTL; };
 
@@ -324,13 +324,15 @@ __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ bloc
   T.B = &blocks[T.b];
   for (int d = 0; d < 3; ++d) T.n[d] = T.B->n[d];
   T.G = make_geo(DIR, T.n);
-  int lt = T.t - tm.tile_start[T.b];
-  const int nch = (T.G.L + TL - 1) / TL;
-  const int nwg = (T.G.nW + TW - 1) / TW;
-  const int ch = lt % nch;
-  lt /= nch;
-  const int wg = lt % nwg;
-  T.o = lt / nwg;
+  // tile = (chunk along the line) + nch * ((line group) + nwg * (outer index))
+  const unsigned lt = (unsigned)(T.t - tm.tile_start[T.b]);
+  const unsigned nch = (unsigned)(T.G.L + TL - 1) / TL;
+  const unsigned nwg = (unsigned)(T.G.nW + TW - 1) / TW;
+  const unsigned q1 = (unsigned)((lt * T.B->tdiv[DIR][0]) >> 40);
+  const unsigned q2 = (unsigned)((q1 * T.B->tdiv[DIR][1]) >> 40);
+  const int ch = (int)(lt - q1 * nch);
+  const int wg = (int)(q1 - q2 * nwg);
+  T.o = (int)q2;
   T.c0 = ch * TL;
   T.cl = min(TL, T.G.L - T.c0);
   T.w0 = wg * TW;
@@ -369,12 +371,20 @@ __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks,
     if (w < T.nw && p < T.cl + 2 * R) {
       const int wl = T.w0 + w;
       const int sa = (DIR == 1) ? T.o : wl, sb = (DIR == 1) ? wl : T.o;
-      double q[5];
-      CellPrim s;
-      if (g >= 0 && g < G.L) {
-        const long long idx = g * G.sL + wl * G.sW + T.o * G.sO;
-        cell_split(B, stage, idx, DIR, P, fp, fn, s, q, st);
-        if (eig && g >= T.c0 && g < T.c0 + T.cl) {
+      // the cell at line position g: this block's, or the neighbour's across the face;
+      // one split call serves both, so a neighbour halo adds no divergent copy of it
+      const bool own = g >= 0 && g < G.L;
+      const BlockDev *CB = &B;
+      long long idx = g * G.sL + wl * G.sW + T.o * G.sO;
+      if (!own) {
+        const int nb = ghost_cell(blocks, B, DIR, g, sa, sb, P.bfs, idx);
+        CB = nb >= 0 ? &blocks[nb] : nullptr;
+      }
+      if (CB) {
+        double q[5];
+        CellPrim s;
+        cell_split(*CB, stage, idx, DIR, P, fp, fn, s, q, st);
+        if (own && eig && g >= T.c0 && g < T.c0 + T.cl) {
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
             const double *m = B.met[d];
@@ -382,16 +392,12 @@ __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks,
             emax = ev > emax ? ev : emax;
           }
         }
-        if (DIR == 2 && sQ && g >= T.c0 && g < T.c0 + T.cl) {
+        if (DIR == 2 && sQ && own && g >= T.c0 && g < T.c0 + T.cl) {
 #pragma unroll
           for (int v = 0; v < 5; ++v) sQ[(v * TW + w) * SQ + (g - T.c0)] = q[v];
         }
       } else {
-        long long nidx;
-        const int nb = ghost_cell(blocks, B, DIR, g, sa, sb, P.bfs, nidx);
-        if (nb >= 0) {
-          cell_split(blocks[nb], stage, nidx, DIR, P, fp, fn, s, q, st);
-        } else if (g == -1 || g == G.L) {
+        if (g == -1 || g == G.L) {
           // ghost next to a physical face, filled by bc_ghost_kernel this stage
           const int f = 2 * DIR + (g < 0 ? 0 : 1);
           const int A = DIR == 0 ? T.n[1] : (DIR == 1 ? T.n[2] : T.n[0]);
@@ -585,13 +591,38 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   __syncthreads();
 
   // ---- faces c0 .. c0+cl: the ten reconstructions of each face ----
+  // Faces within ts of a physical face take the boundary schemes: at most ts faces per
+  // line end.  Items are ordered interior faces of all lines first, then, from the next
+  // warp boundary on, the edge faces, so that one warp at most diverges into them.
   const bool compat = P.weno5z_compat != 0;
-  for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
-    const int fl = e % (TL + 1), w = e / (TL + 1);
-    if (w >= T.nw || fl > T.cl) continue;
+  const int nf = T.cl + 1;
+  const int lo = T.physL ? min(max(T.ts - T.c0, 0), nf) : 0;                // edge: fl < lo
+  const int hi = T.physR ? min(max(T.G.L - T.ts + 1 - T.c0, 0), nf) : nf;   // edge: fl >= hi
+  const int ni = hi > lo ? hi - lo : 0;       // interior faces per line
+  const int nl = ni > 0 ? lo : nf;            // left edge faces (all faces when ni == 0)
+  const int ne = nf - ni;                     // edge faces per line
+  const int ei = TW * ni, e0 = (ei + 31) & ~31;
+  const float rni = ni > 0 ? 1.0f / (float)ni : 0.0f, rne = ne > 0 ? 1.0f / (float)ne : 0.0f;
+  for (int e = threadIdx.x; e < e0 + TW * ne; e += kThreads) {
+    // w = e / ni by a float reciprocal: exact, since (e + 1/2) / ni stays at least
+    // 1/(2 ni) away from an integer and e < 2^9.
+    int w, fl;
+    bool edge;
+    if (e < ei) {
+      w = __float2int_rz(((float)e + 0.5f) * rni);
+      fl = lo + (e - w * ni);
+      edge = false;
+    } else if (e >= e0) {
+      const int j = e - e0;
+      w = __float2int_rz(((float)j + 0.5f) * rne);
+      const int k = j - w * ne;
+      fl = k < nl ? k : hi + (k - nl);
+      edge = true;
+    } else {
+      continue;
+    }
+    if (w >= T.nw) continue;
     const int f = T.c0 + fl;
-    // one test per face: faces within ts of a physical face take the boundary schemes
-    const bool edge = (T.physR && f > T.G.L - T.ts) || (T.physL && f < T.ts);
     if (!edge) {
       const bool cz = compat && f >= T.ts && f <= T.G.L - T.ts;
 #pragma unroll 1

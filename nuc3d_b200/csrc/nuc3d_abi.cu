@@ -337,6 +337,7 @@ int nuc3d_finalize(nuc3d_ctx *c) {
       d.face[f].id = b.bc_id[f];
       for (int v = 0; v < 5; ++v) d.face[f].bcv[v] = b.bcv[f][v];
     }
+    set_tile_divisors(d);
   }
   cudaSetDevice(c->device);
   CUDA_TRY(cudaMalloc(&c->d_blocks, nbk * sizeof(BlockDev)));

@@ -163,6 +163,7 @@ int nuc3d_rhs_noalloc(const nuc3d_config *cfg, int device, int nx, int ny, int n
     B.face[f].id = bc_id[f];
     for (int v = 0; v < 5; ++v) B.face[f].bcv[v] = bc_values ? bc_values[f * 5 + v] : 0.0;
   }
+  set_tile_divisors(B);
   static thread_local FaceJobs J;  // host staging only
   std::memset(&J, 0, sizeof(J));
   for (int f = 0; f < 6; ++f) {
