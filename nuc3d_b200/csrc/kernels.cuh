@@ -267,6 +267,49 @@ __device__ __forceinline__ double recon_neg(int f, int L, int ts, bool physL, bo
   return recon_neg_in<SCH>(f, Nf);
 }
 
+// F+ + F- of a face within ts of a physical face (recon_pos + recon_neg of such a face),
+// without branching on the face: the boundary stencils sit at fixed offsets from the
+// line end, so every candidate of the reference's switch is evaluated with its own
+// expression on values loaded at those offsets and the one for distance k = face to
+// physical face is selected.  Lanes of one warp holding different k then run one path.
+// The right end is tested first, as the reference applies BR after BL.  Positions are
+// clamped to the tile's shared-memory row [first, last] (a one-cell tile at the right end
+// holds fewer cells than the stencils reach; values read there belong only to candidates
+// that k does not select), so every load stays inside the row whichever end it serves.
+template <int SCH, class AccP, class AccN>
+__device__ __forceinline__ double edge_face(int f, int L, int ts, bool physR, int first, int last,
+                                            AccP P, AccN Nf) {
+  constexpr int NJ = (SCH == SCH_WENO7JS || SCH == SCH_HCCS) ? 6 : 4;
+  const bool right = physR && f > L - ts;
+  const int k = right ? L - f : f;
+  auto at = [first, last](int c) { return min(max(c, first), last); };
+  // a[j]: F+ at cells L-1-j (right) or j-1 (left); b[j]: F- at cells L-j (right) or j (left)
+  double a[NJ], b[NJ];
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    a[j] = P(at(right ? L - 1 - j : j - 1));
+    b[j] = Nf(at(right ? L - j : j));
+  }
+  // recon_pos cases: P(L-1) | rb_second(P(L-2),P(L-1)) | rb_third(P(L-4),P(L-3),P(L-2)) |
+  // weno5js(P(L-6..L-2)) on the right; P(-1) | rb_second(P(0),P(1)) | rb_third(P(0),P(1),P(2)) |
+  // weno5js(P(0..4)) on the left
+  const double hp1 = right ? rb_second(a[1], a[0]) : rb_second(a[1], a[2]);
+  const double hp2 = right ? rb_third(a[3], a[2], a[1]) : rb_third(a[1], a[2], a[3]);
+  // recon_neg cases: Nf(L) | rb_second(Nf(L-1),Nf(L-2)) | rb_third(Nf(L-1),Nf(L-2),Nf(L-3)) |
+  // weno5js(Nf(L-1..L-5)) on the right; Nf(0) | rb_second(Nf(1),Nf(0)) |
+  // rb_third(Nf(3),Nf(2),Nf(1)) | weno5js(Nf(5..1)) on the left
+  const double hn1 = rb_second(b[1], right ? b[2] : b[0]);
+  const double hn2 = right ? rb_third(b[1], b[2], b[3]) : rb_third(b[3], b[2], b[1]);
+  double hp = k == 0 ? a[0] : (k == 1 ? hp1 : hp2);
+  double hn = k == 0 ? b[0] : (k == 1 ? hn1 : hn2);
+  if (NJ == 6 && k == 3) {
+    const int i1 = 1, i5 = NJ - 1;
+    hp = right ? weno5js(a[i5], a[4], a[3], a[2], a[i1]) : weno5js(a[i1], a[2], a[3], a[4], a[i5]);
+    hn = right ? weno5js(b[i1], b[2], b[3], b[4], b[i5]) : weno5js(b[i5], b[4], b[3], b[2], b[i1]);
+  }
+  return hp + hn;
+}
+
 // d/dxi of a cell-centred field at line position c: boundaryScheme within ts cells
 // of a physical face (src/fieldOperator.cpp:523-624, src/boundaryScheme.cpp:311-406),
 // cd6 elsewhere (ghost values come from the neighbour across the face).
@@ -573,7 +616,7 @@ __global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
 sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
              int stage, int flags) {
   using M = TileSmem<DIR, SCH>;
-  constexpr int R = M::R, TW = M::TW, TL = M::TL, SP = M::SP, SV = M::SV, SH = M::SH;
+  constexpr int R = M::R, TW = M::TW, SP = M::SP, SV = M::SV, SH = M::SH;
   extern __shared__ double smem[];
   double *sF = smem;                        // [10][TW][SP]: F+ vars 0..4, F- vars 5..9
   double *sH = sF + 10 * TW * SP;           // [5][TW][SH]: face fluxes
@@ -640,9 +683,16 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
         const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - T.c0);
         auto Pacc = [rowP](int c) { return rowP[c]; };
         auto Nacc = [rowN](int c) { return rowN[c]; };
-        double hp = recon_pos<SCH>(f, T.G.L, T.ts, T.physL, T.physR, compat, Pacc);
-        double hn = recon_neg<SCH>(f, T.G.L, T.ts, T.physL, T.physR, Nacc);
+#if NUC3D_FAST
+        sH[(v * TW + w) * SH + fl] =
+            edge_face<SCH>(f, T.G.L, T.ts, T.physR, T.c0 - R, T.c0 - R + M::NP - 1, Pacc, Nacc);
+#else
+        // reference-order build: the reference's switch (IEEE divisions make evaluating
+        // every candidate dearer than the divergence)
+        const double hp = recon_pos<SCH>(f, T.G.L, T.ts, T.physL, T.physR, compat, Pacc);
+        const double hn = recon_neg<SCH>(f, T.G.L, T.ts, T.physL, T.physR, Nacc);
         sH[(v * TW + w) * SH + fl] = hp + hn;
+#endif
       }
     }
   }

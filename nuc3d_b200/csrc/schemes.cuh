@@ -207,6 +207,11 @@ __device__ __forceinline__ double rb_third(double f0, double f1, double f2) {
   double is1 = sq(f1 - f2);
   double q20 = -0.5 * f0 + 1.5 * f1;
   double q21 = 0.5 * f1 + 0.5 * f2;
+#if NUC3D_FAST
+  // one division: w0 : w1 = (1/3)/e0^2 : (2/3)/e1^2 = e1^2 : 2 e0^2, e_k = 1e-6 + is_k
+  const double b0 = sq(1.0e-6 + is0), b1 = sq(1.0e-6 + is1);
+  return qdiv(b1 * q20 + 2.0 * b0 * q21, b1 + 2.0 * b0);
+#endif
   double aa0 = 1.0 / 3.0 / sq(1.0e-6 + is0);
   double aa1 = 2.0 / 3.0 / sq(1.0e-6 + is1);
   double w0 = aa0 / (aa0 + aa1);
