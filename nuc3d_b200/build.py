@@ -73,9 +73,9 @@ def build(verbose: bool = False, force: bool = False, defines=(), out: Path | No
                                                  stderr=subprocess.STDOUT, text=True)))
     failed = []
     for unit, p in procs:
-        out, _ = p.communicate()
-        if out and (verbose or p.returncode):
-            print(out, end="", flush=True)
+        log, _ = p.communicate()
+        if log and (verbose or p.returncode):
+            print(log, end="", flush=True)
         if p.returncode:
             failed.append(unit)
     if failed:
