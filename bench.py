@@ -55,19 +55,23 @@ FLOPS = {
     "rhs_add": 1,          # per cell and variable: src/euler3d.cpp:405,419
     "rk": 14.0 / 3.0,      # per cell and variable, mean of stages 4,5,5: src/TVD-RK3.cpp:57-136
 }
-# HBM bytes a sweep cannot avoid per cell: Q (40) + jac (8) + its direction's metric (24),
-# plus RHS write (xi), RHS read+write (eta), RHS read + Q_n read (stages 1,2) + Q write (zeta).
-SWEEP_BYTES = {0: 72 + 40, 1: 72 + 80, 2: 72 + 40 + 40 * 2.0 / 3.0 + 40}
+# HBM bytes a right-hand-side sweep (the launch profile_sweep times) cannot avoid per
+# cell: Q (40) + jac (8) + its direction's metric (24), plus the RHS write (xi) or the
+# RHS read and write (eta, zeta).
+SWEEP_BYTES = {0: 72 + 40, 1: 72 + 80, 2: 72 + 80}
+# DRAM bytes per cell the same launches moved under ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of a 192^3 block, whose every array is larger than L2, divided by
+# its cells; a launch's traffic grows with its cells): profiles/sweep_kernel_sphere_fast.md.
+SWEEP_TRAFFIC = {0: None, 1: None, 2: None}
 
 
 def sweep_flops_per_cell(d: int, scheme: str = "weno5z", riemann: str = "AUSM") -> float:
+    """Algorithmic flops per cell of one right-hand-side sweep along d (no RK update)."""
     f = FLOPS[riemann] + 10 * FLOPS[scheme] + 5 * FLOPS["combine"] + 5 * FLOPS["difference"]
     if d == 0:
         f += FLOPS["con2prim"]
     else:
         f += 5 * FLOPS["rhs_add"]
-    if d == 2:
-        f += 5 * FLOPS["rk"]
     return f
 
 
@@ -357,14 +361,15 @@ def ours(args):
         "e2e": {"value": e2e_value, "unit": "Mcell-RK3-steps/s",
                 "h2d_bytes_per_step": 5 * cells * 8, "d2h_bytes_per_step": 5 * cells * 8,
                 "steps": e2e_steps},
-        "gpu_launches": 9 * args.steps,
+        "gpu_launches": s.kernels_per_step() * args.steps,
         "roofline": {
             "bound": "fp64", "kernel": f"sweep_kernel<{dom}> ({'xi eta zeta'.split()[dom]})",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured live: libnuc3d_probe DFMA microbenchmark",
             "flops_per_cell": sweep_flops_per_cell(dom), "ms_per_launch": per[dom],
             "ms_per_launch_all": per,
-            "traffic": None,
+            "traffic": (SWEEP_TRAFFIC[dom] * cells if SWEEP_TRAFFIC[dom] else None),
+            "traffic_unit": "bytes per launch",
             "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
                     "frac": hbm_achieved / hbm_peak, "peak_source": hbm_src,
                     "bytes_per_cell": SWEEP_BYTES[dom]},

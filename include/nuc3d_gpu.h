@@ -130,6 +130,12 @@ int nuc3d_use_graph(nuc3d_ctx *ctx, int on);
    return the mean device time per launch in milliseconds (CUDA events). */
 int nuc3d_profile_sweep(nuc3d_ctx *ctx, int dir, int reps, double *ms_per_launch);
 
+/* Kernels one nuc3d_step(ctx, 1) launches (after nuc3d_finalize): per RK stage the BC
+   ghost pass (when a block has a physical face), the NS primitive and gradient passes,
+   and one sweep per direction (three kernels for a compact-scheme direction).  No
+   counterpart in the reference. */
+int nuc3d_kernels_per_step(nuc3d_ctx *ctx, int *kernels);
+
 /* Debug taps: NS primitives (u, v, w, T: 4N) and contravariant viscous fluxes
    ([dir][var 1..4]: 12N) of the last evaluation. */
 int nuc3d_block_get_prim(nuc3d_ctx *ctx, int block, double *prim);

@@ -36,7 +36,7 @@ EXPORTED = (
     "nuc3d_block_q_device", "nuc3d_rhs", "nuc3d_block_get_rhs", "nuc3d_step", "nuc3d_sync",
     "nuc3d_get_time", "nuc3d_set_time", "nuc3d_get_status", "nuc3d_set_stream",
     "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis", "nuc3d_profile_sweep",
-    "nuc3d_rhs_noalloc",
+    "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step",
 )
 
 
@@ -109,6 +109,7 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_block_get_vis.argtypes = [P, I, PD]
     lib.nuc3d_profile_sweep.argtypes = [P, I, I, PD]
     PI = ctypes.POINTER(I)
+    lib.nuc3d_kernels_per_step.argtypes = [P, PI]
     lib.nuc3d_rhs_noalloc.argtypes = [ctypes.POINTER(_Cfg), I, I, I, I, PI, PI, PD, P, P, P, P,
                                       P, P, P, PD, P]
     for name in EXPORTED:
@@ -295,6 +296,12 @@ class Solver:
         ms = ctypes.c_double()
         _check(self.lib.nuc3d_profile_sweep(self._ctx, direction, reps, ctypes.byref(ms)))
         return ms.value
+
+    def kernels_per_step(self) -> int:
+        """Kernels one step launches (the library's own count of its launches)."""
+        n = ctypes.c_int()
+        _check(self.lib.nuc3d_kernels_per_step(self._ctx, ctypes.byref(n)))
+        return n.value
 
     def use_graph(self, on: bool) -> None:
         _check(self.lib.nuc3d_use_graph(self._ctx, int(bool(on))))

@@ -560,6 +560,17 @@ int nuc3d_profile_sweep(nuc3d_ctx *c, int dir, int reps, double *ms) {
   return check_status(c);
 }
 
+int nuc3d_kernels_per_step(nuc3d_ctx *c, int *kernels) {
+  if (!c || !kernels) return fail(NUC3D_EINVAL, "bad argument");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  const Launch &L = c->L;
+  int per_stage = (L.bc_tiles > 0 ? 1 : 0) + (L.P.model == MODEL_NS ? 2 : 0);
+  for (int d = 0; d < 3; ++d)
+    per_stage += (L.P.scheme[d] == SCH_CRWENO5 || L.P.scheme[d] == SCH_HCCS) ? 3 : 1;
+  *kernels = 3 * per_stage;
+  return NUC3D_OK;
+}
+
 int nuc3d_use_graph(nuc3d_ctx *c, int on) {
   if (!c) return fail(NUC3D_EINVAL, "null context");
   c->use_graph = on != 0;

@@ -1,9 +1,13 @@
 """Run the benchmark workload at a chosen size, without timing: the target of ncu captures.
 
     python -m nuc3d_b200.profile_case --shape 128 --steps 1 [--exact] [--ns]
+    python -m nuc3d_b200.profile_case --shape 128 --sweeps 2
 
 Euler: spherical Riemann, WENO5-Z + AUSM, outlet faces (bench.py's workload).
 --ns: Navier-Stokes Taylor-Green, WENO5-JS + LF, periodic (the small-config numerics).
+--sweeps R: instead of stepping, launch each direction's right-hand-side sweep 1 + R
+times (xi, then eta, then zeta: the launches bench.py times for its roofline) and
+print the mean milliseconds per launch.
 """
 from __future__ import annotations
 
@@ -19,6 +23,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--exact", action="store_true")
     ap.add_argument("--ns", action="store_true")
+    ap.add_argument("--sweeps", type=int, default=0)
     a = ap.parse_args()
     shape = (a.shape,) * 3
     if a.ns:
@@ -28,7 +33,7 @@ def main():
         faces = C.periodic_faces()
     else:
         cfg = nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="Euler3d", mach=1.0,
-                        exact=a.exact)
+                        exact=a.exact, weno5z_compat=True)
         q, m = C.spherical_riemann(shape)
         faces = C.outlet_faces()
     s = nb.Solver(cfg)
@@ -36,6 +41,10 @@ def main():
     s.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
     s.finalize()
     s.set_q(b, q)
+    if a.sweeps > 0:
+        print([s.profile_sweep(d, a.sweeps) for d in range(3)])
+        s.close()
+        return
     s.step(a.steps)
     t, dt = s.time_dt()
     print(f"{shape} steps={a.steps} time={t:.6g} dt={dt:.6g} status={s.status()}")

@@ -95,3 +95,15 @@ def test_two_blocks_equal_one(name):
     s.step(int(g.cfg["nsteps"]))
     q = np.concatenate([s.get_q(b0), s.get_q(b1)], axis=3)
     assert np.array_equal(q, g.qn), f"rel {rel_max(q, g.qn):.3g}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,expected", [
+    ("sphere_euler_weno5z_ausm_outlet", 3 * (1 + 3)),      # BC pass + 3 sweeps
+    ("tgv_ns_weno5js_lf", 3 * (2 + 3)),                    # periodic: NS passes + 3 sweeps
+    ("hccs_ns_ausm_bc", 3 * (1 + 2 + 3 * 3)),              # compact: 3 kernels per direction
+    ("mixed_compact_ausmp", 3 * (1 + 3 + 3 + 1)),          # crweno5, hccs, weno5z
+])
+def test_kernels_per_step(name, expected):
+    g = G.load(name)
+    assert G.solver(g, exact=False).kernels_per_step() == expected
