@@ -62,7 +62,7 @@ SWEEP_BYTES = {0: 72 + 40, 1: 72 + 80, 2: 72 + 80}
 # DRAM bytes per cell the same launches moved under ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of a 192^3 block, whose every array is larger than L2, divided by
 # its cells; a launch's traffic grows with its cells): profiles/sweep_kernel_sphere_fast.md.
-SWEEP_TRAFFIC = {0: None, 1: None, 2: None}
+SWEEP_TRAFFIC = {0: 108.1, 1: 152.1, 2: 150.8}
 
 
 def sweep_flops_per_cell(d: int, scheme: str = "weno5z", riemann: str = "AUSM") -> float:
@@ -92,7 +92,7 @@ class ClockSampler:
         try:
             self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
