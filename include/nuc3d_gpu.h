@@ -130,6 +130,20 @@ int nuc3d_use_graph(nuc3d_ctx *ctx, int on);
    return the mean device time per launch in milliseconds (CUDA events). */
 int nuc3d_profile_sweep(nuc3d_ctx *ctx, int dir, int reps, double *ms_per_launch);
 
+/* Flow diagnostics of the current state of every block: postproc::solveQ after
+   block::Post (src/postproc.cpp:743-848, src/block.cpp:601-618), which the reference runs
+   every postStep steps when PostProc.in has SimutaneousData 1 and appends to
+   enstrophy.dat.  Velocity gradients by the block's difference operator, vorticity w,
+   Q criterion; *enstrophy = sum over cells of 0.5|w|^2, *kinetic = sum of 0.5 rho |u|^2
+   (per block in cell order, then over the blocks in order, as the reference's
+   MPI_Allreduce).  The reference-order build reproduces the reference's totals bit for
+   bit; the throughput build sums in a different, fixed order.  The first call allocates
+   88 bytes per cell of workspace. */
+int nuc3d_diagnostics(nuc3d_ctx *ctx, double *enstrophy, double *kinetic);
+/* Fields of the last nuc3d_diagnostics call for one block: 5N doubles, w_x, w_y, w_z,
+   0.5|w|^2, Q (TemporalQField[9..13] of the reference). */
+int nuc3d_block_get_diag(nuc3d_ctx *ctx, int block, double *fields);
+
 /* Kernels one nuc3d_step(ctx, 1) launches (after nuc3d_finalize): per RK stage the BC
    ghost pass (when a block has a physical face), the NS primitive and gradient passes,
    and one sweep per direction (three kernels for a compact-scheme direction).  No

@@ -36,7 +36,7 @@ EXPORTED = (
     "nuc3d_block_q_device", "nuc3d_rhs", "nuc3d_block_get_rhs", "nuc3d_step", "nuc3d_sync",
     "nuc3d_get_time", "nuc3d_set_time", "nuc3d_get_status", "nuc3d_set_stream",
     "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis", "nuc3d_profile_sweep",
-    "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step",
+    "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step", "nuc3d_diagnostics", "nuc3d_block_get_diag",
 )
 
 
@@ -110,6 +110,8 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_profile_sweep.argtypes = [P, I, I, PD]
     PI = ctypes.POINTER(I)
     lib.nuc3d_kernels_per_step.argtypes = [P, PI]
+    lib.nuc3d_diagnostics.argtypes = [P, PD, PD]
+    lib.nuc3d_block_get_diag.argtypes = [P, I, PD]
     lib.nuc3d_rhs_noalloc.argtypes = [ctypes.POINTER(_Cfg), I, I, I, I, PI, PI, PD, P, P, P, P,
                                       P, P, P, PD, P]
     for name in EXPORTED:
@@ -296,6 +298,19 @@ class Solver:
         ms = ctypes.c_double()
         _check(self.lib.nuc3d_profile_sweep(self._ctx, direction, reps, ctypes.byref(ms)))
         return ms.value
+
+    def diagnostics(self) -> tuple[float, float]:
+        """(enstrophy, kinetic energy) totals of the current state (postproc::solveQ)."""
+        e, k = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.nuc3d_diagnostics(self._ctx, ctypes.byref(e), ctypes.byref(k)))
+        return e.value, k.value
+
+    def get_diag(self, block: int):
+        """Fields of the last diagnostics call, shape (5, nz, ny, nx): vorticity x, y, z,
+        enstrophy density 0.5|w|^2, Q criterion."""
+        out = np.empty(self._shape5(block), dtype=np.float64)
+        _check(self.lib.nuc3d_block_get_diag(self._ctx, block, _pd(out)))
+        return out
 
     def kernels_per_step(self) -> int:
         """Kernels one step launches (the library's own count of its launches)."""

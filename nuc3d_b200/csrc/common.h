@@ -123,6 +123,15 @@ struct Launch {
   cudaStream_t stream;
 };
 
+// Diagnostics workspace of one block (postproc::solveQ, src/postproc.cpp:743-848):
+// prim 4N (rho, u, v, w), fields 5N (vorticity x, y, z, 0.5|w|^2, Q), dens 2N (the
+// per-cell enstrophy and kinetic-energy terms of the totals).
+struct DiagDev {
+  double *prim, *fields, *dens;
+};
+// Partial sums per block of the throughput build's two-pass reduction.
+constexpr int kDiagParts = 256;
+
 // One right-hand-side evaluation of every block at RK stage `stage`
 // (state q[stage]); rk: also apply the TVD-RK3 update; eig: reduce the
 // eigenvalue maximum that fixes dt.  Defined once per arithmetic mode.
@@ -131,14 +140,19 @@ void set_error_message(const char *msg);
 
 // configure(): one-time kernel attributes (dynamic shared memory opt-in).
 // tile_count(): CTAs of the dir-sweep over one block of n cells.
+// run_diag(): the solveQ diagnostics of state q[0] of every block into dd[b] and the
+// per-block totals sums[2b] (enstrophy), sums[2b+1] (kinetic energy); parts holds
+// 2 * kDiagParts doubles per block of scratch.
 namespace exact {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 cudaError_t configure();
 int tile_count(int dir, const int n[3]);
 }
 namespace fast {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 cudaError_t configure();
 int tile_count(int dir, const int n[3]);

@@ -81,6 +81,10 @@ struct nuc3d_ctx {
   bool use_graph = true;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  // diagnostics workspace, allocated by the first nuc3d_diagnostics call
+  std::vector<DiagDev> diag;
+  DiagDev *d_diag = nullptr;
+  double *d_dsums = nullptr, *d_dparts = nullptr;
 
   cudaError_t stage(int s, bool rk, bool eig) {
     return exact ? nuc3d::exact::run_stage(L, s, rk, eig) : nuc3d::fast::run_stage(L, s, rk, eig);
@@ -173,6 +177,12 @@ int nuc3d_destroy(nuc3d_ctx *c) {
                    b.ghost, b.fh, b.rows})
       if (p) cudaFree(p);
   }
+  for (auto &d : c->diag)
+    for (auto p : {d.prim, d.fields, d.dens})
+      if (p) cudaFree(p);
+  for (auto p : {c->d_dsums, c->d_dparts})
+    if (p) cudaFree(p);
+  if (c->d_diag) cudaFree(c->d_diag);
   if (c->d_blocks) cudaFree(c->d_blocks);
   if (c->d_jobs) cudaFree(c->d_jobs);
   if (c->d_state) cudaFree(c->d_state);
@@ -558,6 +568,48 @@ int nuc3d_profile_sweep(nuc3d_ctx *c, int dir, int reps, double *ms) {
   cudaEventDestroy(e1);
   *ms = (double)t / reps;
   return check_status(c);
+}
+
+int nuc3d_diagnostics(nuc3d_ctx *c, double *enstrophy, double *kinetic) {
+  if (!c || !enstrophy || !kinetic) return fail(NUC3D_EINVAL, "bad argument");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  cudaSetDevice(c->device);
+  const int nb = (int)c->blocks.size();
+  if (!c->d_diag) {
+    c->diag.assign(nb, DiagDev{nullptr, nullptr, nullptr});
+    for (int bi = 0; bi < nb; ++bi) {
+      const size_t n = (size_t)c->blocks[bi].N * sizeof(double);
+      DiagDev &d = c->diag[bi];
+      CUDA_TRY(cudaMalloc(&d.prim, 4 * n));
+      CUDA_TRY(cudaMalloc(&d.fields, 5 * n));
+      CUDA_TRY(cudaMalloc(&d.dens, 2 * n));
+    }
+    CUDA_TRY(cudaMalloc(&c->d_dsums, 2 * nb * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&c->d_dparts, 2 * (size_t)nb * kDiagParts * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&c->d_diag, nb * sizeof(DiagDev)));
+    CUDA_TRY(cudaMemcpy(c->d_diag, c->diag.data(), nb * sizeof(DiagDev), cudaMemcpyHostToDevice));
+  }
+  CUDA_TRY(c->exact ? nuc3d::exact::run_diag(c->L, c->d_diag, c->d_dsums, c->d_dparts)
+                    : nuc3d::fast::run_diag(c->L, c->d_diag, c->d_dsums, c->d_dparts));
+  std::vector<double> sums(2 * nb);
+  CUDA_TRY(cudaMemcpyAsync(sums.data(), c->d_dsums, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  // MPI_Allreduce(SUM) over the ranks, in rank order (src/postproc.cpp:832-834)
+  double e = sums[0], k = sums[1];
+  for (int bi = 1; bi < nb; ++bi) {
+    e += sums[2 * bi];
+    k += sums[2 * bi + 1];
+  }
+  *enstrophy = e;
+  *kinetic = k;
+  return NUC3D_OK;
+}
+
+int nuc3d_block_get_diag(nuc3d_ctx *c, int bi, double *fields) {
+  if (!c || !fields || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
+  if (!c->d_diag) return fail(NUC3D_ESTATE, "call nuc3d_diagnostics first");
+  return copy_out(c, bi, fields, c->diag[bi].fields, 5);
 }
 
 int nuc3d_kernels_per_step(nuc3d_ctx *c, int *kernels) {

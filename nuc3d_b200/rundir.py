@@ -13,9 +13,13 @@ Reads, relative to RUNDIR, what the reference's singleBlock reads
   bc_topo/BC_Topo_<r>.in   faces xi-,xi+,eta-,eta+,zeta-,zeta+ (src/boundaryConditions.cpp:25-93);
                        a neighbour rank r becomes block r of one GPU context
   flowData/NUC3d_step_<s>_ID_<r>.bin  restart state when startStep > 0 (src/block.cpp:785-855)
+  inp/PostProc.in      5 positional ints; SimutaneousData (the third) 1 asks for
+                       postproc::solveQ (src/postproc.cpp:29-67, 247-260)
 and writes flowData/NUC3d_step_<s>_ID_<r>.bin every saveStep steps when Binary is "yes"
-(src/block.cpp:754-783), with the loop condition of singleBlock::solvePDE
-(src/singleBlock.cpp:51-71): step while time <= tl and step < endStep.
+(src/block.cpp:754-783) and, every postStep steps when SimutaneousData is 1, appends
+"step time enstrophy kinetic" to enstrophy.dat (src/postproc.cpp:836-846), with the
+loop of singleBlock::solvePDE (src/singleBlock.cpp:51-71): step while time <= tl and
+step < endStep; post-process, then save.
 Initial states for startStep == 0 follow block::initialQ (src/block.cpp:523-567) with the
 Benchmark initialisers default / isentropic vortex / Taylor-Green (:658-690), evaluated with
 the C library's sin/cos/exp/pow through Python's math module.
@@ -89,6 +93,15 @@ def read_io(rundir: Path) -> dict:
         elif k in IO_STR:
             io[k] = v
     return io
+
+
+def read_postproc(rundir: Path) -> list[int]:
+    """The positional integers of inp/PostProc.in (the reference exits without the file)."""
+    path = rundir / "inp/PostProc.in"
+    if not path.exists():
+        raise ValueError("inp/PostProc.in does not exist (the reference exits)")
+    words = path.read_text().split()
+    return [int(words[i + 1]) for i in range(0, len(words) - 1, 2)]
 
 
 def read_mesh(path: Path):
@@ -172,6 +185,10 @@ def run(rundir, steps: int | None = None, exact: bool = True, quiet: bool = Fals
     method = read_method(rundir)
     phys = read_phys(rundir)
     io = read_io(rundir)
+    post = read_postproc(rundir)
+    solve_q = len(post) > 2 and post[2] == 1
+    if len(post) > 2 and post[2] not in (0, 1):
+        raise ValueError(f"PostProc.in: no such postproc for {post[2]} (the reference exits)")
     prm = phys["params"]
     cfg = Config(scheme_ivs=tuple(method[f"scheme_{a}_ivs"] for a in "xyz"),
                  scheme_vis=tuple(method[f"scheme_{a}_vis"] for a in "xyz"),
@@ -209,6 +226,10 @@ def run(rundir, steps: int | None = None, exact: bool = True, quiet: bool = Fals
         if not quiet:
             print(f"========step = {step}\n time = {t:.6g}, dt = {dt:.6g}, "
                   f"GPU time = {_time.perf_counter() - w0:.6g}(s) ", flush=True)
+        if solve_q and io["postStep"] != 0 and step % io["postStep"] == 0:
+            ens, kin = s.diagnostics()
+            with open(rundir / "enstrophy.dat", "a") as f:
+                f.write(f"{step} {t:.12g} {ens:.12g} {kin:.12g}\n")
         if io["Binary"] == "yes" and step % io["saveStep"] == 0:
             for r in range(len(shapes)):
                 write_restart(restart_path(rundir, step, r), t, s.get_q(r))

@@ -801,6 +801,101 @@ int oc_step(const oc_config *c, int nb, oc_block *blocks, int nsteps, double *dt
   return 0;
 }
 
+/* ------------------------------------------------------------------ diagnostics
+ * postproc::solveQ (src/postproc.cpp:743-848) after block::Post's getPrim
+ * (src/block.cpp:601-618): velocity gradients by the block's difference operator
+ * (solveGrad, :1797-1820: halo exchange, cd6 inside, boundaryScheme at physical faces),
+ * the chain rule of solveGrad_x/y/z, vorticity, Q, and the totals
+ * enstrophy = sum 0.5|w|^2 and kinetic = sum 0.5 rho |u|^2, summed cell by cell in
+ * k-j-i order per block and then over the blocks in order (MPI_Allreduce in rank order).
+ * fields: per block NULL or 5N (w_x, w_y, w_z, 0.5|w|^2, Q). */
+int oc_diag(const oc_config *c, int nb, oc_block *blocks, double *enstrophy, double *kinetic,
+            double **fields) {
+  int bfs = 3, ts[3];
+  for (int d = 0; d < 3; ++d) {
+    ts[d] = (c->scheme[d] == S_WENO7JS || c->scheme[d] == S_HCCS) ? 4 : 3;
+    if (ts[d] == 4) bfs = 4;
+  }
+  int maxL = 0;
+  for (int bi = 0; bi < nb; ++bi)
+    for (int d = 0; d < 3; ++d)
+      if (blocks[bi].n[d] > maxL) maxL = blocks[bi].n[d];
+  double *ext = malloc(sizeof(double) * (maxL + 2 * bfs + 2));
+  work_t *W = calloc(nb, sizeof(work_t));
+  for (int bi = 0; bi < nb; ++bi) {
+    long N = (long)blocks[bi].n[0] * blocks[bi].n[1] * blocks[bi].n[2];
+    W[bi].b = &blocks[bi];
+    W[bi].N = N;
+    W[bi].w = malloc(sizeof(prim_t) * N);
+    W[bi].grad = malloc(sizeof(double) * 12 * N);
+    pass_con2prim(c, &W[bi]);
+  }
+  for (int bi = 0; bi < nb; ++bi) {
+    oc_block *b = W[bi].b;
+    long N = W[bi].N;
+    for (int d = 0; d < 3; ++d) {
+      int L = b->n[d], A = slabA(b, d), B = slabB(b, d);
+      int pl = b->bc_type[2 * d] < 0, pr = b->bc_type[2 * d + 1] < 0;
+      for (int bb = 0; bb < B; ++bb)
+        for (int a = 0; a < A; ++a)
+          for (int comp = 0; comp < 3; ++comp) {
+            field_line(W, bfs, bi, d, a, bb, 0, comp, ext);
+            for (int pos = 0; pos < L; ++pos) {
+              int i, j, k;
+              unslab(d, pos, a, bb, &i, &j, &k);
+              W[bi].grad[(comp * 3 + d) * N + cell(b, i, j, k)] = line_diff(ext, bfs, pos, L, ts[d], pl, pr);
+            }
+          }
+    }
+  }
+  double ens_glb = 0.0, kin_glb = 0.0;
+  for (int bi = 0; bi < nb; ++bi) {
+    oc_block *b = W[bi].b;
+    long N = W[bi].N;
+    const double *g = W[bi].grad;
+    double ens = 0.0, kin = 0.0;
+    for (long x = 0; x < N; ++x) {
+#define GR(cmp, dd) g[((cmp) * 3 + (dd)) * N + x]
+      double xi_x = b->xi[x], xi_y = b->xi[N + x], xi_z = b->xi[2 * N + x];
+      double eta_x = b->eta[x], eta_y = b->eta[N + x], eta_z = b->eta[2 * N + x];
+      double zeta_x = b->zeta[x], zeta_y = b->zeta[N + x], zeta_z = b->zeta[2 * N + x];
+      double ux = GR(0, 0) * xi_x + GR(0, 1) * eta_x + GR(0, 2) * zeta_x;
+      double uy = GR(0, 0) * xi_y + GR(0, 1) * eta_y + GR(0, 2) * zeta_y;
+      double uz = GR(0, 0) * xi_z + GR(0, 1) * eta_z + GR(0, 2) * zeta_z;
+      double vx = GR(1, 0) * xi_x + GR(1, 1) * eta_x + GR(1, 2) * zeta_x;
+      double vy = GR(1, 0) * xi_y + GR(1, 1) * eta_y + GR(1, 2) * zeta_y;
+      double vz = GR(1, 0) * xi_z + GR(1, 1) * eta_z + GR(1, 2) * zeta_z;
+      double wx = GR(2, 0) * xi_x + GR(2, 1) * eta_x + GR(2, 2) * zeta_x;
+      double wy = GR(2, 0) * xi_y + GR(2, 1) * eta_y + GR(2, 2) * zeta_y;
+      double wz = GR(2, 0) * xi_z + GR(2, 1) * eta_z + GR(2, 2) * zeta_z;
+#undef GR
+      double w0 = wy - vz, w1 = uz - wx, w2 = vx - uy;
+      double q0 = ux * vy + ux * wz + vy * wz - uy * vx - uz * wx - vz * wy;
+      if (fields && fields[bi]) {
+        fields[bi][x] = w0;
+        fields[bi][N + x] = w1;
+        fields[bi][2 * N + x] = w2;
+        fields[bi][3 * N + x] = (w0 * w0 + w1 * w1 + w2 * w2) * 0.5;
+        fields[bi][4 * N + x] = q0;
+      }
+      const prim_t *s = &W[bi].w[x];
+      ens += 0.5 * (w0 * w0 + w1 * w1 + w2 * w2);
+      kin += 0.5 * s->rho * (s->u * s->u + s->v * s->v + s->w * s->w);
+    }
+    ens_glb = bi == 0 ? ens : ens_glb + ens;
+    kin_glb = bi == 0 ? kin : kin_glb + kin;
+  }
+  for (int bi = 0; bi < nb; ++bi) {
+    free(W[bi].w);
+    free(W[bi].grad);
+  }
+  free(W);
+  free(ext);
+  *enstrophy = ens_glb;
+  *kinetic = kin_glb;
+  return 0;
+}
+
 /* ------------------------------------------------------------------ metrics
  * block::getJacobians (src/block.cpp:237-325) with the 4x4x4-cell tile Lagrange
  * reconstruction of src/block.cpp:147-235 (centres) and :327-477 (derivatives),

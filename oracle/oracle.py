@@ -45,6 +45,9 @@ def lib() -> ctypes.CDLL:
                                  ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                  ctypes.POINTER(ctypes.c_double)]
         _lib.oc_metrics.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 8
+        _lib.oc_diag.argtypes = [ctypes.POINTER(OcConfig), ctypes.c_int, ctypes.POINTER(OcBlock),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(ctypes.c_void_p)]
     return _lib
 
 
@@ -118,3 +121,14 @@ class Run:
 
     def q(self, b):
         return self._keep[b][1]
+
+    def diag(self):
+        """postproc::solveQ of the current state: (enstrophy, kinetic, per-block fields of
+        shape (5, nz, ny, nx): vorticity x, y, z, enstrophy density, Q)."""
+        arr = self._arr()
+        fields = [np.empty((5,) + k[0]["jac"].shape) for k in self._keep]
+        ptrs = (ctypes.c_void_p * len(fields))(*[f.ctypes.data for f in fields])
+        ens, kin = ctypes.c_double(), ctypes.c_double()
+        lib().oc_diag(ctypes.byref(self.cfg), len(self.blocks), arr, ctypes.byref(ens),
+                      ctypes.byref(kin), ptrs)
+        return ens.value, kin.value, fields

@@ -14,6 +14,10 @@
 //   nuc3d_ref_taps steps N OUT  N TVD-RK3 steps of block::solve (src/block.cpp:569-594)
 //   nuc3d_ref_taps time  N W    W untimed + N timed steps; prints the reference's own
 //                              per-step wall time (src/block.cpp:576-584) as JSON
+//   nuc3d_ref_taps post  N OUT  N steps, then block::Post (src/block.cpp:601-618), whose
+//                              postproc::solveQ (src/postproc.cpp:743-848) needs
+//                              SimutaneousData 1 in inp/PostProc.in: enstrophy and kinetic
+//                              energy totals and the vorticity / enstrophy / Q fields
 //
 // OUT gets the rank number appended ("OUT.r<rank>").  Format: "NUCT" then records
 // {u32 name_len, name, u32 ndim, i64 dims[ndim], f64 data[prod(dims)]}.
@@ -46,11 +50,32 @@
 #include "physicsModel.h"
 #include "IOcontroller.h"
 #include "fieldOperator.h"
+#include "postproc.hpp"
 #undef private
 #undef protected
 
 using nuc3d::Field;
 using nuc3d::VectorField;
+
+// postproc keeps its totals and fields under the class's default (private) access,
+// which the #define above cannot widen.  An explicit instantiation may name a private
+// member ([temp.spec]/6), so these tags hand out member pointers to them.
+namespace taps_access {
+template <typename Tag, typename Tag::type M>
+struct Grant {
+  friend typename Tag::type member(Tag) { return M; }
+};
+struct EnsGlb { typedef double nuc3d::postproc::*type; friend type member(EnsGlb); };
+struct KinGlb { typedef double nuc3d::postproc::*type; friend type member(KinGlb); };
+struct Ens { typedef double nuc3d::postproc::*type; friend type member(Ens); };
+struct Kin { typedef double nuc3d::postproc::*type; friend type member(Kin); };
+struct QField { typedef VectorField nuc3d::postproc::*type; friend type member(QField); };
+template struct Grant<EnsGlb, &nuc3d::postproc::enstrophy_glb>;
+template struct Grant<KinGlb, &nuc3d::postproc::kinetic_glb>;
+template struct Grant<Ens, &nuc3d::postproc::enstrophy>;
+template struct Grant<Kin, &nuc3d::postproc::kinetic>;
+template struct Grant<QField, &nuc3d::postproc::TemporalQField>;
+}  // namespace taps_access
 
 namespace {
 
@@ -201,6 +226,20 @@ int main(int argc, char **argv) {
         w.rec("dt", {(long long)n}, dts.data());
         w.rec("time", {(long long)n}, times.data());
       }
+    } else if (mode == "post") {
+      if (argc < 4) return 2;
+      int n = std::atoi(argv[2]);
+      for (int s = 0; s < n; ++s) h.myBlock.solve(h.myOperator, h.myPhys, h.myMPI, h.myBC, h.myIO);
+      h.myBlock.Post(h.myOperator, h.myPhys, h.myMPI, h.myBC, h.myIO);
+      nuc3d::postproc &pp = *h.myBlock.myPost;
+      Writer w(ranked(argv[3], rank));
+      w.fields("Q", h.myBlock.myPDE.getQ());
+      using namespace taps_access;
+      w.scalar("enstrophy_glb", pp.*member(EnsGlb()));
+      w.scalar("kinetic_glb", pp.*member(KinGlb()));
+      w.scalar("enstrophy", pp.*member(Ens()));
+      w.scalar("kinetic", pp.*member(Kin()));
+      w.fields("qfield", pp.*member(QField()));
     } else if (mode == "time") {
       if (argc < 4) return 2;
       int n = std::atoi(argv[2]);

@@ -56,6 +56,7 @@ class Case:
     cfl: float = 0.5
     benchmark: int = 0                  # initialiser index when startStep == 0
     start_step: int = 0                 # > 0: Q comes from the restart file
+    post_q: bool = False                # PostProc.in SimutaneousData 1 (postproc::solveQ)
     # per rank: node coordinates x, y, z each shaped (nz+1, ny+1, nx+1)
     nodes: list = field(default_factory=list)
     # per rank: 6 strings "type id [values...]"
@@ -92,7 +93,7 @@ def write_case(case: Case, rundir: Path) -> None:
         f"Benchmark {case.benchmark}\ncfl {_fmt(case.cfl)}\ntl 1e300\ndt 0.01\n"
         "Binary no\nTecplot no\nPostProc no\n")
     (rundir / "inp/PostProc.in").write_text(
-        "AverageType 0\nAverageStartStep 0\nSimutaneousData 0\nAveragedSaveType 0\n"
+        f"AverageType 0\nAverageStartStep 0\nSimutaneousData {int(case.post_q)}\nAveragedSaveType 0\n"
         "SimutaneousSaveType 0\n")
     for r, xyz in enumerate(case.nodes):
         x, y, z = (np.asarray(a, dtype=np.float64) for a in xyz)
@@ -143,7 +144,7 @@ def run(case: Case, mode: str, *args, binary: str = "nuc3d_ref_taps", keep: Path
         env = dict(os.environ, NUC_SHIM_NP=str(case.nranks))
         out = tmp / "dump.nuct"
         argv = [str(ref_binary(binary)), mode, *[str(a) for a in args]]
-        if mode in ("init", "rhs", "steps"):
+        if mode in ("init", "rhs", "steps", "post"):
             argv.append(str(out))
         p = subprocess.run(argv, cwd=tmp, env=env, capture_output=True, text=True,
                            timeout=timeout)

@@ -1,6 +1,6 @@
 """Generate the golden fixtures in tests/golden/ by running the NUC3d reference.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [--diag] [case ...]
 
 Needs the reference binaries built under oracle/_ref (from the reference sources);
 the fixtures it writes are committed so the tests never need the sources.
@@ -12,6 +12,9 @@ Each fixture <name>.npz holds one case:
   dt, time        per-step dt and accumulated time of those nsteps
   metrics_*       (only in the first fixture) the reference's metrics, to pin the
                   host metric computation
+and diag/<name>.npz the postproc::solveQ diagnostics of the state after those n steps
+(--diag regenerates only these; diag/tgv_ns_weno5js_lf.2ranks.npz is the same case run
+as two ranks, to pin the sum over blocks).
 Node coordinates use only + - * / (oracle.refrun.box_nodes), so tests rebuild the
 mesh bit for bit instead of storing it.
 """
@@ -162,14 +165,65 @@ def generate(cd):
     return out
 
 
-def main(names=None):
+DIAG = OUT / "diag"
+
+
+def split_xi(case, cd):
+    """The case as two ranks, the xi range cut in half (periodic xi faces only)."""
+    (x, y, z), = case.nodes
+    h = cd["shape"][0] // 2
+    nodes = [tuple(a[:, :, :h + 1] for a in (x, y, z)), tuple(a[:, :, h:] for a in (x, y, z))]
+    topo = []
+    for r in range(2):
+        lines = [f"{1 - r} 1", f"{1 - r} 0"]
+        lines += [f"{r} {f ^ 1}" for f in range(2, 6)]
+        topo.append(lines)
+    case.nodes, case.bc_topo = nodes, topo
+    return case
+
+
+def generate_diag(cd, nranks=1):
+    """postproc::solveQ after the case's n steps (block::Post, src/block.cpp:601-618):
+    enstrophy and kinetic-energy totals, and the per-cell vorticity (3), enstrophy
+    density and Q-criterion fields."""
+    case = build_case(cd)
+    case.post_q = True
+    if cd["init"] != "tgv":
+        init = R.run(case, "init")[0]
+        xc, yc, zc = (init[f"xyz_center.{i}"] for i in range(3))
+        case.q0 = [R.prim_to_q(initial_prim(cd["init"], xc, yc, zc, cd["params"]), init["jac"],
+                               cd["params"]["Gamma"])]
+        case.start_step = 1
+    if nranks == 2:
+        case = split_xi(case, cd)
+    out = R.run(case, "post", cd["nsteps"])
+    cat = lambda key: np.concatenate([d[key] for d in out], axis=-1)  # noqa: E731
+    res = dict(
+        nsteps=np.array([cd["nsteps"]]), nranks=np.array([nranks]),
+        enstrophy=out[0]["enstrophy_glb"], kinetic=out[0]["kinetic_glb"],
+        fields=np.stack([cat(f"qfield.{k}") for k in range(9, 14)]),
+    )
+    DIAG.mkdir(exist_ok=True)
+    tag = "" if nranks == 1 else f".{nranks}ranks"
+    np.savez_compressed(DIAG / f"{cd['name']}{tag}.npz", **res)
+    return res
+
+
+def main(names=None, diag_only=False):
     for cd in case_defs():
         if names and cd["name"] not in names:
             continue
-        o = generate(cd)
-        extra = f" libm_rel_diff={o['libm_max_rel_diff'][0]:.3g}" if "libm_max_rel_diff" in o else ""
-        print(f"{cd['name']}: dt_local={o['dt_local'][0]:.6g} dt={o['dt']}{extra}")
+        if not diag_only:
+            o = generate(cd)
+            extra = f" libm_rel_diff={o['libm_max_rel_diff'][0]:.3g}" if "libm_max_rel_diff" in o else ""
+            print(f"{cd['name']}: dt_local={o['dt_local'][0]:.6g} dt={o['dt']}{extra}")
+        d = generate_diag(cd)
+        print(f"{cd['name']} diag: enstrophy={d['enstrophy'][0]:.12g} kinetic={d['kinetic'][0]:.12g}")
+        if cd["name"] == "tgv_ns_weno5js_lf":
+            d = generate_diag(cd, nranks=2)
+            print(f"{cd['name']} diag 2 ranks: enstrophy={d['enstrophy'][0]:.12g}")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:])
+    args = sys.argv[1:]
+    main([a for a in args if a != "--diag"], diag_only="--diag" in args)

@@ -31,6 +31,22 @@ def names():
     return sorted(p.stem for p in GOLDEN.glob("*.npz"))
 
 
+def load_diag(name: str) -> dict:
+    """postproc::solveQ of the case's state after its n steps (golden/diag/<name>.npz)."""
+    z = np.load(GOLDEN / "diag" / f"{name}.npz")
+    return {k: z[k] for k in z.files}
+
+
+def split_xi(arrays, h):
+    """Cut cell arrays (..., nz, ny, nx) at i = h into two blocks."""
+    return [a[..., :h] for a in arrays], [a[..., h:] for a in arrays]
+
+
+# two blocks cut along xi from one periodic block: block indices and neighbour faces
+TWO_BLOCK_TYPES = [[1, 1, 0, 0, 0, 0], [0, 0, 1, 1, 1, 1]]
+TWO_BLOCK_IDS = [[1, 0, 3, 2, 5, 4], [1, 0, 3, 2, 5, 4]]
+
+
 def load(name: str) -> Golden:
     z = np.load(GOLDEN / f"{name}.npz")
     data = {k: z[k] for k in z.files}

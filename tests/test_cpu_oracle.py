@@ -1,5 +1,6 @@
 """The C restatement (oracle/nuc3d_oracle.c) reproduces the reference's golden vectors
-bit for bit: metrics, one right-hand side, dt, and the state after 1 and n steps."""
+bit for bit: metrics, one right-hand side, dt, the state after 1 and n steps, and the
+postproc::solveQ diagnostics (totals and fields) of that state."""
 import numpy as np
 import pytest
 
@@ -42,3 +43,31 @@ def test_oracle_steps_bitwise(name):
     dt, t = r.step(n)
     assert np.array_equal(r.q(0), g.qn), np.max(np.abs(r.q(0) - g.qn))
     assert np.array_equal(dt, g.dt) and t == g.time[-1]
+
+
+@pytest.mark.parametrize("name", G.names())
+def test_oracle_diag_bitwise(name):
+    g, d = G.load(name), G.load_diag(name)
+    r = O.Run(g.cfg["schemes"], g.cfg["riemann"], g.cfg["model"], g.cfg["params"])
+    t, i, v = G.bc_arrays(g)
+    r.add_block(O.metrics(*G.nodes(g)), t, i, v, g.qn)
+    ens, kin, f = r.diag()
+    assert ens == d["enstrophy"][0] and kin == d["kinetic"][0], (ens - d["enstrophy"][0], kin - d["kinetic"][0])
+    assert np.array_equal(f[0], d["fields"]), np.max(np.abs(f[0] - d["fields"]))
+
+
+def test_oracle_diag_two_blocks_bitwise():
+    """The reference run as two ranks: fields equal the single block's, totals are the
+    block sums added in rank order."""
+    g, d = G.load("tgv_ns_weno5js_lf"), G.load_diag("tgv_ns_weno5js_lf.2ranks")
+    m = O.metrics(*G.nodes(g))
+    h = g.cfg["shape"][0] // 2
+    keys = ("jac", "xi_xyz", "eta_xyz", "zeta_xyz", "dxyz")
+    left, right = G.split_xi([m[k] for k in keys] + [g.qn], h)
+    r = O.Run(g.cfg["schemes"], g.cfg["riemann"], g.cfg["model"], g.cfg["params"])
+    for b, part in enumerate((left, right)):
+        mb = {k: np.ascontiguousarray(a) for k, a in zip(keys, part[:5])}
+        r.add_block(mb, G.TWO_BLOCK_TYPES[b], G.TWO_BLOCK_IDS[b], None, np.ascontiguousarray(part[5]))
+    ens, kin, f = r.diag()
+    assert ens == d["enstrophy"][0] and kin == d["kinetic"][0]
+    assert np.array_equal(np.concatenate(f, axis=-1), d["fields"])

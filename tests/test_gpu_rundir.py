@@ -1,8 +1,10 @@
 """A reference run directory, unchanged, runs on the GPU and writes the reference's restart files.
 
 The directory is written by oracle.refrun (exactly what the reference reads), the
-reference runs in it and saves flowData/NUC3d_step_<s>_ID_<r>.bin; nuc3d_b200.run runs
-the same directory and its restart files must be byte-identical (reference-order build)."""
+reference runs in it and saves flowData/NUC3d_step_<s>_ID_<r>.bin and, with
+SimutaneousData 1 and postStep 1, appends its enstrophy / kinetic-energy line to
+enstrophy.dat every step; nuc3d_b200.run runs the same directory and both its restart
+files and its enstrophy.dat must be byte-identical (reference-order build)."""
 import math
 import os
 import shutil
@@ -35,12 +37,13 @@ def _case(multi: bool):
 def test_run_directory_restart_files_identical(multi):
     from nuc3d_b200 import rundir as RD
     case = _case(multi)
+    case.post_q = True
     tmp = Path(tempfile.mkdtemp(prefix="nuc3d_rundir_"))
     try:
         R.write_case(case, tmp)
         io = (tmp / "inp/IOController.in").read_text()
         io = io.replace("endStep 1000000000", "endStep 4").replace("saveStep 1000000000", "saveStep 2")
-        io = io.replace("Binary no", "Binary yes")
+        io = io.replace("Binary no", "Binary yes").replace("postStep 0", "postStep 1")
         (tmp / "inp/IOController.in").write_text(io)
         ref = tmp / "ref"
         shutil.copytree(tmp, ref, ignore=shutil.ignore_patterns("ref"))
@@ -54,5 +57,8 @@ def test_run_directory_restart_files_identical(multi):
                 a = (ref / f"flowData/NUC3d_step_{step}_ID_{r}.bin").read_bytes()
                 b = (tmp / f"flowData/NUC3d_step_{step}_ID_{r}.bin").read_bytes()
                 assert a == b, (step, r)
+        a = (ref / "enstrophy.dat").read_text()
+        b = (tmp / "enstrophy.dat").read_text()
+        assert len(a.splitlines()) == 4 and a == b, (a, b)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
