@@ -12,7 +12,12 @@
 
 namespace nuc3d {
 
-enum Scheme : int { SCH_WENO5JS = 0, SCH_WENO5Z = 1, SCH_WENO7JS = 2, SCH_CRWENO5 = 3, SCH_HCCS = 4 };
+enum Scheme : int {
+  SCH_WENO5JS = 0, SCH_WENO5Z = 1, SCH_WENO7JS = 2, SCH_CRWENO5 = 3, SCH_HCCS = 4,
+  SCH_WENO3JS = 5, SCH_UPWIND1 = 6
+};
+// Viscous difference per direction (scheme_x/y/z_vis, src/fieldOperator.cpp:286-367).
+enum VisScheme : int { VIS_CD6 = 0, VIS_CD2 = 1, VIS_CD8 = 2 };
 enum Riemann : int { RIE_LF = 0, RIE_AUSM = 1, RIE_AUSMP = 2 };
 enum Model : int { MODEL_EULER = 0, MODEL_NS = 1 };
 enum BcId : int { BC_INLET = 0, BC_OUTLET = 1, BC_WALL = 2, BC_SYMM = 3 };
@@ -27,7 +32,7 @@ enum StatusBits : unsigned {
 
 // Reference bufferSize per scheme (src/fieldOperator.cpp:127-283).
 inline __host__ __device__ int scheme_tilesize(int s) {
-  return (s == SCH_WENO7JS || s == SCH_HCCS) ? 4 : 3;
+  return (s == SCH_WENO7JS || s == SCH_HCCS) ? 4 : s == SCH_WENO3JS ? 2 : s == SCH_UPWIND1 ? 1 : 3;
 }
 
 struct FaceDev {
@@ -91,6 +96,7 @@ struct SolverParams {
   int riemann;
   int model;
   int weno5z_compat;     // 1: reproduce the interior positive is2 of src/weno5z.cpp:80
+  int vis[3];            // VisScheme per direction
   double gamma, mach, reynolds, prandtl, t_ref, t_inf, t_wall, cfl;
 };
 

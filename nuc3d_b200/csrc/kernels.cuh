@@ -37,8 +37,11 @@ constexpr int kThreads = kTW * kTL + 32;
 template <int DIR> struct Tile { static constexpr int TW = kTW, TL = kTL; };
 
 template <int SCH> struct Halo {
-  static constexpr int R = (SCH == SCH_WENO7JS || SCH == SCH_HCCS) ? 4 : 3;
+  static constexpr int R = (SCH == SCH_WENO7JS || SCH == SCH_HCCS) ? 4
+                           : SCH == SCH_WENO3JS ? 2 : SCH == SCH_UPWIND1 ? 1 : 3;
 };
+// Halo of the viscous tiles: the widest viscous stencil (cd8) reaches 4 cells.
+constexpr int kVisHalo = 4;
 
 // Row strides of the shared-memory tiles, padded so that the TW rows of one warp
 // access fall in different bank halves (stride = 8 mod 16 doubles).
@@ -73,7 +76,7 @@ template <int DIR, int SCH>
 __host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
   constexpr int R = Halo<SCH>::R, TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
   size_t n = (size_t)10 * TW * pad_row(TL + 2 * R) + (size_t)5 * TW * pad_row(TL + 1);
-  if (ns) n += (size_t)4 * TW * pad_row(TL + 6);
+  if (ns) n += (size_t)4 * TW * pad_row(TL + 2 * kVisHalo);
   if (DIR == 2) n += (size_t)5 * TW * pad_row(TL);
   return n * sizeof(double);
 }
@@ -198,6 +201,8 @@ __device__ __forceinline__ void bc_ghost_flux(const BlockDev &B, int stage, int 
 // src/weno5z.cpp:80 (interior positive faces only).
 template <int SCH, class Acc>
 __device__ __forceinline__ double recon_pos_in(int f, bool compat, Acc P) {
+  if (SCH == SCH_WENO3JS) return rb_third(P(f - 2), P(f - 1), P(f));  // src/weno3js.cpp:59-86
+  if (SCH == SCH_UPWIND1) return P(f - 1);                            // src/upwind1st.cpp:57-75
   if (SCH == SCH_WENO7JS || SCH == SCH_HCCS) {
     double s[7] = {P(f - 4), P(f - 3), P(f - 2), P(f - 1), P(f), P(f + 1), P(f + 2)};
     return SCH == SCH_HCCS ? weno7z(s) : weno7js(s);
@@ -210,6 +215,8 @@ __device__ __forceinline__ double recon_pos_in(int f, bool compat, Acc P) {
 
 template <int SCH, class Acc>
 __device__ __forceinline__ double recon_neg_in(int f, Acc Nf) {
+  if (SCH == SCH_WENO3JS) return rb_third(Nf(f + 1), Nf(f), Nf(f - 1));  // src/weno3js.cpp:88-115
+  if (SCH == SCH_UPWIND1) return Nf(f);                                  // src/upwind1st.cpp:96-114
   if (SCH == SCH_WENO7JS || SCH == SCH_HCCS) {
     double s[7] = {Nf(f + 3), Nf(f + 2), Nf(f + 1), Nf(f), Nf(f - 1), Nf(f - 2), Nf(f - 3)};
     return SCH == SCH_HCCS ? weno7z(s) : weno7js(s);
@@ -312,9 +319,11 @@ __device__ __forceinline__ double edge_face(int f, int L, int ts, bool physR, in
 
 // d/dxi of a cell-centred field at line position c: boundaryScheme within ts cells
 // of a physical face (src/fieldOperator.cpp:523-624, src/boundaryScheme.cpp:311-406),
-// cd6 elsewhere (ghost values come from the neighbour across the face).
+// the direction's scheme_vis operator (cd6, cd2 or cd8) elsewhere (ghost values come from
+// the neighbour across the face).
 template <class Acc>
-__device__ __forceinline__ double diff_at(int c, int L, int ts, bool physL, bool physR, Acc V) {
+__device__ __forceinline__ double diff_at(int c, int L, int ts, bool physL, bool physR, int vis,
+                                          Acc V) {
   if (physR && c >= L - ts) {
     switch (L - 1 - c) {
       case 0: return V(c) - V(c - 1);
@@ -331,6 +340,9 @@ __device__ __forceinline__ double diff_at(int c, int L, int ts, bool physL, bool
       default: return bnd_sixth(V(c - 3), V(c - 2), V(c - 1), V(c + 1), V(c + 2), V(c + 3));
     }
   }
+  if (vis == VIS_CD2) return cd2(V(c - 1), V(c + 1));
+  if (vis == VIS_CD8)
+    return cd8(V(c - 4), V(c - 3), V(c - 2), V(c - 1), V(c + 1), V(c + 2), V(c + 3), V(c + 4));
   return cd6(V(c - 3), V(c - 2), V(c - 1), V(c + 1), V(c + 2), V(c + 3));
 }
 
@@ -391,7 +403,7 @@ __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ bloc
 template <int DIR, int SCH> struct TileSmem {
   static constexpr int R = Halo<SCH>::R, TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
   static constexpr int NP = TL + 2 * R, SP = pad_row(NP);
-  static constexpr int NV = TL + 6, SV = pad_row(NV);
+  static constexpr int NV = TL + 2 * kVisHalo, SV = pad_row(NV);
   static constexpr int SH = pad_row(TL + 1), SQ = pad_row(TL);
 };
 
@@ -464,7 +476,7 @@ __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks,
   }
 }
 
-// Viscous fluxes of the tile's line positions c0-3 .. c0+cl+2 into sV ([4][TW][SV]).
+// Viscous fluxes of the tile's line positions c0-4 .. c0+cl+3 into sV ([4][TW][SV]).
 template <int DIR, int SCH>
 __device__ __forceinline__ void phase_vis(const BlockDev *__restrict__ blocks, const TileCtx &T,
                                           const SolverParams &P, double *sV) {
@@ -476,8 +488,10 @@ __device__ __forceinline__ void phase_vis(const BlockDev *__restrict__ blocks, c
     int p, w;
     if (DIR == 0) { p = e % NV; w = e / NV; } else { w = e % TW; p = e / TW; }
     double fv[4] = {0.0, 0.0, 0.0, 0.0};
-    const int g = T.c0 + p - 3;
-    if (w < T.nw && p < T.cl + 6) {
+    const int g = T.c0 + p - kVisHalo;
+    // ghosts exist up to bfsize cells out; the viscous stencil of a direction never
+    // reaches further (nuc3d_create checks reach <= tilesize <= bfsize)
+    if (w < T.nw && p < T.cl + 2 * kVisHalo && g >= -P.bfs && g < G.L + P.bfs) {
       const int wl = T.w0 + w;
       const int sa = (DIR == 1) ? T.o : wl, sb = (DIR == 1) ? wl : T.o;
       const double *vis = nullptr;
@@ -545,9 +559,9 @@ __device__ __forceinline__ void phase_cells(const TileCtx &T, const SolverParams
     if (ns) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        const double *row = sV + (v * TW + w) * SV + (3 - T.c0);
+        const double *row = sV + (v * TW + w) * SV + (kVisHalo - T.c0);
         auto Vacc = [row](int cc) { return row[cc]; };
-        dv[v] = diff_at(g, G.L, T.ts, T.physL, T.physR, Vacc);
+        dv[v] = diff_at(g, G.L, T.ts, T.physL, T.physR, P.vis[DIR], Vacc);
       }
     }
     if (DIR == 0) {
@@ -965,7 +979,7 @@ grad_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       auto V = [&](int g) { return prim_along(blocks, B, d, i, j, k, g, c, P.bfs); };
-      gr[c][d] = diff_at(pos[d], B.n[d], P.ts[d], pl, pr, V);
+      gr[c][d] = diff_at(pos[d], B.n[d], P.ts[d], pl, pr, P.vis[d], V);
     }
   }
   const double jac = __ldg(B.jac + idx);
@@ -1084,7 +1098,7 @@ diag_kernel(const BlockDev *__restrict__ blocks, const DiagDev *__restrict__ dd,
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       auto V = [&](int g) { return diag_prim_along(blocks, dd, b, d, i, j, k, g, c + 1, P.bfs); };
-      gr[c][d] = diff_at(pos[d], B.n[d], P.ts[d], pl, pr, V);
+      gr[c][d] = diff_at(pos[d], B.n[d], P.ts[d], pl, pr, P.vis[d], V);
     }
   }
   double mx[3][3];
@@ -1243,6 +1257,8 @@ inline cudaError_t launch_sweep(const Launch &L, int stage, int flags) {
     case SCH_WENO5JS: return launch_sweep_t<DIR, SCH_WENO5JS>(L, stage, flags);
     case SCH_WENO5Z: return launch_sweep_t<DIR, SCH_WENO5Z>(L, stage, flags);
     case SCH_WENO7JS: return launch_sweep_t<DIR, SCH_WENO7JS>(L, stage, flags);
+    case SCH_WENO3JS: return launch_sweep_t<DIR, SCH_WENO3JS>(L, stage, flags);
+    case SCH_UPWIND1: return launch_sweep_t<DIR, SCH_UPWIND1>(L, stage, flags);
     case SCH_CRWENO5: return launch_compact_t<DIR, SCH_CRWENO5>(L, stage, flags);
     case SCH_HCCS: return launch_compact_t<DIR, SCH_HCCS>(L, stage, flags);
     default: return cudaErrorInvalidValue;
@@ -1330,6 +1346,8 @@ inline cudaError_t configure_dir() {
   if ((e = configure_t<DIR, SCH_WENO5Z>()) != cudaSuccess) return e;
   if ((e = configure_compact_t<DIR, SCH_CRWENO5>()) != cudaSuccess) return e;
   if ((e = configure_compact_t<DIR, SCH_HCCS>()) != cudaSuccess) return e;
+  if ((e = configure_t<DIR, SCH_WENO3JS>()) != cudaSuccess) return e;
+  if ((e = configure_t<DIR, SCH_UPWIND1>()) != cudaSuccess) return e;
   return configure_t<DIR, SCH_WENO7JS>();
 }
 

@@ -58,9 +58,27 @@ int parse_scheme(const char *s, int *out) {
   else if (!std::strcmp(s, "weno7js")) *out = SCH_WENO7JS;
   else if (!std::strcmp(s, "crweno5")) *out = SCH_CRWENO5;
   else if (!std::strcmp(s, "hccs")) *out = SCH_HCCS;
+  else if (!std::strcmp(s, "weno3js")) *out = SCH_WENO3JS;
+  else if (!std::strcmp(s, "upwind1st")) *out = SCH_UPWIND1;
+  else if (!std::strcmp(s, "hccs77"))
+    return fail(NUC3D_ENOTSUP, "reconstruction scheme 'hccs77' is not implemented");
   else return fail(NUC3D_EINVAL, "unknown reconstruction scheme '%s'", s);
   return NUC3D_OK;
 }
+
+// scheme_x/y/z_vis (src/fieldOperator.cpp:286-367); null means cd6, the reference default
+int parse_vis(const char *s, int *out) {
+  if (!s || !std::strcmp(s, "cd6")) *out = VIS_CD6;
+  else if (!std::strcmp(s, "cd2")) *out = VIS_CD2;
+  else if (!std::strcmp(s, "cd8")) *out = VIS_CD8;
+  else return fail(NUC3D_EINVAL, "unknown viscous scheme '%s' (cd2 | cd6 | cd8)", s);
+  return NUC3D_OK;
+}
+
+// Cells the viscous stencil reaches.  The reference's difference loops start at the
+// direction's tilesize (src/centraldifference6th.cpp:26-43, 8th :27-52) and take ghosts
+// from slabs bfsize wide, so a reach beyond the tilesize reads outside its rows.
+int vis_reach(int vis) { return vis == VIS_CD2 ? 1 : vis == VIS_CD8 ? 4 : 3; }
 
 }  // namespace
 
@@ -115,9 +133,7 @@ int nuc3d_create(const nuc3d_config *cfg, int device, nuc3d_ctx **out) {
   for (int d = 0; d < 3; ++d) {
     int r = parse_scheme(cfg->scheme_ivs[d], &P.scheme[d]);
     if (r) return r;
-    const char *v = cfg->scheme_vis[d];
-    if (v && std::strcmp(v, "cd6"))
-      return fail(NUC3D_ENOTSUP, "viscous scheme '%s' is not implemented (cd6 only)", v);
+    if ((r = parse_vis(cfg->scheme_vis[d], &P.vis[d]))) return r;
     P.ts[d] = scheme_tilesize(P.scheme[d]);
   }
   // block::initialData: bfsize = max of the three bufferSizes (src/block.cpp:506-507)
@@ -132,6 +148,13 @@ int nuc3d_create(const nuc3d_config *cfg, int device, nuc3d_ctx **out) {
   if (!std::strcmp(cfg->model, "Euler3d")) P.model = MODEL_EULER;
   else if (!std::strcmp(cfg->model, "NavierStokes3d")) P.model = MODEL_NS;
   else return fail(NUC3D_EINVAL, "unknown model '%s' (Euler3d | NavierStokes3d)", cfg->model);
+  if (P.model == MODEL_NS)
+    for (int d = 0; d < 3; ++d)
+      if (vis_reach(P.vis[d]) > P.ts[d])
+        return fail(NUC3D_ENOTSUP,
+                    "direction %d: the viscous stencil reaches %d cells but the reconstruction's "
+                    "bufferSize is %d; the reference reads outside its arrays there", d,
+                    vis_reach(P.vis[d]), P.ts[d]);
   P.reynolds = cfg->reynolds;
   P.mach = cfg->mach;
   P.prandtl = cfg->prandtl;
@@ -573,6 +596,12 @@ int nuc3d_profile_sweep(nuc3d_ctx *c, int dir, int reps, double *ms) {
 int nuc3d_diagnostics(nuc3d_ctx *c, double *enstrophy, double *kinetic) {
   if (!c || !enstrophy || !kinetic) return fail(NUC3D_EINVAL, "bad argument");
   if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  for (int d = 0; d < 3; ++d)
+    if (vis_reach(c->P.vis[d]) > c->P.ts[d])
+      return fail(NUC3D_ENOTSUP,
+                  "direction %d: the velocity-gradient stencil reaches %d cells but the "
+                  "reconstruction's bufferSize is %d; the reference reads outside its arrays there",
+                  d, vis_reach(c->P.vis[d]), c->P.ts[d]);
   cudaSetDevice(c->device);
   const int nb = (int)c->blocks.size();
   if (!c->d_diag) {

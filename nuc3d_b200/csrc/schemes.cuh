@@ -28,6 +28,7 @@ __device__ constexpr double kG0 = 13.0 / 12.0;
 __device__ constexpr double kG1 = 1.0 / 4.0;
 __device__ constexpr double kCD6[3] = {3.0 / 4.0, -3.0 / 20.0, 1.0 / 60.0};
 __device__ constexpr double kCD4[2] = {2.0 / 3.0, -1.0 / 12.0};
+__device__ constexpr double kCD8[4] = {4.0 / 5.0, -1.0 / 5.0, 4.0 / 105.0, -1.0 / 280.0};
 __device__ constexpr double kCD2 = 0.5;
 
 // WENO5 candidate values and smoothness indicators (src/weno5js.cpp:75-95).
@@ -227,6 +228,13 @@ __device__ __forceinline__ double cd6(double m3, double m2, double m1, double p1
                                       double p3) {
   return kCD6[2] * (p3 - m3) + kCD6[1] * (p2 - m2) + kCD6[0] * (p1 - m1);
 }
+// centraldifference8th (src/centraldifference8th.cpp:16-52)
+__device__ __forceinline__ double cd8(double m4, double m3, double m2, double m1, double p1,
+                                      double p2, double p3, double p4) {
+  return kCD8[3] * (p4 - m4) + kCD8[2] * (p3 - m3) + kCD8[1] * (p2 - m2) + kCD8[0] * (p1 - m1);
+}
+// centraldifference2nd (src/centraldifference2nd.cpp:16-37)
+__device__ __forceinline__ double cd2(double m1, double p1) { return 0.5 * (p1 - m1); }
 __device__ __forceinline__ double bnd_second(double m1, double p1) { return kCD2 * (p1 - m1); }
 __device__ __forceinline__ double bnd_fourth(double m2, double m1, double p1, double p2) {
   return kCD4[1] * (p2 - m2) + kCD4[0] * (p1 - m1);

@@ -46,7 +46,8 @@ PHYS_DEFAULTS = {"Reynolds": 1000.0, "Mach": 0.5, "Pt": 0.72, "Gamma": 1.4, "T_r
 IO_INT = {"startStep": 0, "endStep": 100000, "saveStep": 1000, "postStep": 1, "Benchmark": 0}
 IO_DBL = {"cfl": 0.5, "tl": 0.0, "dt": 0.01}
 IO_STR = {"Binary": "yes", "Tecplot": "yes", "PostProc": "yes"}
-KNOWN_SCHEMES = ("weno5js", "weno5z", "weno7js", "crweno5", "hccs")
+KNOWN_SCHEMES = ("weno5js", "weno5z", "weno7js", "crweno5", "hccs", "hccs77", "weno3js", "upwind1st")
+KNOWN_VIS = ("cd2", "cd6", "cd8")
 
 
 def _pairs(path: Path):
@@ -63,6 +64,9 @@ def read_method(rundir: Path) -> dict:
         if m[f"scheme_{ax}_ivs"] not in KNOWN_SCHEMES:
             # the reference falls back to weno5js for unknown names (src/fieldOperator.cpp:171-174)
             m[f"scheme_{ax}_ivs"] = "weno5js"
+        if m[f"scheme_{ax}_vis"] not in KNOWN_VIS:
+            # and to cd6 for unknown viscous schemes (src/fieldOperator.cpp:298-301)
+            m[f"scheme_{ax}_vis"] = "cd6"
     return m
 
 

@@ -28,7 +28,8 @@
 #include <stdlib.h>
 #include <string.h>
 
-enum { S_WENO5JS = 0, S_WENO5Z = 1, S_WENO7JS = 2, S_CRWENO5 = 3, S_HCCS = 4 };
+enum { S_WENO5JS = 0, S_WENO5Z = 1, S_WENO7JS = 2, S_CRWENO5 = 3, S_HCCS = 4, S_WENO3JS = 5, S_UPWIND1 = 6 };
+enum { V_CD6 = 0, V_CD2 = 1, V_CD8 = 2 };
 enum { R_LF = 0, R_AUSM = 1, R_AUSMP = 2 };
 
 typedef struct {
@@ -36,8 +37,21 @@ typedef struct {
   int riemann;
   int model; /* 0 Euler3d, 1 NavierStokes3d */
   int compat;
+  int vis[3]; /* V_CD6 / V_CD2 / V_CD8 per direction (scheme_x/y/z_vis) */
   double gamma, mach, reynolds, prandtl, t_ref, t_inf, t_wall, cfl;
 } oc_config;
+
+/* bufferSize of a reconstruction scheme (src/fieldOperator.cpp:127-175) */
+static int tilesize(int sch) {
+  return (sch == S_WENO7JS || sch == S_HCCS) ? 4 : sch == S_WENO3JS ? 2 : sch == S_UPWIND1 ? 1 : 3;
+}
+/* bfsize = max of the three (src/block.cpp:506-507) */
+static int ghost_width(const oc_config *c) {
+  int m = 0;
+  for (int d = 0; d < 3; ++d)
+    if (tilesize(c->scheme[d]) > m) m = tilesize(c->scheme[d]);
+  return m;
+}
 
 typedef struct {
   int n[3];
@@ -448,6 +462,8 @@ static double face_explicit(const oc_config *c, int d, int side, int f, int L, i
       double s[5] = {P(0), P(1), P(2), P(3), P(4)};
       return weno5(s, 0, 0);
     }
+    if (sch == S_WENO3JS) return rb3(P(f - 2), P(f - 1), P(f)); /* src/weno3js.cpp:59-86 */
+    if (sch == S_UPWIND1) return P(f - 1);                     /* src/upwind1st.cpp:57-75 */
     if (sch == S_WENO7JS || sch == S_HCCS) {
       double s[7];
       for (int k = 0; k < 7; ++k) s[k] = P(f - 4 + k);
@@ -473,6 +489,8 @@ static double face_explicit(const oc_config *c, int d, int side, int f, int L, i
     double s[5] = {P(5), P(4), P(3), P(2), P(1)};
     return weno5(s, 0, 0);
   }
+  if (sch == S_WENO3JS) return rb3(P(f + 1), P(f), P(f - 1)); /* src/weno3js.cpp:88-115 */
+  if (sch == S_UPWIND1) return P(f);                         /* src/upwind1st.cpp:96-114 */
   if (sch == S_WENO7JS || sch == S_HCCS) {
     double s[7];
     for (int k = 0; k < 7; ++k) s[k] = P(f + 3 - k);
@@ -488,7 +506,7 @@ static double face_explicit(const oc_config *c, int d, int side, int f, int L, i
 static void line_faces(const oc_config *c, const oc_block *b, int d, int bfs, const double *eP,
                        const double *eN, double *face) {
   int L = b->n[d], sch = c->scheme[d];
-  int ts = (sch == S_WENO7JS || sch == S_HCCS) ? 4 : 3;
+  int ts = tilesize(sch);
   int physL = b->bc_type[2 * d] < 0, physR = b->bc_type[2 * d + 1] < 0;
   int compact = sch == S_CRWENO5 || sch == S_HCCS;
   static double hs[2][4096], ra[4096], rb[4096], rc[4096], rd[4096];
@@ -523,7 +541,9 @@ static void line_faces(const oc_config *c, const oc_block *b, int d, int bfs, co
 }
 
 /* derivative of an extended line (ghosts at [-bfs, 0) and [L, L+bfs)) at position pos */
-static double line_diff(const double *e, int bfs, int pos, int L, int ts, int physL, int physR) {
+static const double CD8[4] = {4.0 / 5.0, -1.0 / 5.0, 4.0 / 105.0, -1.0 / 280.0};
+static double line_diff(const double *e, int bfs, int pos, int L, int ts, int physL, int physR,
+                        int vis) {
 #define V(cc) e[(cc) + bfs]
   if (physR && pos >= L - ts) {
     int m = L - 1 - pos;
@@ -538,6 +558,12 @@ static double line_diff(const double *e, int bfs, int pos, int L, int ts, int ph
     if (pos == 2) return CD4[1] * (V(pos + 2) - V(pos - 2)) + CD4[0] * (V(pos + 1) - V(pos - 1));
     return CD6[2] * (V(pos + 3) - V(pos - 3)) + CD6[1] * (V(pos + 2) - V(pos - 2)) + CD4[0] * (V(pos + 1) - V(pos - 1));
   }
+  /* inside the block and at block edges with neighbour ghosts: the scheme_vis operator
+     (src/centraldifference2nd.cpp:16-37, 6th :16-183, 8th :16-52) */
+  if (vis == V_CD2) return 0.5 * (V(pos + 1) - V(pos - 1));
+  if (vis == V_CD8)
+    return CD8[3] * (V(pos + 4) - V(pos - 4)) + CD8[2] * (V(pos + 3) - V(pos - 3)) +
+           CD8[1] * (V(pos + 2) - V(pos - 2)) + CD8[0] * (V(pos + 1) - V(pos - 1));
   return CD6[2] * (V(pos + 3) - V(pos - 3)) + CD6[1] * (V(pos + 2) - V(pos - 2)) + CD6[0] * (V(pos + 1) - V(pos - 1));
 #undef V
 }
@@ -600,7 +626,7 @@ static void pass_inviscid(const oc_config *c, work_t *W, int nb, int bfs, double
 
 static void pass_viscous(const oc_config *c, work_t *W, int nb, int bfs, double *ext) {
   int ts[3];
-  for (int d = 0; d < 3; ++d) ts[d] = (c->scheme[d] == S_WENO7JS || c->scheme[d] == S_HCCS) ? 4 : 3;
+  for (int d = 0; d < 3; ++d) ts[d] = tilesize(c->scheme[d]);
   /* gradients of u, v, w, T along xi, eta, zeta (src/NaiverStokes3d.cpp:63-168) */
   for (int bi = 0; bi < nb; ++bi) {
     oc_block *b = W[bi].b;
@@ -615,7 +641,7 @@ static void pass_viscous(const oc_config *c, work_t *W, int nb, int bfs, double 
             for (int pos = 0; pos < L; ++pos) {
               int i, j, k;
               unslab(d, pos, a, bb, &i, &j, &k);
-              W[bi].grad[(comp * 3 + d) * N + cell(b, i, j, k)] = line_diff(ext, bfs, pos, L, ts[d], pl, pr);
+              W[bi].grad[(comp * 3 + d) * N + cell(b, i, j, k)] = line_diff(ext, bfs, pos, L, ts[d], pl, pr, c->vis[d]);
             }
           }
     }
@@ -677,7 +703,7 @@ static void pass_viscous(const oc_config *c, work_t *W, int nb, int bfs, double 
             for (int pos = 0; pos < L; ++pos) {
               int i, j, k;
               unslab(d, pos, a, bb, &i, &j, &k);
-              W[bi].dvis[d][(comp + 1) * N + cell(b, i, j, k)] = line_diff(ext, bfs, pos, L, ts[d], pl, pr);
+              W[bi].dvis[d][(comp + 1) * N + cell(b, i, j, k)] = line_diff(ext, bfs, pos, L, ts[d], pl, pr, c->vis[d]);
             }
           }
     }
@@ -687,9 +713,7 @@ static void pass_viscous(const oc_config *c, work_t *W, int nb, int bfs, double 
 /* One right-hand side of every block at its current q.  Returns dt_local
    (min over blocks and directions of 1/maxEigen). */
 static int eval_rhs(const oc_config *c, int nb, oc_block *blocks, work_t *W, double *dt_local) {
-  int bfs = 3;
-  for (int d = 0; d < 3; ++d)
-    if (c->scheme[d] == S_WENO7JS || c->scheme[d] == S_HCCS) bfs = 4;
+  int bfs = ghost_width(c);
   int maxL = 0;
   for (int bi = 0; bi < nb; ++bi)
     for (int d = 0; d < 3; ++d)
@@ -811,11 +835,8 @@ int oc_step(const oc_config *c, int nb, oc_block *blocks, int nsteps, double *dt
  * fields: per block NULL or 5N (w_x, w_y, w_z, 0.5|w|^2, Q). */
 int oc_diag(const oc_config *c, int nb, oc_block *blocks, double *enstrophy, double *kinetic,
             double **fields) {
-  int bfs = 3, ts[3];
-  for (int d = 0; d < 3; ++d) {
-    ts[d] = (c->scheme[d] == S_WENO7JS || c->scheme[d] == S_HCCS) ? 4 : 3;
-    if (ts[d] == 4) bfs = 4;
-  }
+  int bfs = ghost_width(c), ts[3];
+  for (int d = 0; d < 3; ++d) ts[d] = tilesize(c->scheme[d]);
   int maxL = 0;
   for (int bi = 0; bi < nb; ++bi)
     for (int d = 0; d < 3; ++d)
@@ -843,7 +864,7 @@ int oc_diag(const oc_config *c, int nb, oc_block *blocks, double *enstrophy, dou
             for (int pos = 0; pos < L; ++pos) {
               int i, j, k;
               unslab(d, pos, a, bb, &i, &j, &k);
-              W[bi].grad[(comp * 3 + d) * N + cell(b, i, j, k)] = line_diff(ext, bfs, pos, L, ts[d], pl, pr);
+              W[bi].grad[(comp * 3 + d) * N + cell(b, i, j, k)] = line_diff(ext, bfs, pos, L, ts[d], pl, pr, c->vis[d]);
             }
           }
     }

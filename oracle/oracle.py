@@ -12,14 +12,16 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_ref" / "liboracle.so"
-SCHEMES = {"weno5js": 0, "weno5z": 1, "weno7js": 2, "crweno5": 3, "hccs": 4}
+SCHEMES = {"weno5js": 0, "weno5z": 1, "weno7js": 2, "crweno5": 3, "hccs": 4, "weno3js": 5,
+           "upwind1st": 6}
+VIS = {"cd6": 0, "cd2": 1, "cd8": 2}
 RIEMANN = {"LF": 0, "AUSM": 1, "AUSMp": 2}
 MODELS = {"Euler3d": 0, "NavierStokes3d": 1}
 
 
 class OcConfig(ctypes.Structure):
     _fields_ = [("scheme", ctypes.c_int * 3), ("riemann", ctypes.c_int), ("model", ctypes.c_int),
-                ("compat", ctypes.c_int)] + [
+                ("compat", ctypes.c_int), ("vis", ctypes.c_int * 3)] + [
         (k, ctypes.c_double) for k in ("gamma", "mach", "reynolds", "prandtl", "t_ref", "t_inf",
                                        "t_wall", "cfl")]
 
@@ -72,10 +74,11 @@ def metrics(x, y, z) -> dict:
 class Run:
     """A set of blocks (metrics, BCs, state) advanced by the restatement."""
 
-    def __init__(self, scheme, riemann, model, params, cfl=0.5, compat=True):
+    def __init__(self, scheme, riemann, model, params, cfl=0.5, compat=True, vis=("cd6",) * 3):
         c = OcConfig()
         for d in range(3):
             c.scheme[d] = SCHEMES[scheme[d]]
+            c.vis[d] = VIS[vis[d]]
         c.riemann, c.model, c.compat = RIEMANN[riemann], MODELS[model], int(compat)
         c.gamma, c.mach, c.reynolds = params["Gamma"], params["Mach"], params["Reynolds"]
         c.prandtl, c.t_ref, c.t_inf = params["Pt"], params["T_ref"], params["T_inf"]

@@ -31,6 +31,12 @@ def names():
     return sorted(p.stem for p in GOLDEN.glob("*.npz"))
 
 
+def diag_names():
+    """Cases with a diagnostics fixture (not the ones whose reference diagnostics read
+    outside the field: low-order schemes with cd6)."""
+    return sorted(p.name[:-4] for p in (GOLDEN / "diag").glob("*.npz") if p.name.count(".") == 1)
+
+
 def load_diag(name: str) -> dict:
     """postproc::solveQ of the case's state after its n steps (golden/diag/<name>.npz)."""
     z = np.load(GOLDEN / "diag" / f"{name}.npz")
@@ -77,10 +83,15 @@ def bc_arrays(g: Golden, self_index: int = 0):
     return types, ids, vals
 
 
+def vis(g: Golden) -> tuple:
+    """scheme_x/y/z_vis of the case (cd6 unless the case names others)."""
+    return tuple(g.cfg.get("vis", ("cd6",) * 3))
+
+
 def nuc3d_config(g: Golden, exact: bool = True):
     import nuc3d_b200 as nb
     p = g.cfg["params"]
-    return nb.Config(scheme_ivs=tuple(g.cfg["schemes"]), riemann=g.cfg["riemann"],
+    return nb.Config(scheme_ivs=tuple(g.cfg["schemes"]), scheme_vis=vis(g), riemann=g.cfg["riemann"],
                      model=g.cfg["model"], reynolds=p["Reynolds"], mach=p["Mach"],
                      prandtl=p["Pt"], gamma=p["Gamma"], t_ref=p["T_ref"], t_inf=p["T_inf"],
                      t_wall=p["T_wall"], cfl=0.5, exact=exact, weno5z_compat=True)

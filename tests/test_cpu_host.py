@@ -52,3 +52,27 @@ def test_golden_fixtures_consistent():
         if "libm_max_rel_diff" in g.data:
             # hccs weights (eps 1e-40) amplify glibc pow rounding the most: 7e-12
             assert g.libm_max_rel_diff[0] < 1e-10
+
+
+@pytest.mark.parametrize("ivs,vis,code", [
+    (("weno3js",) * 3, ("cd6",) * 3, 5),              # cd6 reaches 3 > bufferSize 2
+    (("upwind1st", "weno5js", "weno5js"), ("cd2",) * 3, None),  # cd2 reaches 1: allowed
+    (("weno5js",) * 3, ("cd8", "cd6", "cd6"), 5),     # cd8 reaches 4 > bufferSize 3
+    (("hccs77",) * 3, ("cd6",) * 3, 5),               # not implemented
+    (("weno5js",) * 3, ("cd4",) * 3, 1),              # unknown name
+])
+def test_create_rejects_undefined_viscous_pairs(ivs, vis, code):
+    """Navier-Stokes contexts whose viscous stencil reaches past the reconstruction's
+    bufferSize are refused (the reference reads outside its arrays there); the check runs
+    before any CUDA call, so it holds on a machine without a GPU."""
+    import nuc3d_b200 as nb
+    lib = nb.load_library()
+    cfg = nb.Config(scheme_ivs=ivs, scheme_vis=vis, model="NavierStokes3d")._c()
+    ctx = ctypes.c_void_p()
+    rc = lib.nuc3d_create(ctypes.byref(cfg), 0, ctypes.byref(ctx))
+    if code is None:
+        assert rc != 5 and rc != 1, lib.nuc3d_last_error()
+        if rc == 0:
+            lib.nuc3d_destroy(ctx)
+    else:
+        assert rc == code, (rc, lib.nuc3d_last_error())

@@ -9,7 +9,8 @@ from tests import golden_cases as G
 
 
 def oracle_run(g):
-    r = O.Run(g.cfg["schemes"], g.cfg["riemann"], g.cfg["model"], g.cfg["params"])
+    r = O.Run(g.cfg["schemes"], g.cfg["riemann"], g.cfg["model"], g.cfg["params"],
+              vis=G.vis(g))
     t, i, v = G.bc_arrays(g)
     r.add_block(O.metrics(*G.nodes(g)), t, i, v, g.q0)
     return r
@@ -45,10 +46,10 @@ def test_oracle_steps_bitwise(name):
     assert np.array_equal(dt, g.dt) and t == g.time[-1]
 
 
-@pytest.mark.parametrize("name", G.names())
+@pytest.mark.parametrize("name", G.diag_names())
 def test_oracle_diag_bitwise(name):
     g, d = G.load(name), G.load_diag(name)
-    r = O.Run(g.cfg["schemes"], g.cfg["riemann"], g.cfg["model"], g.cfg["params"])
+    r = O.Run(g.cfg["schemes"], g.cfg["riemann"], g.cfg["model"], g.cfg["params"], vis=G.vis(g))
     t, i, v = G.bc_arrays(g)
     r.add_block(O.metrics(*G.nodes(g)), t, i, v, g.qn)
     ens, kin, f = r.diag()

@@ -21,7 +21,7 @@ def _state_solver(g, exact):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", G.names())
+@pytest.mark.parametrize("name", G.diag_names())
 def test_diag_bitwise(name):
     g, d = G.load(name), G.load_diag(name)
     s = _state_solver(g, True)
@@ -34,7 +34,7 @@ def test_diag_bitwise(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", G.names())
+@pytest.mark.parametrize("name", G.diag_names())
 def test_diag_fast_roundoff(name):
     g, d = G.load(name), G.load_diag(name)
     s = _state_solver(g, False)
@@ -79,3 +79,14 @@ def test_diag_taylor_green_initial_energy():
     ens, kin = s.diagnostics()
     assert abs(kin / n - 0.125) < 1e-12
     assert abs(ens / n - 0.375) < 5e-3
+
+
+@pytest.mark.gpu
+def test_diag_refuses_undefined_gradient_stencil():
+    """weno3js (bufferSize 2) with the default cd6 gradients: the reference's diagnostics
+    read outside its rows, so the library refuses with NUC3D_ENOTSUP."""
+    import nuc3d_b200 as nb
+    s = G.solver(G.load("weno3js_euler_lf_bc"), exact=True)
+    with pytest.raises(nb.Nuc3dError) as e:
+        s.diagnostics()
+    assert e.value.code == 5
