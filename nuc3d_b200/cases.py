@@ -6,6 +6,8 @@ No dataset is involved: every state is generated from a formula.
                         outlet (extrapolation) faces; the reference has no initialiser
                         for it, so the state is injected like its restart file
                         (src/block.cpp:785-816)
+  * isotropic_turbulence + uneven_blocks -- decaying isotropic turbulence in a periodic
+                        2 pi box cut into blocks of uneven sizes (seeded), injected the same way
 Uniform boxes get analytic metrics (xi_x = 1/hx, jac = 1/(hx hy hz)); curvilinear
 meshes go through nuc3d_b200.metrics (block::getJacobians).
 """
@@ -77,3 +79,70 @@ def outlet_faces():
 
 def periodic_faces(block=0):
     return [block] * 6, list(PERIODIC_NEIGHBOUR_FACE)
+
+
+def isotropic_turbulence(shape, seed=0, k0=4.0, mt=0.6, gamma=1.4, re_lambda=100.0):
+    """Seeded random-phase solenoidal velocity on the periodic [0, 2 pi]^3 box of
+    shape = (nx, ny, nz) cells, energy spectrum E(k) ~ k^4 exp(-2 (k/k0)^2), rho = T = 1.
+
+    Nondimensionalised as the reference (T = gamma Ma^2 p / rho): with the reference Mach
+    number Ma = mt and the velocity scaled to rms |u| = 1 the sound speed is 1/mt, so the
+    turbulent Mach number is mt.  Returns (prim (5, nz, ny, nx), reynolds) where reynolds
+    is the reference's Reynolds number that gives Taylor-scale Reynolds number re_lambda
+    (mu(T = 1) = 1/Re under Sutherland's law)."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng(seed)
+    kz = np.fft.fftfreq(nz, 1.0 / nz)[:, None, None]
+    ky = np.fft.fftfreq(ny, 1.0 / ny)[None, :, None]
+    kx = np.fft.fftfreq(nx, 1.0 / nx)[None, None, :]
+    k2 = kx * kx + ky * ky + kz * kz
+    k = np.sqrt(k2)
+    amp = np.where(k > 0, np.sqrt(k ** 4 * np.exp(-2.0 * (k / k0) ** 2) / np.maximum(k2, 1.0)), 0.0)
+    # no Nyquist modes: their real part has no conjugate partner to stay solenoidal with
+    amp = np.where((np.abs(kx) == nx // 2) | (np.abs(ky) == ny // 2) | (np.abs(kz) == nz // 2), 0.0, amp)
+    comps = []
+    for _ in range(3):
+        ph = rng.uniform(0.0, 2.0 * np.pi, k.shape)
+        comps.append(amp * (rng.standard_normal(k.shape)) * np.exp(1j * ph))
+    # solenoidal projection: u_hat - k (k . u_hat) / k^2
+    kd = (kx * comps[0] + ky * comps[1] + kz * comps[2]) / np.maximum(k2, 1.0)
+    uh = [comps[0] - kx * kd, comps[1] - ky * kd, comps[2] - kz * kd]
+    vel = [np.real(np.fft.ifftn(c)) for c in uh]
+    scale = 1.0 / np.sqrt(np.mean(vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2))
+    u, v, w = (scale * a for a in vel)
+    # Taylor scale from the spectral derivative of u along x
+    dudx = np.real(np.fft.ifftn(1j * kx * np.fft.fftn(u)))
+    urms = np.sqrt(np.mean(u * u))
+    lam = urms / np.sqrt(np.mean(dudx * dudx))
+    rho = np.ones_like(u)
+    p = rho / (gamma * mt * mt)
+    return np.stack([rho, u, v, w, p]), re_lambda / (urms * lam)
+
+
+def uneven_blocks(nblocks=(2, 3, 4), sizes=(48, 64, 96, 128, 160), seed=0):
+    """Per-axis block sizes of a tensor-product partition, drawn with a fixed seed
+    (neighbouring faces match, as the reference's buffers require:
+    src/bufferData.cpp:16-47).  Returns [sizes along x, along y, along z]."""
+    rng = np.random.default_rng(seed)
+    return [[int(s) for s in rng.choice(sizes, size=n)] for n in nblocks]
+
+
+def block_topology(parts):
+    """Blocks of a periodic tensor-product partition, x fastest: for block (a, b, c) the
+    BC_Topo face types (neighbour block index) and ids (neighbour face)."""
+    na, nb, nc = (len(p) for p in parts)
+    idx = lambda a, b, c: a + na * (b + nb * c)  # noqa: E731
+    types, ids = [], []
+    for c in range(nc):
+        for b in range(nb):
+            for a in range(na):
+                pos, n = [a, b, c], [na, nb, nc]
+                t = []
+                for f in range(6):
+                    d, side = f // 2, f % 2
+                    q = list(pos)
+                    q[d] = (q[d] + (1 if side else -1)) % n[d]
+                    t.append(idx(*q))
+                types.append(t)
+                ids.append(list(PERIODIC_NEIGHBOUR_FACE))
+    return types, ids

@@ -72,3 +72,25 @@ def test_oracle_diag_two_blocks_bitwise():
     ens, kin, f = r.diag()
     assert ens == d["enstrophy"][0] and kin == d["kinetic"][0]
     assert np.array_equal(np.concatenate(f, axis=-1), d["fields"])
+
+
+def test_oracle_uneven_blocks_bitwise():
+    """24 uneven blocks of decaying turbulence (tests/test_gpu_multiblock_turbulence.py):
+    the restatement against the reference run as 24 ranks, 3 steps."""
+    from oracle import refrun as R
+    from tests import test_gpu_multiblock_turbulence as T
+    if not (R.REF_BIN_DIR / "nuc3d_ref_taps").exists():
+        pytest.skip("reference binaries not built (make -C oracle ref)")
+    blocks, types, ids, params = T._setup()
+    topo = [[f"{types[r][f]} {ids[r][f]}" for f in range(6)] for r in range(len(blocks))]
+    ref = R.Case(model="NavierStokes3d", riemann="AUSM", schemes=("weno5z",) * 3, params=params,
+                 nodes=[b["nodes"] for b in blocks], bc_topo=topo, q0=[b["q"] for b in blocks],
+                 start_step=1)
+    out = R.run(ref, "steps", T.STEPS, timeout=1200)
+    r = O.Run(("weno5z",) * 3, "AUSM", "NavierStokes3d", params)
+    for i, b in enumerate(blocks):
+        r.add_block(O.metrics(*b["nodes"]), types[i], ids[i], None, b["q"])
+    dt, t = r.step(T.STEPS)
+    assert np.array_equal(dt, out[0]["dt"])
+    for i in range(len(blocks)):
+        assert np.array_equal(r.q(i), R.stack(out[i], "Q", 5)), i
