@@ -960,6 +960,29 @@ __device__ __forceinline__ double prim_along(const BlockDev *__restrict__ blocks
   return __ldg(blocks[nb].prim + comp * blocks[nb].N + nidx);
 }
 
+// d/d(direction d) of primitive components c0 .. c0+nc-1 of cell (i,j,k) near a block
+// face: neighbour ghosts and the physical-face schemes.  Out of line, so that the
+// kernels' common path (all stencil cells inside the block) stays small.
+__device__ __noinline__ void prim_grad_edge(const BlockDev *__restrict__ blocks, const BlockDev &B,
+                                            const SolverParams &P, int d, int i, int j, int k,
+                                            int c0, int nc, double *out) {
+  const int pos = d == 0 ? i : (d == 1 ? j : k);
+  const bool pl = B.face[2 * d].type < 0, pr = B.face[2 * d + 1].type < 0;
+  for (int c = 0; c < nc; ++c) {
+    auto V = [&](int g) { return prim_along(blocks, B, d, i, j, k, g, c0 + c, P.bfs); };
+    out[c] = diff_at(pos, B.n[d], P.ts[d], pl, pr, P.vis[d], V);
+  }
+}
+
+// The direction's scheme_vis operator on a field with stride s from cell pointer f
+// (every stencil cell inside the block).
+__device__ __forceinline__ double diff_inner(const double *__restrict__ f, long long s, int vis) {
+  auto V = [&](int o) { return __ldg(f + o * s); };
+  if (vis == VIS_CD2) return cd2(V(-1), V(1));
+  if (vis == VIS_CD8) return cd8(V(-4), V(-3), V(-2), V(-1), V(1), V(2), V(3), V(4));
+  return cd6(V(-3), V(-2), V(-1), V(1), V(2), V(3));
+}
+
 // NaiverStokesData3d::solveGrads + solveViscousFlux (src/NaiverStokes3d.cpp:63-326)
 // with physicsModel::sutherland (src/physicsModel.cpp:199-234).
 __global__ void __launch_bounds__(kCellTile)
@@ -972,14 +995,19 @@ grad_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P) {
   const int nx = B.n[0], ny = B.n[1];
   const int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((long long)nx * ny));
   const int pos[3] = {i, j, k};
+  const long long stride[3] = {1, nx, (long long)nx * ny};
   double gr[4][3];  // [u,v,w,T][xi,eta,zeta]
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const bool pl = B.face[2 * d].type < 0, pr = B.face[2 * d + 1].type < 0;
+    // one-sided schemes within ts of a physical face, ghosts within reach <= ts of any face
+    if (pos[d] >= P.ts[d] && pos[d] < B.n[d] - P.ts[d]) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      auto V = [&](int g) { return prim_along(blocks, B, d, i, j, k, g, c, P.bfs); };
-      gr[c][d] = diff_at(pos[d], B.n[d], P.ts[d], pl, pr, P.vis[d], V);
+      for (int c = 0; c < 4; ++c) gr[c][d] = diff_inner(B.prim + c * N + idx, stride[d], P.vis[d]);
+    } else {
+      double g4[4];
+      prim_grad_edge(blocks, B, P, d, i, j, k, 0, 4, g4);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) gr[c][d] = g4[c];
     }
   }
   const double jac = __ldg(B.jac + idx);
@@ -1080,6 +1108,18 @@ __device__ __forceinline__ double diag_prim_along(const BlockDev *__restrict__ b
   return __ldg(dd[nb].prim + comp * blocks[nb].N + nidx);
 }
 
+__device__ __noinline__ void diag_grad_edge(const BlockDev *__restrict__ blocks,
+                                            const DiagDev *__restrict__ dd, const SolverParams &P,
+                                            int b, int d, int i, int j, int k, double *out) {
+  const BlockDev &B = blocks[b];
+  const int pos = d == 0 ? i : (d == 1 ? j : k);
+  const bool pl = B.face[2 * d].type < 0, pr = B.face[2 * d + 1].type < 0;
+  for (int c = 0; c < 3; ++c) {
+    auto V = [&](int g) { return diag_prim_along(blocks, dd, b, d, i, j, k, g, c + 1, P.bfs); };
+    out[c] = diff_at(pos, B.n[d], P.ts[d], pl, pr, P.vis[d], V);
+  }
+}
+
 __global__ void __launch_bounds__(kCellTile)
 diag_kernel(const BlockDev *__restrict__ blocks, const DiagDev *__restrict__ dd, TileMap tm,
             SolverParams P) {
@@ -1091,14 +1131,19 @@ diag_kernel(const BlockDev *__restrict__ blocks, const DiagDev *__restrict__ dd,
   const int nx = B.n[0], ny = B.n[1];
   const int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((long long)nx * ny));
   const int pos[3] = {i, j, k};
+  const long long stride[3] = {1, nx, (long long)nx * ny};
   double gr[3][3];  // [u,v,w][xi,eta,zeta]
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const bool pl = B.face[2 * d].type < 0, pr = B.face[2 * d + 1].type < 0;
+    if (pos[d] >= P.ts[d] && pos[d] < B.n[d] - P.ts[d]) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      auto V = [&](int g) { return diag_prim_along(blocks, dd, b, d, i, j, k, g, c + 1, P.bfs); };
-      gr[c][d] = diff_at(pos[d], B.n[d], P.ts[d], pl, pr, P.vis[d], V);
+      for (int c = 0; c < 3; ++c)
+        gr[c][d] = diff_inner(dd[b].prim + (c + 1) * N + idx, stride[d], P.vis[d]);
+    } else {
+      double g3[3];
+      diag_grad_edge(blocks, dd, P, b, d, i, j, k, g3);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) gr[c][d] = g3[c];
     }
   }
   double mx[3][3];
