@@ -13,6 +13,7 @@
  *                           physicsModel (src/physicsModel.cpp:13-112, PhysModel.in)
  *   nuc3d_block_add         block::initial's per-rank block + BC_Topo
  *                           (src/block.cpp:31-100, src/boundaryConditions.cpp:25-93)
+ *   nuc3d_block_set_nodes   block::getJacobians on the GPU (src/block.cpp:237-477)
  *   nuc3d_block_set_metrics block::getJacobians output (src/block.cpp:237-325):
  *                           EulerData3D::jacobian, xi_xyz, eta_xyz, zeta_xyz, dx, dy, dz
  *                           (src/euler3d.h:38-46)
@@ -93,6 +94,18 @@ int nuc3d_block_add(nuc3d_ctx *ctx, int nx, int ny, int nz, const int bc_type[6]
    only by symmetry faces, may be NULL otherwise. */
 int nuc3d_block_set_metrics(nuc3d_ctx *ctx, int block, const double *jac, const double *xi_xyz,
                             const double *eta_xyz, const double *zeta_xyz, const double *dxyz);
+
+/* Metrics computed on the GPU from the block's node coordinates: block::getJacobians
+   (src/block.cpp:237-325) with its tile-Lagrange derivatives (:327-477).  x, y, z: host
+   arrays of (nx+1)(ny+1)(nz+1) nodes, i fastest (mesh_<r>.x, src/block.cpp:42-81); cells
+   per axis must be multiples of 4, as in the reference.  Bitwise the reference's metrics;
+   a negative Jacobian returns NUC3D_EINVAL (the reference exits). */
+int nuc3d_block_set_nodes(nuc3d_ctx *ctx, int block, const double *x, const double *y,
+                          const double *z);
+/* Copy a block's metrics back (any pointer may be NULL; dxyz exists for blocks with a
+   symmetry face or when given to nuc3d_block_set_metrics). */
+int nuc3d_block_get_metrics(nuc3d_ctx *ctx, int block, double *jac, double *xi_xyz,
+                            double *eta_xyz, double *zeta_xyz, double *dxyz);
 
 /* Validate the block topology and upload the descriptors.  Call once, after all
    blocks are added and before any evaluation. */

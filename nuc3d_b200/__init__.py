@@ -37,6 +37,7 @@ EXPORTED = (
     "nuc3d_get_time", "nuc3d_set_time", "nuc3d_get_status", "nuc3d_set_stream",
     "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis", "nuc3d_profile_sweep",
     "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step", "nuc3d_diagnostics", "nuc3d_block_get_diag",
+    "nuc3d_block_set_nodes", "nuc3d_block_get_metrics",
 )
 
 
@@ -111,6 +112,8 @@ def load_library() -> ctypes.CDLL:
     PI = ctypes.POINTER(I)
     lib.nuc3d_kernels_per_step.argtypes = [P, PI]
     lib.nuc3d_diagnostics.argtypes = [P, PD, PD]
+    lib.nuc3d_block_set_nodes.argtypes = [P, I, PD, PD, PD]
+    lib.nuc3d_block_get_metrics.argtypes = [P, I, PD, PD, PD, PD, PD]
     lib.nuc3d_block_get_diag.argtypes = [P, I, PD]
     lib.nuc3d_rhs_noalloc.argtypes = [ctypes.POINTER(_Cfg), I, I, I, I, PI, PI, PD, P, P, P, P,
                                       P, P, P, PD, P]
@@ -216,6 +219,21 @@ class Solver:
         m = metrics_from_nodes(x, y, z)
         self.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
         return m
+
+    def set_nodes(self, b, x, y, z) -> None:
+        """Metrics of block b computed on the GPU from its node coordinates
+        (block::getJacobians; bitwise the host set_mesh)."""
+        arrs = [_f64(a) for a in (x, y, z)]
+        _check(self.lib.nuc3d_block_set_nodes(self._ctx, b, *[_pd(a) for a in arrs]))
+
+    def get_metrics(self, b) -> dict:
+        nx, ny, nz = self.blocks[b]
+        sh = (nz, ny, nx)
+        out = {"jac": np.empty(sh), "xi_xyz": np.empty((3,) + sh), "eta_xyz": np.empty((3,) + sh),
+               "zeta_xyz": np.empty((3,) + sh)}
+        _check(self.lib.nuc3d_block_get_metrics(self._ctx, b, *[_pd(out[k]) for k in
+                                                ("jac", "xi_xyz", "eta_xyz", "zeta_xyz")], None))
+        return out
 
     def finalize(self) -> None:
         _check(self.lib.nuc3d_finalize(self._ctx))

@@ -146,11 +146,15 @@ void set_error_message(const char *msg);
 
 // configure(): one-time kernel attributes (dynamic shared memory opt-in).
 // tile_count(): CTAs of the dir-sweep over one block of n cells.
+// run_metrics(): block::getJacobians of an nx x ny x nz block from its node coordinates
+// ((n+1) per axis, device arrays); *bad gets 1 for a negative Jacobian.
 // run_diag(): the solveQ diagnostics of state q[0] of every block into dd[b] and the
 // per-block totals sums[2b] (enstrophy), sums[2b+1] (kinetic energy); parts holds
 // 2 * kDiagParts doubles per block of scratch.
 namespace exact {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_metrics(const double *x, const double *y, const double *z, const int n[3],
+                        double *jac, double *met, double *dxyz, unsigned *bad, cudaStream_t st);
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 cudaError_t configure();
@@ -158,6 +162,8 @@ int tile_count(int dir, const int n[3]);
 }
 namespace fast {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_metrics(const double *x, const double *y, const double *z, const int n[3],
+                        double *jac, double *met, double *dxyz, unsigned *bad, cudaStream_t st);
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 cudaError_t configure();

@@ -1254,6 +1254,87 @@ __global__ void diag_sum_parts_kernel(int nblocks, const double *__restrict__ pa
 }
 
 // ---------------------------------------------------------------------------------
+// Metrics: block::getJacobians (src/block.cpp:237-325) from the node coordinates, with the
+// tile-Lagrange reconstruction of the derivatives (interpolation_derlag :327-477,
+// coefficients src/block.h:36-48): every cell sums the 5x5x5 nodes of its 4x4x4-cell tile,
+// xi innermost, then eta, then zeta, each sum from 0.0, as the reference does.
+// ---------------------------------------------------------------------------------
+__device__ constexpr double kLag[4][5] = {
+    {35.0 / 128.0, 35.0 / 32.0, -35.0 / 64.0, 7.0 / 32.0, -5.0 / 128.0},
+    {-5.0 / 128.0, 15.0 / 32.0, 45.0 / 64.0, -5.0 / 32.0, 3.0 / 128.0},
+    {3.0 / 128.0, -5.0 / 32.0, 45.0 / 64.0, 15.0 / 32.0, -5.0 / 128.0},
+    {-5.0 / 128.0, 7.0 / 32.0, -35.0 / 64.0, 35.0 / 32.0, 35.0 / 128.0}};
+__device__ constexpr double kDerLag[4][5] = {
+    {-11.0 / 12.0, 17.0 / 24.0, 3.0 / 8.0, -5.0 / 24.0, 1.0 / 24.0},
+    {1.0 / 24.0, -9.0 / 8.0, 9.0 / 8.0, -1.0 / 24.0, 0.0},
+    {0.0, 1.0 / 24.0, -9.0 / 8.0, 9.0 / 8.0, -1.0 / 24.0},
+    {-1.0 / 24.0, 5.0 / 24.0, -3.0 / 8.0, -17.0 / 24.0, 11.0 / 12.0}};
+
+// d(f)/d(xi, eta, zeta) of one coordinate f at cell (i,j,k): out[d]
+__device__ __forceinline__ void tile_derivs(const double *__restrict__ f, int nx0, int ny0, int i,
+                                            int j, int k, double out[3]) {
+  const int ti = i & ~3, tj = j & ~3, tk = k & ~3, ai = i & 3, aj = j & 3, ak = k & 3;
+  double vz[3] = {0.0, 0.0, 0.0};
+  for (int kk = 0; kk < 5; ++kk) {
+    double vy[3] = {0.0, 0.0, 0.0};
+    for (int jj = 0; jj < 5; ++jj) {
+      const double *row = f + ((long long)(tk + kk) * ny0 + (tj + jj)) * nx0 + ti;
+      double vxd = 0.0, vxl = 0.0;  // DERLAG and LAG along xi
+      for (int ii = 0; ii < 5; ++ii) {
+        const double v = __ldg(row + ii);
+        vxd = vxd + kDerLag[ai][ii] * v;
+        vxl = vxl + kLag[ai][ii] * v;
+      }
+      vy[0] = vy[0] + kLag[aj][jj] * vxd;     // d/dxi:   DERLAG, LAG, LAG
+      vy[1] = vy[1] + kDerLag[aj][jj] * vxl;  // d/deta:  LAG, DERLAG, LAG
+      vy[2] = vy[2] + kLag[aj][jj] * vxl;     // d/dzeta: LAG, LAG, DERLAG
+    }
+    vz[0] = vz[0] + kLag[ak][kk] * vy[0];
+    vz[1] = vz[1] + kLag[ak][kk] * vy[1];
+    vz[2] = vz[2] + kDerLag[ak][kk] * vy[2];
+  }
+  out[0] = vz[0];
+  out[1] = vz[1];
+  out[2] = vz[2];
+}
+
+__global__ void __launch_bounds__(256)
+metrics_kernel(const double *__restrict__ x, const double *__restrict__ y,
+               const double *__restrict__ z, int nx, int ny, int nz, double *__restrict__ jac,
+               double *__restrict__ met, double *__restrict__ dxyz, unsigned *__restrict__ bad) {
+  const long long N = (long long)nx * ny * nz;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((long long)nx * ny));
+  double dx[3], dy[3], dz[3];
+  tile_derivs(x, nx + 1, ny + 1, i, j, k, dx);
+  tile_derivs(y, nx + 1, ny + 1, i, j, k, dy);
+  tile_derivs(z, nx + 1, ny + 1, i, j, k, dz);
+  const double x_xi = dx[0], x_eta = dx[1], x_zeta = dx[2];
+  const double y_xi = dy[0], y_eta = dy[1], y_zeta = dy[2];
+  const double z_xi = dz[0], z_eta = dz[1], z_zeta = dz[2];
+  const double jacob = 1.0 / (x_xi * (y_eta * z_zeta - y_zeta * z_eta) +
+                              x_eta * (y_zeta * z_xi - y_xi * z_zeta) +
+                              x_zeta * (y_xi * z_eta - y_eta * z_xi));
+  if (jacob < 0.0) atomicOr(bad, 1u);  // the reference exits (src/block.cpp:314-318)
+  jac[idx] = jacob;
+  met[idx] = (y_eta * z_zeta - y_zeta * z_eta) * jacob;
+  met[N + idx] = (x_zeta * z_eta - x_eta * z_zeta) * jacob;
+  met[2 * N + idx] = (x_eta * y_zeta - x_zeta * y_eta) * jacob;
+  met[3 * N + idx] = (y_zeta * z_xi - y_xi * z_zeta) * jacob;
+  met[4 * N + idx] = (x_xi * z_zeta - x_zeta * z_xi) * jacob;
+  met[5 * N + idx] = (x_zeta * y_xi - x_xi * y_zeta) * jacob;
+  met[6 * N + idx] = (y_xi * z_eta - y_eta * z_xi) * jacob;
+  met[7 * N + idx] = (x_eta * z_xi - x_xi * z_eta) * jacob;
+  met[8 * N + idx] = (x_xi * y_eta - x_eta * y_xi) * jacob;
+  if (dxyz) {
+    const double d9[9] = {x_xi, x_eta, x_zeta, y_xi, y_eta, y_zeta, z_xi, z_eta, z_zeta};
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dxyz[c * N + idx] = d9[c];
+  }
+}
+
+// ---------------------------------------------------------------------------------
 // Host-side launchers (called by the C-ABI layer).
 // ---------------------------------------------------------------------------------
 template <int DIR, int SCH>
@@ -1334,6 +1415,14 @@ inline cudaError_t launch_stage(const Launch &L, int stage, bool rk, bool eig) {
 
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig) {
   return launch_stage(L, stage, rk, eig);
+}
+
+cudaError_t run_metrics(const double *x, const double *y, const double *z, const int n[3],
+                        double *jac, double *met, double *dxyz, unsigned *bad, cudaStream_t st) {
+  const long long N = (long long)n[0] * n[1] * n[2];
+  metrics_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(x, y, z, n[0], n[1], n[2], jac, met,
+                                                              dxyz, bad);
+  return cudaGetLastError();
 }
 
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts) {

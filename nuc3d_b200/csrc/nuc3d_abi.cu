@@ -311,6 +311,64 @@ int nuc3d_block_set_metrics(nuc3d_ctx *c, int bi, const double *jac, const doubl
   return NUC3D_OK;
 }
 
+int nuc3d_block_set_nodes(nuc3d_ctx *c, int bi, const double *x, const double *y,
+                          const double *z) {
+  if (!c || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad block index");
+  if (!x || !y || !z) return fail(NUC3D_EINVAL, "null node array");
+  HostBlock &b = c->blocks[bi];
+  for (int d = 0; d < 3; ++d)
+    if (b.n[d] % 4)
+      return fail(NUC3D_EINVAL, "the reference's tile-Lagrange metrics need cells per axis to be "
+                  "a multiple of 4 (block %d axis %d has %d)", bi, d, b.n[d]);
+  bool symm = false;
+  for (int f = 0; f < 6; ++f) symm = symm || (b.bc_type[f] == -1 && b.bc_id[f] == BC_SYMM);
+  const size_t nn = (size_t)(b.n[0] + 1) * (b.n[1] + 1) * (b.n[2] + 1) * sizeof(double);
+  const size_t nb = (size_t)b.N * sizeof(double);
+  cudaSetDevice(c->device);
+  if (symm && !b.dxyz) CUDA_TRY(cudaMalloc(&b.dxyz, 9 * nb));
+  double *nodes = nullptr;
+  unsigned *bad = nullptr;
+  CUDA_TRY(cudaMalloc(&nodes, 3 * nn + 256));
+  cudaError_t e = cudaSuccess;
+  unsigned h_bad = 0;
+  bad = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(nodes) + 3 * nn);
+  const double *src[3] = {x, y, z};
+  for (int a = 0; a < 3 && e == cudaSuccess; ++a)
+    e = cudaMemcpy(reinterpret_cast<char *>(nodes) + a * nn, src[a], nn, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(bad, 0, sizeof(unsigned));
+  if (e == cudaSuccess) {
+    const double *dx = nodes, *dy = reinterpret_cast<const double *>(reinterpret_cast<char *>(nodes) + nn),
+                 *dz = reinterpret_cast<const double *>(reinterpret_cast<char *>(nodes) + 2 * nn);
+    e = nuc3d::exact::run_metrics(dx, dy, dz, b.n, b.jac, b.met, symm ? b.dxyz : nullptr, bad,
+                                  nullptr);
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(&h_bad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  cudaFree(nodes);
+  if (e != cudaSuccess) return fail(NUC3D_ECUDA, "metrics: %s", cudaGetErrorString(e));
+  if (h_bad) return fail(NUC3D_EINVAL, "block %d: negative Jacobian (the reference exits)", bi);
+  b.metrics = true;
+  return NUC3D_OK;
+}
+
+int nuc3d_block_get_metrics(nuc3d_ctx *c, int bi, double *jac, double *xi_xyz, double *eta_xyz,
+                            double *zeta_xyz, double *dxyz) {
+  if (!c || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad block index");
+  HostBlock &b = c->blocks[bi];
+  if (!b.metrics) return fail(NUC3D_ESTATE, "block %d has no metrics", bi);
+  const size_t nb = (size_t)b.N * sizeof(double);
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (jac) CUDA_TRY(cudaMemcpy(jac, b.jac, nb, cudaMemcpyDeviceToHost));
+  if (xi_xyz) CUDA_TRY(cudaMemcpy(xi_xyz, b.met, 3 * nb, cudaMemcpyDeviceToHost));
+  if (eta_xyz) CUDA_TRY(cudaMemcpy(eta_xyz, b.met + 3 * b.N, 3 * nb, cudaMemcpyDeviceToHost));
+  if (zeta_xyz) CUDA_TRY(cudaMemcpy(zeta_xyz, b.met + 6 * b.N, 3 * nb, cudaMemcpyDeviceToHost));
+  if (dxyz) {
+    if (!b.dxyz) return fail(NUC3D_ESTATE, "block %d has no dxyz metrics", bi);
+    CUDA_TRY(cudaMemcpy(dxyz, b.dxyz, 9 * nb, cudaMemcpyDeviceToHost));
+  }
+  return NUC3D_OK;
+}
+
 int nuc3d_finalize(nuc3d_ctx *c) {
   if (!c) return fail(NUC3D_EINVAL, "null context");
   if (c->finalized) return fail(NUC3D_ESTATE, "already finalized");

@@ -202,15 +202,20 @@ def run(rundir, steps: int | None = None, exact: bool = True, quiet: bool = Fals
     meshes = sorted(rundir.glob("mesh/mesh_*.x"), key=lambda p: int(p.stem.split("_")[1]))
     s = Solver(cfg)
     shapes, metrics = [], []
+    start = io["startStep"]
     for r, mp in enumerate(meshes):
         x, y, z = read_mesh(mp)
         t, i, v = read_bc_topo(rundir / f"bc_topo/BC_Topo_{r}.in")
         nz, ny, nx = (d - 1 for d in x.shape)
         b = s.add_block(nx, ny, nz, t, i, v)
-        metrics.append(s.set_mesh(b, x, y, z))
+        symm = any(tt == -1 and ii == 3 for tt, ii in zip(t, i))
+        if start > 0 and not symm:
+            s.set_nodes(b, x, y, z)           # metrics on the GPU
+            metrics.append(None)
+        else:                                  # cell centres (initial state) or dxyz needed
+            metrics.append(s.set_mesh(b, x, y, z))
         shapes.append((nz, ny, nx))
     s.finalize()
-    start = io["startStep"]
     t0 = 0.0
     for r, sh in enumerate(shapes):
         if start > 0:
