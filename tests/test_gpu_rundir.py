@@ -60,5 +60,16 @@ def test_run_directory_restart_files_identical(multi):
         a = (ref / "enstrophy.dat").read_text()
         b = (tmp / "enstrophy.dat").read_text()
         assert len(a.splitlines()) == 4 and a == b, (a, b)
+        # restart from the step-2 files (block::initial reads them, src/block.cpp:785-855;
+        # metrics then come from the GPU) and run to step 4: same bytes as the continuous run
+        io = (tmp / "inp/IOController.in").read_text().replace("startStep 0", "startStep 2")
+        (tmp / "inp/IOController.in").write_text(io)
+        for r in range(case.nranks):
+            (tmp / f"flowData/NUC3d_step_4_ID_{r}.bin").unlink()
+        RD.run(tmp, quiet=True)
+        for r in range(case.nranks):
+            a = (ref / f"flowData/NUC3d_step_4_ID_{r}.bin").read_bytes()
+            b = (tmp / f"flowData/NUC3d_step_4_ID_{r}.bin").read_bytes()
+            assert a == b, ("restart", r)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
