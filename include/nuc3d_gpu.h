@@ -157,6 +157,33 @@ int nuc3d_diagnostics(nuc3d_ctx *ctx, double *enstrophy, double *kinetic);
    0.5|w|^2, Q (TemporalQField[9..13] of the reference). */
 int nuc3d_block_get_diag(nuc3d_ctx *ctx, int block, double *fields);
 
+/* ---- Learned face sensor (hybrid WENO-Z) --------------------------------------------
+   No counterpart in the reference.  A 19 -> 32 -> 32 -> 1 MLP decides per face whether
+   WENO-Z needs its nonlinear weights; parameters are NUC3D_SENSOR_PARAMS floats, in the
+   order W1[32][19], b1[32], W2[32][32], b2[32], W3[32], b3. */
+#define NUC3D_SENSOR_PARAMS 1729
+/* Features (19 floats per face) and labels (1: some WENO-Z weight is more than 0.05 from
+   its linear weight) of the interior faces of direction dir at the current state, written
+   to device buffers in no particular order; where (may be NULL) gets each face's index in
+   its block's face grid (n[dir]+1 faces along dir, i fastest); *count = faces written (at
+   most cap).  dir must use weno5z. */
+int nuc3d_sensor_record(nuc3d_ctx *ctx, int dir, float *feat, unsigned char *label,
+                        long long *where, unsigned long long cap, unsigned long long *count);
+/* Training, on device buffers and the given CUDA stream: loss (BCE on the logit, positives
+   weighted by pos_weight, mean over n) and its gradient w.r.t. the parameters (grad is
+   overwritten); logits (n floats) may be NULL.  Then one Adam step (step >= 1). */
+int nuc3d_sensor_loss_grad(const float *params, const float *feat, const unsigned char *label,
+                           long long n, float pos_weight, float *grad, float *loss, float *logits,
+                           void *stream);
+int nuc3d_sensor_adam(float *params, const float *grad, float *m, float *v, float lr, float beta1,
+                      float beta2, float eps, int step, void *stream);
+/* Hybrid WENO-Z (throughput build only): from now on every interior face of a weno5z
+   direction whose sensor logit is below logit_threshold takes the linear weights
+   (0.1, 0.6, 0.3); the others, and the faces of the boundary schemes, are unchanged.
+   params: NUC3D_SENSOR_PARAMS floats (copied, rounded to BF16 as in the training), or
+   NULL to return to plain WENO-Z. */
+int nuc3d_set_sensor(nuc3d_ctx *ctx, const float *params, float logit_threshold);
+
 /* Kernels one nuc3d_step(ctx, 1) launches (after nuc3d_finalize): per RK stage the BC
    ghost pass (when a block has a physical face), the NS primitive and gradient passes,
    and one sweep per direction (three kernels for a compact-scheme direction).  No

@@ -37,7 +37,8 @@ EXPORTED = (
     "nuc3d_get_time", "nuc3d_set_time", "nuc3d_get_status", "nuc3d_set_stream",
     "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis", "nuc3d_profile_sweep",
     "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step", "nuc3d_diagnostics", "nuc3d_block_get_diag",
-    "nuc3d_block_set_nodes", "nuc3d_block_get_metrics",
+    "nuc3d_block_set_nodes", "nuc3d_block_get_metrics", "nuc3d_sensor_record",
+    "nuc3d_sensor_loss_grad", "nuc3d_sensor_adam", "nuc3d_set_sensor",
 )
 
 
@@ -113,6 +114,12 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_kernels_per_step.argtypes = [P, PI]
     lib.nuc3d_diagnostics.argtypes = [P, PD, PD]
     lib.nuc3d_block_set_nodes.argtypes = [P, I, PD, PD, PD]
+    ULL = ctypes.c_ulonglong
+    lib.nuc3d_sensor_record.argtypes = [P, I, P, P, P, ULL, ctypes.POINTER(ULL)]
+    F = ctypes.c_float
+    lib.nuc3d_sensor_loss_grad.argtypes = [P, P, P, ctypes.c_longlong, F, P, P, P, P]
+    lib.nuc3d_sensor_adam.argtypes = [P, P, P, P, F, F, F, F, I, P]
+    lib.nuc3d_set_sensor.argtypes = [P, ctypes.POINTER(F), F]
     lib.nuc3d_block_get_metrics.argtypes = [P, I, PD, PD, PD, PD, PD]
     lib.nuc3d_block_get_diag.argtypes = [P, I, PD]
     lib.nuc3d_rhs_noalloc.argtypes = [ctypes.POINTER(_Cfg), I, I, I, I, PI, PI, PD, P, P, P, P,
@@ -329,6 +336,29 @@ class Solver:
         out = np.empty(self._shape5(block), dtype=np.float64)
         _check(self.lib.nuc3d_block_get_diag(self._ctx, block, _pd(out)))
         return out
+
+    def sensor_record(self, direction: int, feat_ptr: int, label_ptr: int, where_ptr: int,
+                      cap: int) -> int:
+        """Record face features/labels of one direction into device buffers (pointers);
+        returns the number written."""
+        n = ctypes.c_ulonglong()
+        _check(self.lib.nuc3d_sensor_record(self._ctx, direction, ctypes.c_void_p(feat_ptr),
+                                            ctypes.c_void_p(label_ptr),
+                                            ctypes.c_void_p(where_ptr) if where_ptr else None,
+                                            cap, ctypes.byref(n)))
+        return n.value
+
+    def set_sensor(self, params=None, logit_threshold: float = -4.0) -> None:
+        """Hybrid WENO-Z with the learned face sensor (params: 1729 floats; None: plain)."""
+        if params is None:
+            _check(self.lib.nuc3d_set_sensor(self._ctx, None, 0.0))
+            return
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != 1729:
+            raise ValueError("the sensor has 1729 parameters")
+        self._sensor_keep = p
+        _check(self.lib.nuc3d_set_sensor(self._ctx, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                         float(logit_threshold)))
 
     def kernels_per_step(self) -> int:
         """Kernels one step launches (the library's own count of its launches)."""

@@ -29,6 +29,7 @@ UNITS = {
     "kernels_fast.cu": ["-fmad=true"],
     "nuc3d_abi.cu": [],
     "nuc3d_noalloc.cu": [],
+    "sensor_train.cu": [],
 }
 
 

@@ -89,6 +89,18 @@ struct FaceJobs {
   int start[kMaxFaceJobs + 1];  // prefix sums of 256-cell tiles
 };
 
+// The face sensor of the hybrid WENO-Z sweep (sensor.cuh), arranged for the tensor-core
+// inference: BF16 weight pairs in mma.sync m16n8k16 B-fragment order, [k-step][n-tile][lane],
+// and BF16-rounded biases and output weights as floats.
+struct SensorDev {
+  uint32_t w1[2][4][32][2];
+  float b1[32];
+  uint32_t w2[2][4][32][2];
+  float b2[32];
+  float w3[32];
+  float b3;
+};
+
 struct SolverParams {
   int scheme[3];         // per direction
   int ts[3];             // per-direction bufferSize (scheme_tilesize)
@@ -98,6 +110,8 @@ struct SolverParams {
   int weno5z_compat;     // 1: reproduce the interior positive is2 of src/weno5z.cpp:80
   int vis[3];            // VisScheme per direction
   double gamma, mach, reynolds, prandtl, t_ref, t_inf, t_wall, cfl;
+  const SensorDev *sensor;  // hybrid WENO-Z: the face sensor, or null (plain WENO-Z)
+  float sensor_threshold;   // logit below which a face takes the linear weights
 };
 
 // Per-launch work list: tiles of every block, laid end to end.
@@ -153,6 +167,8 @@ void set_error_message(const char *msg);
 // 2 * kDiagParts doubles per block of scratch.
 namespace exact {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
+                            long long *where, unsigned long long *count, unsigned long long cap);
 cudaError_t run_metrics(const double *x, const double *y, const double *z, const int n[3],
                         double *jac, double *met, double *dxyz, unsigned *bad, cudaStream_t st);
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
@@ -162,6 +178,8 @@ int tile_count(int dir, const int n[3]);
 }
 namespace fast {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
+                            long long *where, unsigned long long *count, unsigned long long cap);
 cudaError_t run_metrics(const double *x, const double *y, const double *z, const int n[3],
                         double *jac, double *met, double *dxyz, unsigned *bad, cudaStream_t st);
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);

@@ -18,6 +18,7 @@
 // Ghost cells across block faces are read directly from the neighbour block's
 // arrays in HBM; this replaces the MPI halo exchange (src/MPICommunicator.cpp:36-115).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include "schemes.cuh"
 
@@ -410,10 +411,11 @@ template <int DIR, int SCH> struct TileSmem {
 // Phase 1: split fluxes F+/F- of the tile's line positions c0-R .. c0+cl+R-1 into sF
 // ([10][TW][SP]); own cells of the zeta tile also leave their state in sQ; eig reduces
 // max(|U|+c|grad xi|) over the three directions.
-template <int DIR, int SCH>
+template <int DIR, int SCH, bool RHOP = false>
 __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks, const TileCtx &T,
                                             const SolverParams &P, int stage, bool eig, double *sF,
-                                            double *sQ, unsigned &st, double &emax) {
+                                            double *sQ, unsigned &st, double &emax,
+                                            double *sRP = nullptr) {
   using M = TileSmem<DIR, SCH>;
   constexpr int R = M::R, TW = M::TW, NP = M::NP, SP = M::SP, SQ = M::SQ;
   const BlockDev &B = *T.B;
@@ -439,6 +441,10 @@ __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks,
         double q[5];
         CellPrim s;
         cell_split(*CB, stage, idx, DIR, P, fp, fn, s, q, st);
+        if (RHOP) {  // density and pressure of the position, for the face sensor
+          sRP[w * SP + p] = s.rho;
+          sRP[(TW + w) * SP + p] = s.p;
+        }
         if (own && eig && g >= T.c0 && g < T.c0 + T.cl) {
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
@@ -624,8 +630,28 @@ __device__ __forceinline__ void reduce_eig(double emax, double *sRed, StepState 
   }
 }
 
-// Explicit-scheme sweep: phases split -> faces -> cells in one CTA.
+#include "sensor.cuh"
+
+// The five reconstructions of one boundary-scheme face, out of line: the hybrid sweep's
+// hot loop stays small.
 template <int DIR, int SCH>
+__device__ __noinline__ void edge_faces_of_line(const TileCtx &T, int f, int fl, int w,
+                                                const double *sF, double *sH) {
+  using M = TileSmem<DIR, SCH>;
+  constexpr int R = M::R, TW = M::TW, SP = M::SP, SH = M::SH;
+  for (int v = 0; v < 5; ++v) {
+    const double *rowP = sF + (v * TW + w) * SP + (R - T.c0);
+    const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - T.c0);
+    auto Pacc = [rowP](int c) { return rowP[c]; };
+    auto Nacc = [rowN](int c) { return rowN[c]; };
+    sH[(v * TW + w) * SH + fl] =
+        edge_face<SCH>(f, T.G.L, T.ts, T.physR, T.c0 - R, T.c0 - R + M::NP - 1, Pacc, Nacc);
+  }
+}
+
+// Explicit-scheme sweep: phases split -> faces -> cells in one CTA.  HYB: the hybrid
+// WENO-Z face loop of the throughput build (P.sensor set).
+template <int DIR, int SCH, bool HYB = false>
 __global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
 sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
              int stage, int flags) {
@@ -637,13 +663,14 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   const bool ns = (flags & SW_NS) != 0;
   double *sV = sH + 5 * TW * SH;            // [4][TW][SV]: viscous fluxes (NS)
   double *sQ = sV + (ns ? 4 * TW * SV : 0); // [5][TW][SQ]: stage state (zeta sweep)
+  double *sRP = sQ + (DIR == 2 ? 5 * TW * M::SQ : 0);  // hybrid: [2][TW][SP] rho, p
   __shared__ double sRed[kThreads / 32];
 
   const TileCtx T = decode_tile<DIR>(blocks, tm, P);
   const bool eig = (flags & SW_EIG) != 0;
   unsigned st = 0;
   double emax = 0.0;
-  phase_split<DIR, SCH>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st, emax);
+  phase_split<DIR, SCH, HYB>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st, emax, sRP);
   if (ns) phase_vis<DIR, SCH>(blocks, T, P, sV);
   __syncthreads();
 
@@ -660,6 +687,61 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   const int ne = nf - ni;                     // edge faces per line
   const int ei = TW * ni, e0 = (ei + 31) & ~31;
   const float rni = ni > 0 ? 1.0f / (float)ni : 0.0f, rne = ne > 0 ? 1.0f / (float)ne : 0.0f;
+  if constexpr (HYB) {
+    // hybrid WENO-Z: the face sensor picks linear or nonlinear weights per interior face.
+    // The loop runs the same number of rounds in every thread: the sensor is warp-collective.
+    for (int base = 0; base < e0 + TW * ne; base += kThreads) {
+      const int e = base + threadIdx.x;
+      int w = 0, fl = 0;
+      bool edge = false, valid = true;
+      if (e < ei) {
+        w = __float2int_rz(((float)e + 0.5f) * rni);
+        fl = lo + (e - w * ni);
+      } else if (e >= e0 && e < e0 + TW * ne) {
+        const int j = e - e0;
+        w = __float2int_rz(((float)j + 0.5f) * rne);
+        const int k = j - w * ne;
+        fl = k < nl ? k : hi + (k - nl);
+        edge = true;
+      } else {
+        valid = false;
+      }
+      valid = valid && w < T.nw;
+      uint32_t xr[10];
+#pragma unroll
+      for (int i = 0; i < 10; ++i) xr[i] = 0u;
+      if (valid && !edge) {
+        const double *rows[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) rows[v] = sF + (v * TW + w) * SP + (R + fl);
+        sensor_features_packed(rows, sRP + w * SP + (R + fl), sRP + (TW + w) * SP + (R + fl), xr);
+      }
+      const float logit = sensor_logit(P.sensor, xr);
+      if (!valid) continue;
+      const int f = T.c0 + fl;
+      if (!edge && logit < P.sensor_threshold) {
+#pragma unroll 1
+        for (int v = 0; v < 5; ++v) {
+          const double *rowP = sF + (v * TW + w) * SP + (R + fl);
+          const double *rowN = sF + ((5 + v) * TW + w) * SP + (R + fl);
+          sH[(v * TW + w) * SH + fl] = weno5_linear(rowP[-3], rowP[-2], rowP[-1], rowP[0], rowP[1]) +
+                                       weno5_linear(rowN[2], rowN[1], rowN[0], rowN[-1], rowN[-2]);
+        }
+      } else if (!edge) {
+        const bool cz = compat && f >= T.ts && f <= T.G.L - T.ts;
+#pragma unroll 1
+        for (int v = 0; v < 5; ++v) {
+          const double *rowP = sF + (v * TW + w) * SP + (R + fl);
+          const double *rowN = sF + ((5 + v) * TW + w) * SP + (R + fl);
+          auto Pacc = [rowP](int c) { return rowP[c]; };
+          auto Nacc = [rowN](int c) { return rowN[c]; };
+          sH[(v * TW + w) * SH + fl] = recon_pos_in<SCH>(0, cz, Pacc) + recon_neg_in<SCH>(0, Nacc);
+        }
+      } else {
+        edge_faces_of_line<DIR, SCH>(T, f, fl, w, sF, sH);
+      }
+    }
+  } else
   for (int e = threadIdx.x; e < e0 + TW * ne; e += kThreads) {
     // w = e / ni by a float reciprocal: exact, since (e + 1/2) / ni stays at least
     // 1/(2 ni) away from an integer and e < 2^9.
@@ -1337,10 +1419,26 @@ metrics_kernel(const double *__restrict__ x, const double *__restrict__ y,
 // ---------------------------------------------------------------------------------
 // Host-side launchers (called by the C-ABI layer).
 // ---------------------------------------------------------------------------------
+// Shared memory of the hybrid sweep: the plain sweep's plus rho and p per position.
+template <int DIR, int SCH>
+__host__ __device__ inline size_t hybrid_smem_bytes(bool ns) {
+  return sweep_smem_bytes<DIR, SCH>(ns) + (size_t)2 * kTW * TileSmem<DIR, SCH>::SP * sizeof(double);
+}
+
 template <int DIR, int SCH>
 inline cudaError_t launch_sweep_t(const Launch &L, int stage, int flags) {
   const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
-  const size_t smem = sweep_smem_bytes<DIR, SCH>((flags & SW_NS) != 0);
+  const bool ns = (flags & SW_NS) != 0;
+#if NUC3D_FAST
+  if constexpr (SCH == SCH_WENO5Z) {
+    if (L.P.sensor) {
+      sweep_kernel<DIR, SCH, true><<<ntiles, kThreads, hybrid_smem_bytes<DIR, SCH>(ns), L.stream>>>(
+          L.d_blocks, L.tm_dir[DIR], L.P, L.d_state, stage, flags);
+      return cudaGetLastError();
+    }
+  }
+#endif
+  const size_t smem = sweep_smem_bytes<DIR, SCH>(ns);
   sweep_kernel<DIR, SCH><<<ntiles, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[DIR], L.P,
                                                                L.d_state, stage, flags);
   return cudaGetLastError();
@@ -1425,6 +1523,23 @@ cudaError_t run_metrics(const double *x, const double *y, const double *z, const
   return cudaGetLastError();
 }
 
+cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
+                            long long *where, unsigned long long *count, unsigned long long cap) {
+  if (L.P.scheme[dir] != SCH_WENO5Z) return cudaErrorInvalidValue;
+  const int nt = L.tm_dir[dir].tile_start[L.tm_dir[dir].nblocks];
+  const size_t smem = (size_t)12 * kTW * TileSmem<0, SCH_WENO5Z>::SP * sizeof(double);
+  if (dir == 0)
+    sensor_data_kernel<0><<<nt, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[0], L.P, L.d_state,
+                                                            0, feat, label, where, count, cap);
+  else if (dir == 1)
+    sensor_data_kernel<1><<<nt, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[1], L.P, L.d_state,
+                                                            0, feat, label, where, count, cap);
+  else
+    sensor_data_kernel<2><<<nt, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[2], L.P, L.d_state,
+                                                            0, feat, label, where, count, cap);
+  return cudaGetLastError();
+}
+
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts) {
   const int nt = L.tm_cells.tile_start[L.tm_cells.nblocks];
   const int nb = L.tm_cells.nblocks;
@@ -1458,6 +1573,14 @@ cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags) {
 
 template <int DIR, int SCH>
 inline cudaError_t configure_t() {
+#if NUC3D_FAST
+  if constexpr (SCH == SCH_WENO5Z) {
+    const cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIR, SCH, true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)hybrid_smem_bytes<DIR, SCH>(true));
+    if (e != cudaSuccess) return e;
+  }
+#endif
   return cudaFuncSetAttribute(sweep_kernel<DIR, SCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sweep_smem_bytes<DIR, SCH>(true));
 }

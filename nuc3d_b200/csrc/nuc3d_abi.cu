@@ -103,6 +103,7 @@ struct nuc3d_ctx {
   std::vector<DiagDev> diag;
   DiagDev *d_diag = nullptr;
   double *d_dsums = nullptr, *d_dparts = nullptr;
+  SensorDev *d_sensor = nullptr;  // hybrid WENO-Z face sensor (nuc3d_set_sensor)
 
   cudaError_t stage(int s, bool rk, bool eig) {
     return exact ? nuc3d::exact::run_stage(L, s, rk, eig) : nuc3d::fast::run_stage(L, s, rk, eig);
@@ -206,6 +207,7 @@ int nuc3d_destroy(nuc3d_ctx *c) {
   for (auto p : {c->d_dsums, c->d_dparts})
     if (p) cudaFree(p);
   if (c->d_diag) cudaFree(c->d_diag);
+  if (c->d_sensor) cudaFree(c->d_sensor);
   if (c->d_blocks) cudaFree(c->d_blocks);
   if (c->d_jobs) cudaFree(c->d_jobs);
   if (c->d_state) cudaFree(c->d_state);
@@ -697,6 +699,83 @@ int nuc3d_block_get_diag(nuc3d_ctx *c, int bi, double *fields) {
   if (!c || !fields || bi < 0 || bi >= (int)c->blocks.size()) return fail(NUC3D_EINVAL, "bad argument");
   if (!c->d_diag) return fail(NUC3D_ESTATE, "call nuc3d_diagnostics first");
   return copy_out(c, bi, fields, c->diag[bi].fields, 5);
+}
+
+int nuc3d_sensor_record(nuc3d_ctx *c, int dir, float *feat, unsigned char *label,
+                        long long *where, unsigned long long cap, unsigned long long *count) {
+  if (!c || !feat || !label || !count || dir < 0 || dir > 2) return fail(NUC3D_EINVAL, "bad argument");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  if (c->P.scheme[dir] != SCH_WENO5Z)
+    return fail(NUC3D_ENOTSUP, "the face sensor is defined for weno5z directions");
+  cudaSetDevice(c->device);
+  unsigned long long *d_count = nullptr;
+  CUDA_TRY(cudaMallocAsync(&d_count, sizeof(unsigned long long), c->stream));
+  cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), c->stream);
+  if (e == cudaSuccess)
+    e = c->exact ? nuc3d::exact::run_sensor_data(c->L, dir, feat, label, where, d_count, cap)
+                 : nuc3d::fast::run_sensor_data(c->L, dir, feat, label, where, d_count, cap);
+  unsigned long long n = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&n, d_count, sizeof(n), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFreeAsync(d_count, c->stream);
+  if (e != cudaSuccess) return fail(NUC3D_ECUDA, "sensor record: %s", cudaGetErrorString(e));
+  *count = n < cap ? n : cap;
+  return NUC3D_OK;
+}
+
+namespace {
+// float -> BF16 bits, round to nearest even (NaN stays NaN)
+uint32_t bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return (u >> 16) | 0x40u;
+  return (u + 0x7fffu + ((u >> 16) & 1u)) >> 16;
+}
+float bf16_value(float f) {
+  const uint32_t u = bf16_bits(f) << 16;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+}  // namespace
+
+int nuc3d_set_sensor(nuc3d_ctx *c, const float *params, float logit_threshold) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  if (c->exact && params)
+    return fail(NUC3D_ENOTSUP, "the hybrid sweep exists in the throughput build only (exact = 0)");
+  cudaSetDevice(c->device);
+  c->drop_graph();
+  if (!params) {
+    c->P.sensor = c->L.P.sensor = nullptr;
+    return NUC3D_OK;
+  }
+  // W1[32][19] b1[32] W2[32][32] b2[32] W3[32] b3: B fragments of mma.sync m16n8k16
+  // (rows k = 2q, 2q+1 and 2q+8, 2q+9 of the k-step, column n = lane / 4 of the n-tile)
+  SensorDev h{};
+  auto W1 = [&](int n, int k) { return k < 19 ? params[n * 19 + k] : 0.0f; };
+  auto W2 = [&](int n, int k) { return params[640 + n * 32 + k]; };
+  for (int ks = 0; ks < 2; ++ks)
+    for (int nt = 0; nt < 4; ++nt)
+      for (int lane = 0; lane < 32; ++lane) {
+        const int n = nt * 8 + lane / 4, k0 = ks * 16 + 2 * (lane % 4);
+        h.w1[ks][nt][lane][0] = bf16_bits(W1(n, k0)) | (bf16_bits(W1(n, k0 + 1)) << 16);
+        h.w1[ks][nt][lane][1] = bf16_bits(W1(n, k0 + 8)) | (bf16_bits(W1(n, k0 + 9)) << 16);
+        h.w2[ks][nt][lane][0] = bf16_bits(W2(n, k0)) | (bf16_bits(W2(n, k0 + 1)) << 16);
+        h.w2[ks][nt][lane][1] = bf16_bits(W2(n, k0 + 8)) | (bf16_bits(W2(n, k0 + 9)) << 16);
+      }
+  for (int j = 0; j < 32; ++j) {
+    h.b1[j] = bf16_value(params[608 + j]);
+    h.b2[j] = bf16_value(params[1664 + j]);
+    h.w3[j] = bf16_value(params[1696 + j]);
+  }
+  h.b3 = bf16_value(params[1728]);
+  if (!c->d_sensor) CUDA_TRY(cudaMalloc(&c->d_sensor, sizeof(SensorDev)));
+  CUDA_TRY(cudaMemcpy(c->d_sensor, &h, sizeof(SensorDev), cudaMemcpyHostToDevice));
+  c->P.sensor = c->L.P.sensor = c->d_sensor;
+  c->P.sensor_threshold = c->L.P.sensor_threshold = logit_threshold;
+  return NUC3D_OK;
 }
 
 int nuc3d_kernels_per_step(nuc3d_ctx *c, int *kernels) {
