@@ -236,6 +236,24 @@ def reference_arm(args):
 
 
 # ---------------------------------------------------------------------------------
+# multi-rank bookkeeping (replicas: one independent block per GPU, no data-path collective)
+# ---------------------------------------------------------------------------------
+def rank_max(x: float, dist=None, device="cpu") -> float:
+    """The slowest rank's time: all-reduce(MAX) over the process group (identity alone)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, cells_per_rank: int, steps: int, ms_max: float) -> float:
+    """Mcell-RK3-steps/s of the whole job: every rank's cells over the slowest rank's time."""
+    return world * cells_per_rank * steps / (ms_max * 1e-3) / 1e6
+
+
+# ---------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------
 def ours(args):
@@ -274,11 +292,7 @@ def ours(args):
         s.sync()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, dist, dev)
 
     # ---- device-resident timing ----
     s.step(args.warmup)
@@ -293,7 +307,7 @@ def ours(args):
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     s.sync()
     status = s.status()
-    value = world * cells * args.steps / (ms * 1e-3) / 1e6
+    value = whole_job_rate(world, cells, args.steps, ms)
 
     # ---- end to end through the public API with pinned host buffers ----
     host_in = torch.empty(5 * cells, dtype=torch.float64, pin_memory=True)
@@ -314,7 +328,7 @@ def ours(args):
     ev3.record(stream)
     ev3.synchronize()
     e2e_ms = max_over_ranks(ev2.elapsed_time(ev3))
-    e2e_value = world * cells * e2e_steps / (e2e_ms * 1e-3) / 1e6
+    e2e_value = whole_job_rate(world, cells, e2e_steps, e2e_ms)
 
     # ---- hybrid WENO-Z with the learned face sensor: same workload, same step count ----
     hybrid = None
@@ -337,7 +351,7 @@ def ours(args):
         hms = max_over_ranks(ev4.elapsed_time(ev5))
         rho_h = s.get_q(b)[0]
         s.set_sensor(None)
-        hv = world * cells * args.steps / (hms * 1e-3) / 1e6
+        hv = whole_job_rate(world, cells, args.steps, hms)
         hybrid = {"value": hv, "unit": "Mcell-RK3-steps/s", "ms_per_step": hms / args.steps,
                   "vs_plain": hv / value, "logit_threshold": SENS.DEFAULT_THRESHOLD,
                   "l1_density_error_vs_plain": float(np.abs(rho_h - rho_plain).sum() /
