@@ -56,7 +56,8 @@ typedef struct nuc3d_ctx nuc3d_ctx;
 
 typedef struct {
   /* Method.in: scheme_{x,y,z}_ivs and scheme_{x,y,z}_vis (src/fieldOperator.cpp:20-33).
-     ivs: "weno5js" | "weno5z" | "weno7js" | "crweno5" | "hccs"; vis: "cd6". */
+     ivs: "weno5js" | "weno5z" | "weno7js" | "crweno5" | "hccs" | "hccs77" | "weno3js" |
+     "upwind1st"; vis: "cd6" (NULL) | "cd2" | "cd8". */
   const char *scheme_ivs[3];
   const char *scheme_vis[3];
   /* PhysModel.in positional entries (src/physicsModel.cpp:65-69):
@@ -84,7 +85,10 @@ int nuc3d_destroy(nuc3d_ctx *ctx);
    as in BC_Topo_<rank>.in (src/boundaryConditions.cpp:69-93):
      bc_type[f] = -1 for a physical face, else the index of the neighbour block;
      bc_id[f]   = physical: 0 inlet, 1 outlet, 2 wall, 3 symmetry; else the neighbour's face.
-   bc_values: 6*5 doubles (rho, u, v, w, p per face, used by inlet faces); may be NULL. */
+   bc_values: 6*5 doubles (rho, u, v, w, p per face, used by inlet faces); may be NULL.
+   NUC3D_ENOTSUP for an hccs77 direction with a physical face, or with more than 127 cells
+   along it or more than 128 across it: the reference's hccs77 is defined only for
+   neighbour faces and lines that fit its 128^3 row arrays (src/hccs77.hpp:15-18). */
 int nuc3d_block_add(nuc3d_ctx *ctx, int nx, int ny, int nz, const int bc_type[6],
                     const int bc_id[6], const double *bc_values, int *block_id);
 

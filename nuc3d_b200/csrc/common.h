@@ -14,7 +14,7 @@ namespace nuc3d {
 
 enum Scheme : int {
   SCH_WENO5JS = 0, SCH_WENO5Z = 1, SCH_WENO7JS = 2, SCH_CRWENO5 = 3, SCH_HCCS = 4,
-  SCH_WENO3JS = 5, SCH_UPWIND1 = 6
+  SCH_WENO3JS = 5, SCH_UPWIND1 = 6, SCH_HCCS77 = 7
 };
 // Viscous difference per direction (scheme_x/y/z_vis, src/fieldOperator.cpp:286-367).
 enum VisScheme : int { VIS_CD6 = 0, VIS_CD2 = 1, VIS_CD8 = 2 };
@@ -32,7 +32,8 @@ enum StatusBits : unsigned {
 
 // Reference bufferSize per scheme (src/fieldOperator.cpp:127-283).
 inline __host__ __device__ int scheme_tilesize(int s) {
-  return (s == SCH_WENO7JS || s == SCH_HCCS) ? 4 : s == SCH_WENO3JS ? 2 : s == SCH_UPWIND1 ? 1 : 3;
+  return (s == SCH_WENO7JS || s == SCH_HCCS || s == SCH_HCCS77) ? 4
+         : s == SCH_WENO3JS ? 2 : s == SCH_UPWIND1 ? 1 : 3;
 }
 
 struct FaceDev {

@@ -801,7 +801,11 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
 // ---------------------------------------------------------------------------------
 // Compact schemes (crweno5, hccs): the reference solves, per line, variable and split,
 // a tridiagonal system over faces ts .. n-ts (src/crweno5.cpp:44-401, src/hccs.cpp:45-493)
-// with explicit end rows and explicit block-edge faces.  Three kernels per direction:
+// with explicit end rows and explicit block-edge faces.  hccs77 (WHOLE) solves one system
+// over all faces 0 .. n: WENO7-Z end rows at faces 0 and n from the neighbour's ghost
+// cells and hccs rows everywhere else, the rows next to the block edges included
+// (src/hccs77.cpp:45-195 inner, :218-568 left, :592-943 right, :945-978 the solve).
+// Three kernels per direction:
 //   compact_rows_kernel   split fluxes (phase 1 of the sweep), then per face either the
 //                         explicit value (into fh) or the tridiagonal row (a, b, c, d)
 //   compact_thomas_kernel one thread per system: the reference's Thomas elimination and
@@ -817,10 +821,11 @@ __device__ __forceinline__ void compact_row(const double f[5], double &lo, doubl
   else hccs_row(f, lo, di, up, rhs);
 }
 
-template <int DIR, int SCH>
+template <int DIR, int SCH, bool WHOLE = false>
 __global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
 compact_rows_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
                     int stage, int flags) {
+  static_assert(!WHOLE || SCH == SCH_HCCS, "the whole-line system is the hccs77 form of hccs");
   using M = TileSmem<DIR, SCH>;
   constexpr int R = M::R, TW = M::TW, TL = M::TL, SP = M::SP;
   extern __shared__ double smem[];
@@ -833,7 +838,7 @@ compact_rows_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParam
   phase_split<DIR, SCH>(blocks, T, P, stage, eig, sF, nullptr, st, emax);
   __syncthreads();
   const BlockDev &B = *T.B;
-  const int L = T.G.L, ts = T.ts, m = L - 2 * ts + 1;
+  const int L = T.G.L, ts = T.ts, f0 = WHOLE ? 0 : ts, m = L - 2 * f0 + 1;
   const long long nl = (long long)T.G.nW * T.G.nO;
   const long long S10 = 10 * nl;
   for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
@@ -847,19 +852,19 @@ compact_rows_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParam
       const double *row = sF + ((side ? 5 + v : v) * TW + w) * SP + (R - T.c0);
       auto A = [row](int c) { return row[c]; };
       const long long sidx = sys * nl + line;
-      if (f < ts || f > L - ts) {
+      if (!WHOLE && (f < ts || f > L - ts)) {
         const double h = side ? recon_neg<SCH>(f, L, ts, T.physL, T.physR, A)
                               : recon_pos<SCH>(f, L, ts, T.physL, T.physR, false, A);
         B.fh[sidx * (L + 1) + f] = h;
         continue;
       }
-      const int r = f - ts;
+      const int r = f - f0;
       double a, b, c, d;
       if (r == 0 || r == m - 1) {
-        // explicit end rows: WENO5-JS (crweno5) or WENO7-Z (hccs)
+        // explicit end rows: WENO5-JS (crweno5) or WENO7-Z (hccs, hccs77), the interior
+        // stencil (hccs77: its faces 0 and n read the neighbour's ghost cells)
         a = 0.0; b = 1.0; c = 0.0;
-        d = side ? recon_neg<SCH>(f, L, ts, false, false, A)
-                 : recon_pos<SCH>(f, L, ts, false, false, false, A);
+        d = side ? recon_neg_in<SCH>(f, A) : recon_pos_in<SCH>(f, false, A);
       } else {
         double s5[5];
         if (side) { s5[0] = A(f + 2); s5[1] = A(f + 1); s5[2] = A(f); s5[3] = A(f - 1); s5[4] = A(f - 2); }
@@ -881,9 +886,10 @@ compact_rows_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParam
 }
 
 // One thread per (line, variable, split) system of one direction.
+// f0: the face of the system's first row (ts; 0 for hccs77).
 template <int DIR>
 __global__ void __launch_bounds__(256)
-compact_thomas_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P) {
+compact_thomas_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, int f0) {
   const int b = find_block(tm, blockIdx.x);
   const BlockDev &B = blocks[b];
   const int n[3] = {B.n[0], B.n[1], B.n[2]};
@@ -891,7 +897,7 @@ compact_thomas_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverPar
   const long long nl = (long long)G.nW * G.nO, S10 = 10 * nl;
   const long long s = (long long)(blockIdx.x - tm.tile_start[b]) * 256 + threadIdx.x;
   if (s >= S10) return;
-  const int L = G.L, ts = P.ts[DIR], m = L - 2 * ts + 1;
+  const int L = G.L, m = L - 2 * f0 + 1;
   double *rw = B.rows + s;
   double cp = rw[2 * S10], dp = rw[3 * S10];
   for (int r = 1; r < m; ++r) {
@@ -903,7 +909,7 @@ compact_thomas_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverPar
     x[2 * S10] = cp;
     x[3 * S10] = dp;
   }
-  double *fh = B.fh + s * (L + 1) + ts;
+  double *fh = B.fh + s * (L + 1) + f0;
   double xv = dp;
   fh[m - 1] = xv;
   for (int r = m - 2; r >= 0; --r) {
@@ -1458,15 +1464,17 @@ __host__ __device__ inline size_t compact_finish_smem_bytes(bool ns) {
   return n * sizeof(double);
 }
 
-template <int DIR, int SCH>
+template <int DIR, int SCH, bool WHOLE = false>
 inline cudaError_t launch_compact_t(const Launch &L, int stage, int flags) {
   const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
-  compact_rows_kernel<DIR, SCH><<<ntiles, kThreads, compact_rows_smem_bytes<DIR, SCH>(), L.stream>>>(
-      L.d_blocks, L.tm_dir[DIR], L.P, L.d_state, stage, flags & SW_EIG);
+  compact_rows_kernel<DIR, SCH, WHOLE>
+      <<<ntiles, kThreads, compact_rows_smem_bytes<DIR, SCH>(), L.stream>>>(
+          L.d_blocks, L.tm_dir[DIR], L.P, L.d_state, stage, flags & SW_EIG);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int nsys = L.tm_sys[DIR].tile_start[L.tm_sys[DIR].nblocks];
-  compact_thomas_kernel<DIR><<<nsys, 256, 0, L.stream>>>(L.d_blocks, L.tm_sys[DIR], L.P);
+  compact_thomas_kernel<DIR><<<nsys, 256, 0, L.stream>>>(L.d_blocks, L.tm_sys[DIR], L.P,
+                                                         WHOLE ? 0 : L.P.ts[DIR]);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   compact_finish_kernel<DIR, SCH><<<ntiles, kThreads,
                                     compact_finish_smem_bytes<DIR, SCH>((flags & SW_NS) != 0),
@@ -1485,6 +1493,7 @@ inline cudaError_t launch_sweep(const Launch &L, int stage, int flags) {
     case SCH_UPWIND1: return launch_sweep_t<DIR, SCH_UPWIND1>(L, stage, flags);
     case SCH_CRWENO5: return launch_compact_t<DIR, SCH_CRWENO5>(L, stage, flags);
     case SCH_HCCS: return launch_compact_t<DIR, SCH_HCCS>(L, stage, flags);
+    case SCH_HCCS77: return launch_compact_t<DIR, SCH_HCCS, true>(L, stage, flags);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1591,6 +1600,12 @@ inline cudaError_t configure_compact_t() {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)compact_rows_smem_bytes<DIR, SCH>());
   if (e != cudaSuccess) return e;
+  if constexpr (SCH == SCH_HCCS) {
+    e = cudaFuncSetAttribute(compact_rows_kernel<DIR, SCH, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)compact_rows_smem_bytes<DIR, SCH>());
+    if (e != cudaSuccess) return e;
+  }
   return cudaFuncSetAttribute(compact_finish_kernel<DIR, SCH>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)compact_finish_smem_bytes<DIR, SCH>(true));

@@ -60,8 +60,7 @@ int parse_scheme(const char *s, int *out) {
   else if (!std::strcmp(s, "hccs")) *out = SCH_HCCS;
   else if (!std::strcmp(s, "weno3js")) *out = SCH_WENO3JS;
   else if (!std::strcmp(s, "upwind1st")) *out = SCH_UPWIND1;
-  else if (!std::strcmp(s, "hccs77"))
-    return fail(NUC3D_ENOTSUP, "reconstruction scheme 'hccs77' is not implemented");
+  else if (!std::strcmp(s, "hccs77")) *out = SCH_HCCS77;
   else return fail(NUC3D_EINVAL, "unknown reconstruction scheme '%s'", s);
   return NUC3D_OK;
 }
@@ -242,6 +241,25 @@ int nuc3d_block_add(nuc3d_ctx *c, int nx, int ny, int nz, const int bc_type[6], 
     if (bc_type[f] == -1 && bc_id[f] == BC_INLET && !bc_values)
       return fail(NUC3D_EINVAL, "face %d is an inlet but no bc_values were given", f);
   }
+  for (int d = 0; d < 3; ++d) {
+    if (c->P.scheme[d] != SCH_HCCS77) continue;
+    // hccs77 builds its rows in file-static a, b, c, d[128][128][128] (src/hccs77.hpp:15-18),
+    // row n of a line at [k][j][n], and solves them only from interpolationBoundaryR
+    // (src/hccs77.cpp:570-590), which the reference calls for neighbour faces alone
+    // (src/fieldOperator.cpp:400-412).  A physical face would leave rows of an earlier
+    // call in the system (or no solve at all), a longer line would write into the next
+    // line's rows.
+    if (bc_type[2 * d] == -1 || bc_type[2 * d + 1] == -1)
+      return fail(NUC3D_ENOTSUP,
+                  "direction %d: hccs77 with a physical face; the reference then solves rows "
+                  "left from an earlier call", d);
+    for (int e = 0; e < 3; ++e)
+      if (n[e] > (e == d ? 127 : 128))
+        return fail(NUC3D_ENOTSUP,
+                    "direction %d: hccs77 keeps its rows in 128x128x128 arrays; the line "
+                    "extent must be <= 127 cells and the other two <= 128 (dimension %d is %d)",
+                    d, e, n[e]);
+  }
   cudaSetDevice(c->device);
   const size_t nb = (size_t)b.N * sizeof(double);
   cudaError_t e = cudaSuccess;
@@ -272,9 +290,9 @@ int nuc3d_block_add(nuc3d_ctx *c, int nx, int ny, int nz, const int bc_type[6], 
     long long fh_n = 0, rows_n = 0;
     for (int d = 0; d < 3; ++d) {
       const int sc = c->P.scheme[d];
-      if (sc != SCH_CRWENO5 && sc != SCH_HCCS) continue;
+      if (sc != SCH_CRWENO5 && sc != SCH_HCCS && sc != SCH_HCCS77) continue;
       const long long nl = (long long)b.N / n[d];
-      const long long m = n[d] - 2 * c->P.ts[d] + 1;
+      const long long m = n[d] - 2 * (sc == SCH_HCCS77 ? 0 : c->P.ts[d]) + 1;
       fh_n = std::max(fh_n, 10 * nl * (n[d] + 1));
       rows_n = std::max(rows_n, 4 * m * 10 * nl);
     }
@@ -784,7 +802,8 @@ int nuc3d_kernels_per_step(nuc3d_ctx *c, int *kernels) {
   const Launch &L = c->L;
   int per_stage = (L.bc_tiles > 0 ? 1 : 0) + (L.P.model == MODEL_NS ? 2 : 0);
   for (int d = 0; d < 3; ++d)
-    per_stage += (L.P.scheme[d] == SCH_CRWENO5 || L.P.scheme[d] == SCH_HCCS) ? 3 : 1;
+    per_stage += (L.P.scheme[d] == SCH_CRWENO5 || L.P.scheme[d] == SCH_HCCS ||
+                  L.P.scheme[d] == SCH_HCCS77) ? 3 : 1;
   *kernels = 3 * per_stage;
   return NUC3D_OK;
 }

@@ -28,7 +28,8 @@
 #include <stdlib.h>
 #include <string.h>
 
-enum { S_WENO5JS = 0, S_WENO5Z = 1, S_WENO7JS = 2, S_CRWENO5 = 3, S_HCCS = 4, S_WENO3JS = 5, S_UPWIND1 = 6 };
+enum { S_WENO5JS = 0, S_WENO5Z = 1, S_WENO7JS = 2, S_CRWENO5 = 3, S_HCCS = 4, S_WENO3JS = 5, S_UPWIND1 = 6,
+       S_HCCS77 = 7 };
 enum { V_CD6 = 0, V_CD2 = 1, V_CD8 = 2 };
 enum { R_LF = 0, R_AUSM = 1, R_AUSMP = 2 };
 
@@ -43,7 +44,8 @@ typedef struct {
 
 /* bufferSize of a reconstruction scheme (src/fieldOperator.cpp:127-175) */
 static int tilesize(int sch) {
-  return (sch == S_WENO7JS || sch == S_HCCS) ? 4 : sch == S_WENO3JS ? 2 : sch == S_UPWIND1 ? 1 : 3;
+  return (sch == S_WENO7JS || sch == S_HCCS || sch == S_HCCS77) ? 4
+         : sch == S_WENO3JS ? 2 : sch == S_UPWIND1 ? 1 : 3;
 }
 /* bfsize = max of the three (src/block.cpp:506-507) */
 static int ghost_width(const oc_config *c) {
@@ -444,7 +446,7 @@ static void line_ext(const oc_config *c, work_t *W, int bfs, int bi, int d, int 
 static double face_explicit(const oc_config *c, int d, int side, int f, int L, int ts, int physL,
                             int physR, int bfs, const double *e) {
 #define P(cc) e[(cc) + bfs]
-  int sch = c->scheme[d];
+  int sch = c->scheme[d] == S_HCCS77 ? S_HCCS : c->scheme[d]; /* end rows: WENO7-Z */
   int exL = physL && f < ts, exR = physR && f > L - ts;
   if (side == 0) {
     if (exR) {
@@ -508,24 +510,28 @@ static void line_faces(const oc_config *c, const oc_block *b, int d, int bfs, co
   int L = b->n[d], sch = c->scheme[d];
   int ts = tilesize(sch);
   int physL = b->bc_type[2 * d] < 0, physR = b->bc_type[2 * d + 1] < 0;
-  int compact = sch == S_CRWENO5 || sch == S_HCCS;
+  int compact = sch == S_CRWENO5 || sch == S_HCCS || sch == S_HCCS77;
+  /* hccs77: one system over faces 0 .. L, WENO7-Z rows at 0 and L from the ghost cells,
+     hccs rows elsewhere (src/hccs77.cpp:45-195, :218-568, :592-943, solve :945-978);
+     defined for neighbour faces only */
+  int f0 = sch == S_HCCS77 ? 0 : ts;
   static double hs[2][4096], ra[4096], rb[4096], rc[4096], rd[4096];
   for (int side = 0; side < 2; ++side) {
     const double *e = side ? eN : eP;
     for (int f = 0; f <= L; ++f)
-      if (!compact || f < ts || f > L - ts) hs[side][f] = face_explicit(c, d, side, f, L, ts, physL, physR, bfs, e);
+      if (!compact || f < f0 || f > L - f0) hs[side][f] = face_explicit(c, d, side, f, L, ts, physL, physR, bfs, e);
     if (!compact) continue;
-    /* tridiagonal system over faces ts .. L-ts (src/crweno5.cpp:82-218) */
-    int m = L - 2 * ts + 1;
+    /* tridiagonal system over faces f0 .. L-f0 (src/crweno5.cpp:82-218) */
+    int m = L - 2 * f0 + 1;
     for (int r = 0; r < m; ++r) {
-      int f = ts + r;
+      int f = f0 + r;
       if (r == 0 || r == m - 1) {
         ra[r] = 0.0; rb[r] = 1.0; rc[r] = 0.0;
         rd[r] = face_explicit(c, d, side, f, L, ts, 0, 0, bfs, e);
       } else {
         double s5[5], lo, di, up;
         for (int k = 0; k < 5; ++k) s5[k] = side ? e[f + 2 - k + bfs] : e[f - 3 + k + bfs];
-        compact_row(sch == S_HCCS, s5, &lo, &di, &up, &rd[r]);
+        compact_row(sch != S_CRWENO5, s5, &lo, &di, &up, &rd[r]);
         rb[r] = di;
         if (side) { ra[r] = up; rc[r] = lo; } else { ra[r] = lo; rc[r] = up; }
       }
@@ -534,8 +540,8 @@ static void line_faces(const oc_config *c, const oc_block *b, int d, int bfs, co
       rc[i] = rc[i] / (rb[i] - rc[i - 1] * ra[i]);
       rd[i] = (rd[i] - rd[i - 1] * ra[i]) / (rb[i] - rc[i - 1] * ra[i]);
     }
-    hs[side][ts + m - 1] = rd[m - 1];
-    for (int i = m - 2; i >= 0; --i) hs[side][ts + i] = rd[i] - rc[i] * hs[side][ts + i + 1];
+    hs[side][f0 + m - 1] = rd[m - 1];
+    for (int i = m - 2; i >= 0; --i) hs[side][f0 + i] = rd[i] - rc[i] * hs[side][f0 + i + 1];
   }
   for (int f = 0; f <= L; ++f) face[f] = hs[0][f] + hs[1][f];
 }

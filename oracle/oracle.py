@@ -13,7 +13,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_ref" / "liboracle.so"
 SCHEMES = {"weno5js": 0, "weno5z": 1, "weno7js": 2, "crweno5": 3, "hccs": 4, "weno3js": 5,
-           "upwind1st": 6}
+           "upwind1st": 6, "hccs77": 7}
 VIS = {"cd6": 0, "cd2": 1, "cd8": 2}
 RIEMANN = {"LF": 0, "AUSM": 1, "AUSMp": 2}
 MODELS = {"Euler3d": 0, "NavierStokes3d": 1}
@@ -93,6 +93,9 @@ class Run:
         b.n[0], b.n[1], b.n[2] = sh[2], sh[1], sh[0]
         for f in range(6):
             b.bc_type[f], b.bc_id[f] = int(bc_type[f]), int(bc_id[f])
+            if self.cfg.scheme[f // 2] == SCHEMES["hccs77"] and int(bc_type[f]) == -1:
+                raise ValueError("hccs77 is defined for neighbour faces only "
+                                 "(src/fieldOperator.cpp:400-412, src/hccs77.cpp:570-590)")
         vals = np.zeros(30) if bc_values is None else np.asarray(bc_values, dtype=np.float64).ravel()
         for i in range(30):
             b.bcv[i] = vals[i]

@@ -12,7 +12,8 @@ Each fixture <name>.npz holds one case:
   dt, time        per-step dt and accumulated time of those nsteps
   metrics_*       (only in the first fixture) the reference's metrics, to pin the
                   host metric computation
-and diag/<name>.npz the postproc::solveQ diagnostics of the state after those n steps
+multi/<name>.2ranks.npz the same case run as two ranks (cases marked ranks2), and
+diag/<name>.npz the postproc::solveQ diagnostics of the state after those n steps
 (--diag regenerates only these; diag/tgv_ns_weno5js_lf.2ranks.npz is the same case run
 as two ranks, to pin the sum over blocks).
 Node coordinates use only + - * / (oracle.refrun.box_nodes), so tests rebuild the
@@ -119,6 +120,18 @@ def case_defs():
              faces=["inlet", "outlet", "periodic", "periodic", "wall", "symm"], init="channel",
              params=dict(Reynolds=250.0, Mach=0.5, Pt=0.72, Gamma=1.4, T_ref=110.4,
                          T_inf=288.0, T_wall=1.1), nsteps=3),
+        dict(name="tgv_ns_hccs77_lf", model="NavierStokes3d", riemann="LF",
+             schemes=("hccs77",) * 3, shape=(16, 12, 12), lo=(0, 0, 0), hi=(TWO_PI,) * 3,
+             wavy=0.0, faces=["periodic"] * 6, init="tgv",
+             params=dict(Reynolds=1600.0, Mach=0.1, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=3),
+        dict(name="mixed_hccs77_euler_ausmp", model="Euler3d", riemann="AUSMp",
+             schemes=("hccs77", "weno5z", "hccs77"), shape=(24, 12, 12), lo=(0, 0, 0),
+             hi=(1.0, 1.0, 1.0), wavy=0.2,
+             faces=["periodic", "periodic", "outlet", "symm", "periodic", "periodic"],
+             init="sphere",
+             params=dict(Reynolds=1000.0, Mach=1.0, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=3, ranks2=True),
         dict(name="mixed_compact_ausmp", model="Euler3d", riemann="AUSMp",
              schemes=("crweno5", "hccs", "weno5z"), shape=(12, 16, 12), lo=(0, 0, 0),
              hi=(1.0, 1.5, 1.0), wavy=0.2,
@@ -203,23 +216,46 @@ def generate(cd):
 
 
 DIAG = OUT / "diag"
+MULTI = OUT / "multi"
+
+
+def generate_two_ranks(cd, q0):
+    """The case as two ranks cut in half along xi (periodic xi faces), run for its n
+    steps: multi/<name>.2ranks.npz holds Q of both ranks side by side.  For hccs77 this
+    is not the one-rank result: each block solves its own system with explicit rows at
+    the cut."""
+    case = build_case(cd)
+    if cd["init"] != "tgv":
+        h = cd["shape"][0] // 2
+        case.q0 = [q0[..., :h], q0[..., h:]]
+        case.start_step = 1
+    case = split_xi(case, cd)
+    out = R.run(case, "steps", cd["nsteps"])
+    MULTI.mkdir(exist_ok=True)
+    res = dict(nsteps=np.array([cd["nsteps"]]), q0=q0,
+               qn=np.concatenate([R.stack(o, "Q", 5) for o in out], axis=-1),
+               dt=out[0]["dt"], time=out[0]["time"])
+    np.savez_compressed(MULTI / f"{cd['name']}.2ranks.npz", **res)
+    return res
 
 
 def split_xi(case, cd):
-    """The case as two ranks, the xi range cut in half (periodic xi faces only)."""
+    """The case as two ranks, the xi range cut in half (periodic xi faces only); the
+    other faces keep their kind (periodic ones join the rank to itself)."""
     (x, y, z), = case.nodes
     h = cd["shape"][0] // 2
     nodes = [tuple(a[:, :, :h + 1] for a in (x, y, z)), tuple(a[:, :, h:] for a in (x, y, z))]
     topo = []
     for r in range(2):
         lines = [f"{1 - r} 1", f"{1 - r} 0"]
-        lines += [f"{r} {f ^ 1}" for f in range(2, 6)]
+        lines += [f"{r} {f ^ 1}" if cd["faces"][f] == "periodic" else case.bc_topo[0][f]
+                  for f in range(2, 6)]
         topo.append(lines)
     case.nodes, case.bc_topo = nodes, topo
     return case
 
 
-TILESIZE = {"weno7js": 4, "hccs": 4, "weno3js": 2, "upwind1st": 1}
+TILESIZE = {"weno7js": 4, "hccs": 4, "hccs77": 4, "weno3js": 2, "upwind1st": 1}
 VIS_REACH = {"cd2": 1, "cd6": 3, "cd8": 4}
 
 
@@ -265,6 +301,9 @@ def main(names=None, diag_only=False):
             o = generate(cd)
             extra = f" libm_rel_diff={o['libm_max_rel_diff'][0]:.3g}" if "libm_max_rel_diff" in o else ""
             print(f"{cd['name']}: dt_local={o['dt_local'][0]:.6g} dt={o['dt']}{extra}")
+            if cd.get("ranks2"):
+                t = generate_two_ranks(cd, o["q0"])
+                print(f"{cd['name']} 2 ranks: dt={t['dt']}")
         if not diag_defined(cd):
             print(f"{cd['name']} diag: skipped (the reference's difference reads past its tile)")
             continue

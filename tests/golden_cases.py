@@ -53,6 +53,25 @@ TWO_BLOCK_TYPES = [[1, 1, 0, 0, 0, 0], [0, 0, 1, 1, 1, 1]]
 TWO_BLOCK_IDS = [[1, 0, 3, 2, 5, 4], [1, 0, 3, 2, 5, 4]]
 
 
+def two_block_bc(g: Golden, b: int):
+    """BC arrays of block b (0 left, 1 right) of the case cut in half along xi: the xi
+    faces join the two blocks, the other faces keep the case's (periodic ones point at
+    the block itself)."""
+    t, i, v = bc_arrays(g, b)
+    t[0], i[0], t[1], i[1] = 1 - b, 1, 1 - b, 0
+    return t, i, v
+
+
+def multi_names():
+    """Cases with a two-rank fixture (golden/multi/<name>.2ranks.npz)."""
+    return sorted(p.name[:-len(".2ranks.npz")] for p in (GOLDEN / "multi").glob("*.2ranks.npz"))
+
+
+def load_multi(name: str) -> dict:
+    z = np.load(GOLDEN / "multi" / f"{name}.2ranks.npz")
+    return {k: z[k] for k in z.files}
+
+
 def load(name: str) -> Golden:
     z = np.load(GOLDEN / f"{name}.npz")
     data = {k: z[k] for k in z.files}

@@ -58,7 +58,7 @@ def test_golden_fixtures_consistent():
     (("weno3js",) * 3, ("cd6",) * 3, 5),              # cd6 reaches 3 > bufferSize 2
     (("upwind1st", "weno5js", "weno5js"), ("cd2",) * 3, None),  # cd2 reaches 1: allowed
     (("weno5js",) * 3, ("cd8", "cd6", "cd6"), 5),     # cd8 reaches 4 > bufferSize 3
-    (("hccs77",) * 3, ("cd6",) * 3, 5),               # not implemented
+    (("hccs77",) * 3, ("cd8",) * 3, None),            # cd8 reaches 4 = hccs77's bufferSize
     (("weno5js",) * 3, ("cd4",) * 3, 1),              # unknown name
 ])
 def test_create_rejects_undefined_viscous_pairs(ivs, vis, code):

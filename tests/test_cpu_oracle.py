@@ -74,6 +74,27 @@ def test_oracle_diag_two_blocks_bitwise():
     assert np.array_equal(np.concatenate(f, axis=-1), d["fields"])
 
 
+@pytest.mark.parametrize("name", G.multi_names())
+def test_oracle_two_ranks_bitwise(name):
+    """The reference run as two ranks cut along xi, n steps: each block's own system
+    (hccs77 solves per block, so this is not the one-rank result)."""
+    g, mr = G.load(name), G.load_multi(name)
+    m = O.metrics(*G.nodes(g))
+    h = g.cfg["shape"][0] // 2
+    keys = ("jac", "xi_xyz", "eta_xyz", "zeta_xyz", "dxyz")
+    left, right = G.split_xi([m[k] for k in keys] + [mr["q0"]], h)
+    r = O.Run(g.cfg["schemes"], g.cfg["riemann"], g.cfg["model"], g.cfg["params"], vis=G.vis(g))
+    for b, part in enumerate((left, right)):
+        mb = {k: np.ascontiguousarray(a) for k, a in zip(keys, part[:5])}
+        t, i, v = G.two_block_bc(g, b)
+        r.add_block(mb, t, i, v, np.ascontiguousarray(part[5]))
+    dt, t = r.step(int(mr["nsteps"][0]))
+    assert np.array_equal(dt, mr["dt"]) and t == mr["time"][-1]
+    q = np.concatenate([r.q(0), r.q(1)], axis=-1)
+    assert np.array_equal(q, mr["qn"]), np.max(np.abs(q - mr["qn"]))
+    assert not np.array_equal(q, g.qn)
+
+
 def test_oracle_uneven_blocks_bitwise():
     """24 uneven blocks of decaying turbulence (tests/test_gpu_multiblock_turbulence.py):
     the restatement against the reference run as 24 ranks, 3 steps."""

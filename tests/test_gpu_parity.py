@@ -57,7 +57,18 @@ def test_fast_mode_roundoff(name):
     s = G.solver(g, exact=False)
     n = int(g.cfg["nsteps"])
     s.step(n)
-    assert rel_max(s.get_q(0), g.qn) < FAST_RTOL
+    assert rel_max(s.get_q(0), g.qn) < fast_rtol(g)
+
+
+def fast_rtol(g):
+    """FAST_RTOL, or 100 times the case's own sensitivity to one-ulp changes where that is
+    larger: libm_max_rel_diff is how far the reference's stock-glibc-pow build lands from
+    its correctly rounded one after the same steps.  The hccs/hccs77 weights (eps 1e-40,
+    tau / is of two near-zero indicators on the smooth Taylor-Green field) amplify
+    rounding by ~1e3 there, and FMA contraction changes many more operations by an ulp
+    than pow does."""
+    sens = float(g.libm_max_rel_diff[0]) if "libm_max_rel_diff" in g.data else 0.0
+    return max(FAST_RTOL, 100.0 * sens)
 
 
 @pytest.mark.gpu
@@ -103,7 +114,70 @@ def test_two_blocks_equal_one(name):
     ("tgv_ns_weno5js_lf", 3 * (2 + 3)),                    # periodic: NS passes + 3 sweeps
     ("hccs_ns_ausm_bc", 3 * (1 + 2 + 3 * 3)),              # compact: 3 kernels per direction
     ("mixed_compact_ausmp", 3 * (1 + 3 + 3 + 1)),          # crweno5, hccs, weno5z
+    ("mixed_hccs77_euler_ausmp", 3 * (1 + 3 + 1 + 3)),     # hccs77, weno5z, hccs77
 ])
 def test_kernels_per_step(name, expected):
     g = G.load(name)
     assert G.solver(g, exact=False).kernels_per_step() == expected
+
+
+def _two_rank_solver(g, exact):
+    import nuc3d_b200 as nb
+    mr = G.load_multi(g.name)
+    nx, ny, nz = g.cfg["shape"]
+    x, y, z = G.nodes(g)
+    h = nx // 2
+    s = nb.Solver(G.nuc3d_config(g, exact=exact))
+    blocks = []
+    for b, (lo, hi) in enumerate(((0, h), (h, nx))):
+        t, i, v = G.two_block_bc(g, b)
+        blocks.append(s.add_block(hi - lo, ny, nz, t, i, v))
+        s.set_mesh(blocks[b], x[:, :, lo:hi + 1], y[:, :, lo:hi + 1], z[:, :, lo:hi + 1])
+    s.finalize()
+    for b, (lo, hi) in enumerate(((0, h), (h, nx))):
+        s.set_q(blocks[b], mr["q0"][..., lo:hi])
+    return s, mr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", G.multi_names())
+def test_two_ranks_bitwise(name):
+    """The reference run as two ranks cut along xi (hccs77: one tridiagonal system per
+    block line, with the WENO7-Z rows at the cut) against two blocks of one context."""
+    g = G.load(name)
+    s, mr = _two_rank_solver(g, exact=True)
+    s.step(int(mr["nsteps"][0]))
+    q = np.concatenate([s.get_q(0), s.get_q(1)], axis=3)
+    assert np.array_equal(q, mr["qn"]), f"rel {rel_max(q, mr['qn']):.3g}"
+    t, dt = s.time_dt()
+    assert dt == mr["dt"][-1] and t == mr["time"][-1]
+    s, mr = _two_rank_solver(g, exact=False)
+    s.step(int(mr["nsteps"][0]))
+    q = np.concatenate([s.get_q(0), s.get_q(1)], axis=3)
+    assert rel_max(q, mr["qn"]) < fast_rtol(g)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,faces,ok", [
+    ((16, 12, 12), "periodic", True),
+    ((16, 12, 12), "outlet_xi", False),     # physical face on the hccs77 direction
+    ((127, 12, 12), "periodic", True),      # 128 rows along xi: fits
+    ((128, 12, 12), "periodic", False),     # row 128 would be the next line's row 0
+    ((16, 129, 12), "periodic", False),     # more than 128 lines across
+])
+def test_hccs77_defined_blocks_only(n, faces, ok):
+    """hccs77 is accepted only where the reference's hccs77 is defined: neighbour faces on
+    its direction and lines that fit its 128^3 row arrays (NUC3D_ENOTSUP otherwise)."""
+    import nuc3d_b200 as nb
+    s = nb.Solver(nb.Config(scheme_ivs=("hccs77", "weno5js", "weno5js"), riemann="LF",
+                            model="Euler3d", exact=True))
+    t, i = [0] * 6, [1, 0, 3, 2, 5, 4]
+    if faces == "outlet_xi":
+        t[1], i[1] = -1, 1
+    if ok:
+        s.add_block(*n, t, i)
+    else:
+        with pytest.raises(nb.Nuc3dError) as e:
+            s.add_block(*n, t, i)
+        assert e.value.code == 5
+    s.close()
