@@ -25,6 +25,7 @@
  *   nuc3d_step              block::solve: 3 x (RHS; PDEData3d::solve -> tvdrk3rd)
  *                           (src/block.cpp:569-594, src/PDEData3d.cpp:152-170,
  *                           src/TVD-RK3.cpp:16-137), time += dt
+ *   nuc3d_solve_host        the same on host arrays, in place, every step
  *   (MPI halo exchange, src/MPICommunicator.cpp:36-115, has no entry point: blocks
  *    added to one context read each other's cells directly on the device.)
  */
@@ -131,6 +132,13 @@ int nuc3d_block_get_rhs(nuc3d_ctx *ctx, int block, double *rhs);
 /* nsteps TVD-RK3 steps (each: three stages; dt fixed at stage 0 as cfl/max eigenvalue).
    Asynchronous on the context's stream; nuc3d_sync waits and checks the status. */
 int nuc3d_step(nuc3d_ctx *ctx, int nsteps);
+/* block::solve on host arrays (src/block.cpp:569-594, which updates Q_work in place):
+   nsteps steps, each reading every block's Q = U/J from q_host[block] (5N doubles, the
+   nuc3d_block_set_q layout) and writing the new Q back there.  The download of a step and
+   the upload of the next run at the same time in 16 MiB chunks (PCIe is full duplex), so
+   q_host should be pinned (cudaHostAlloc / cudaHostRegister).  Synchronous: returns
+   when q_host holds the last step's state, with nuc3d_sync's status check. */
+int nuc3d_solve_host(nuc3d_ctx *ctx, double *const *q_host, int nsteps);
 int nuc3d_sync(nuc3d_ctx *ctx);
 /* time accumulated over the steps and the dt of the last step */
 int nuc3d_get_time(nuc3d_ctx *ctx, double *time, double *dt);

@@ -33,7 +33,8 @@ BC_INLET, BC_OUTLET, BC_WALL, BC_SYMM = 0, 1, 2, 3
 EXPORTED = (
     "nuc3d_last_error", "nuc3d_create", "nuc3d_destroy", "nuc3d_block_add",
     "nuc3d_block_set_metrics", "nuc3d_finalize", "nuc3d_block_set_q", "nuc3d_block_get_q",
-    "nuc3d_block_q_device", "nuc3d_rhs", "nuc3d_block_get_rhs", "nuc3d_step", "nuc3d_sync",
+    "nuc3d_block_q_device", "nuc3d_rhs", "nuc3d_block_get_rhs", "nuc3d_step", "nuc3d_solve_host",
+    "nuc3d_sync",
     "nuc3d_get_time", "nuc3d_set_time", "nuc3d_get_status", "nuc3d_set_stream",
     "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis", "nuc3d_profile_sweep",
     "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step", "nuc3d_diagnostics", "nuc3d_block_get_diag",
@@ -101,6 +102,7 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_rhs.argtypes = [P, PD]
     lib.nuc3d_block_get_rhs.argtypes = [P, I, PD]
     lib.nuc3d_step.argtypes = [P, I]
+    lib.nuc3d_solve_host.argtypes = [P, ctypes.POINTER(P), I]
     lib.nuc3d_sync.argtypes = [P]
     lib.nuc3d_get_time.argtypes = [P, PD, PD]
     lib.nuc3d_set_time.argtypes = [P, D]
@@ -301,6 +303,14 @@ class Solver:
         _check(self.lib.nuc3d_step(self._ctx, int(n)))
         if sync:
             self.sync()
+
+    def solve_host(self, host_ptrs, n: int = 1) -> None:
+        """n steps on host arrays, in place: every step reads each block's Q from its host
+        pointer (pinned memory for full speed) and writes the new Q back there."""
+        if len(host_ptrs) != len(self.blocks):
+            raise ValueError("one host pointer per block")
+        arr = (ctypes.c_void_p * len(host_ptrs))(*[int(p) for p in host_ptrs])
+        _check(self.lib.nuc3d_solve_host(self._ctx, arr, int(n)))
 
     def sync(self) -> None:
         _check(self.lib.nuc3d_sync(self._ctx))

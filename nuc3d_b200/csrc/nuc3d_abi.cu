@@ -103,6 +103,10 @@ struct nuc3d_ctx {
   DiagDev *d_diag = nullptr;
   double *d_dsums = nullptr, *d_dparts = nullptr;
   SensorDev *d_sensor = nullptr;  // hybrid WENO-Z face sensor (nuc3d_set_sensor)
+  // nuc3d_solve_host: copy streams and events, created by its first call
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_h2d = nullptr, ev_step = nullptr, ev_end = nullptr;
+  std::vector<cudaEvent_t> ev_chunk;
 
   cudaError_t stage(int s, bool rk, bool eig) {
     return exact ? nuc3d::exact::run_stage(L, s, rk, eig) : nuc3d::fast::run_stage(L, s, rk, eig);
@@ -210,6 +214,11 @@ int nuc3d_destroy(nuc3d_ctx *c) {
   if (c->d_blocks) cudaFree(c->d_blocks);
   if (c->d_jobs) cudaFree(c->d_jobs);
   if (c->d_state) cudaFree(c->d_state);
+  for (auto ev : c->ev_chunk) cudaEventDestroy(ev);
+  for (auto ev : {c->ev_start, c->ev_h2d, c->ev_step, c->ev_end})
+    if (ev) cudaEventDestroy(ev);
+  for (auto st : {c->h2d, c->d2h})
+    if (st) cudaStreamDestroy(st);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NUC3D_OK;
@@ -595,6 +604,66 @@ int nuc3d_step(nuc3d_ctx *c, int nsteps) {
     else CUDA_TRY(c->one_step());
   }
   return NUC3D_OK;
+}
+
+// Copy chunks of nuc3d_solve_host: small enough that the upload of chunk j (next step)
+// trails the download of chunk j (this step) by little, large enough that each copy runs
+// at full PCIe speed.
+constexpr size_t kHostChunk = 16u << 20;
+
+int nuc3d_solve_host(nuc3d_ctx *c, double *const *q_host, int nsteps) {
+  if (!c || !q_host) return fail(NUC3D_EINVAL, "null argument");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  if (nsteps < 0) return fail(NUC3D_EINVAL, "nsteps < 0");
+  for (size_t b = 0; b < c->blocks.size(); ++b)
+    if (!q_host[b]) return fail(NUC3D_EINVAL, "q_host[%zu] is null", b);
+  cudaSetDevice(c->device);
+  struct Chunk { int b; size_t off, bytes; };
+  std::vector<Chunk> chunks;
+  for (size_t b = 0; b < c->blocks.size(); ++b) {
+    const size_t total = 5 * (size_t)c->blocks[b].N * sizeof(double);
+    for (size_t off = 0; off < total; off += kHostChunk)
+      chunks.push_back({(int)b, off, std::min(kHostChunk, total - off)});
+  }
+  if (!c->h2d) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+    for (cudaEvent_t *ev : {&c->ev_start, &c->ev_h2d, &c->ev_step, &c->ev_end})
+      CUDA_TRY(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  }
+  while (c->ev_chunk.size() < chunks.size()) {
+    cudaEvent_t ev;
+    CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    c->ev_chunk.push_back(ev);
+  }
+  auto dev = [&](const Chunk &k) { return reinterpret_cast<char *>(c->blocks[k.b].q[0]) + k.off; };
+  auto host = [&](const Chunk &k) { return reinterpret_cast<char *>(q_host[k.b]) + k.off; };
+  // uploads start after the work already queued on the context's stream
+  CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
+  CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_start, 0));
+  for (int s = 0; s < nsteps; ++s) {
+    for (size_t j = 0; j < chunks.size(); ++j) {
+      // the host chunk is read only once the previous step's download has written it
+      if (s > 0) CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_chunk[j], 0));
+      CUDA_TRY(cudaMemcpyAsync(dev(chunks[j]), host(chunks[j]), chunks[j].bytes,
+                               cudaMemcpyHostToDevice, c->h2d));
+    }
+    CUDA_TRY(cudaEventRecord(c->ev_h2d, c->h2d));
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_h2d, 0));
+    if (int r = nuc3d_step(c, 1)) return r;
+    CUDA_TRY(cudaEventRecord(c->ev_step, c->stream));
+    CUDA_TRY(cudaStreamWaitEvent(c->d2h, c->ev_step, 0));
+    for (size_t j = 0; j < chunks.size(); ++j) {
+      CUDA_TRY(cudaMemcpyAsync(host(chunks[j]), dev(chunks[j]), chunks[j].bytes,
+                               cudaMemcpyDeviceToHost, c->d2h));
+      CUDA_TRY(cudaEventRecord(c->ev_chunk[j], c->d2h));
+    }
+  }
+  // the context's stream (and events recorded on it) cover the last download
+  CUDA_TRY(cudaEventRecord(c->ev_end, c->d2h));
+  CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_end, 0));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return check_status(c);
 }
 
 int nuc3d_sync(nuc3d_ctx *c) {
