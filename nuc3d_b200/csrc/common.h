@@ -68,7 +68,13 @@ struct BlockDev {
 };
 
 // Sweep tiles: kTileW lines x kTileL cells along one direction.
-constexpr int kTileW = 4, kTileL = 64;
+#ifndef NUC3D_TILE_W
+#define NUC3D_TILE_W 4
+#endif
+#ifndef NUC3D_TILE_L
+#define NUC3D_TILE_L 64
+#endif
+constexpr int kTileW = NUC3D_TILE_W, kTileL = NUC3D_TILE_L;
 
 // Fills BlockDev::tdiv from n[].  q = (x * tdiv) >> 40 equals x / k exactly for
 // x < 2^24 (the tile count of a block of fewer than 2^32 cells) and k < 2^16.
