@@ -76,13 +76,16 @@ struct BlockDev {
 #endif
 constexpr int kTileW = NUC3D_TILE_W, kTileL = NUC3D_TILE_L;
 
-// Fills BlockDev::tdiv from n[].  q = (x * tdiv) >> 40 equals x / k exactly for
-// x < 2^24 (the tile count of a block of fewer than 2^32 cells) and k < 2^16.
+// Fills BlockDev::tdiv from n[]: the two radices of the tile index decode (decode_tile),
+// chunks and line groups for xi and eta, line groups and outer lines for zeta.
+// q = (x * tdiv) >> 40 equals x / k exactly for x < 2^24 (the tile count of a block of
+// fewer than 2^32 cells) and k < 2^16.
 inline void set_tile_divisors(BlockDev &b) {
   for (int d = 0; d < 3; ++d) {
     const unsigned long long L = (unsigned long long)b.n[d];
     const unsigned long long nW = (unsigned long long)(d == 0 ? b.n[1] : b.n[0]);
-    const unsigned long long k[2] = {(L + kTileL - 1) / kTileL, (nW + kTileW - 1) / kTileW};
+    const unsigned long long nch = (L + kTileL - 1) / kTileL, nwg = (nW + kTileW - 1) / kTileW;
+    const unsigned long long k[2] = {d == 2 ? nwg : nch, d == 2 ? (unsigned long long)b.n[1] : nwg};
     for (int j = 0; j < 2; ++j) b.tdiv[d][j] = ((1ull << 40) + k[j] - 1) / k[j];
   }
 }
@@ -98,7 +101,9 @@ struct FaceJobs {
 
 // The face sensor of the hybrid WENO-Z sweep (sensor.cuh), arranged for the tensor-core
 // inference: BF16 weight pairs in mma.sync m16n8k16 B-fragment order, [k-step][n-tile][lane],
-// and BF16-rounded biases and output weights as floats.
+// and BF16-rounded biases and output weights as floats.  zero_logit: the network's logit
+// for all-zero features (a face inside a uniform region), evaluated once on the GPU by
+// the same tensor-core code when the sensor is set.
 struct SensorDev {
   uint32_t w1[2][4][32][2];
   float b1[32];
@@ -106,6 +111,7 @@ struct SensorDev {
   float b2[32];
   float w3[32];
   float b3;
+  float zero_logit;
 };
 
 struct SolverParams {
@@ -166,6 +172,7 @@ constexpr int kDiagParts = 256;
 void set_error_message(const char *msg);
 
 // configure(): one-time kernel attributes (dynamic shared memory opt-in).
+// run_sensor_zero(): fills S->zero_logit (one warp).
 // tile_count(): CTAs of the dir-sweep over one block of n cells.
 // run_metrics(): block::getJacobians of an nx x ny x nz block from its node coordinates
 // ((n+1) per axis, device arrays); *bad gets 1 for a negative Jacobian.
@@ -174,6 +181,7 @@ void set_error_message(const char *msg);
 // 2 * kDiagParts doubles per block of scratch.
 namespace exact {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
                             long long *where, unsigned long long *count, unsigned long long cap);
 cudaError_t run_metrics(const double *x, const double *y, const double *z, const int n[3],
@@ -185,6 +193,7 @@ int tile_count(int dir, const int n[3]);
 }
 namespace fast {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
                             long long *where, unsigned long long *count, unsigned long long cap);
 cudaError_t run_metrics(const double *x, const double *y, const double *z, const int n[3],

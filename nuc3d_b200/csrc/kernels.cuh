@@ -106,9 +106,15 @@ __host__ __device__ inline size_t rhs_stage_bytes(bool ns) {
   return rhs_prefetch<DIR>(ns) ? (size_t)5 * Tile<DIR>::TW * Tile<DIR>::TL * sizeof(double) : 0;
 }
 
+// Shared memory of the hybrid sweep: its copy of the sensor weights, then one decision
+// byte per face item of the tile (16-byte multiples).
+constexpr size_t kSensorSmem = ((sizeof(SensorDev) + 15) / 16) * 16;
+constexpr size_t kHybSmem = kSensorSmem + ((size_t)(kTW * (kTL + 1)) + 15) / 16 * 16;
+
 __device__ __forceinline__ void cp_async8(double *dst_smem, const double *src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  const size_t g = __cvta_generic_to_global(src);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(g) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -412,15 +418,25 @@ __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ bloc
   T.B = &blocks[T.b];
   for (int d = 0; d < 3; ++d) T.n[d] = T.B->n[d];
   T.G = make_geo(DIR, T.n);
-  // tile = (chunk along the line) + nch * ((line group) + nwg * (outer index))
+  // xi, eta: tile = (chunk along the line) + nch * ((line group) + nwg * (outer index)).
+  // zeta: tile = (line group) + nwg * ((outer index) + nO * (chunk)): the CTAs resident at
+  // one time then share one chunk of z-planes (3% faster at 256^3 than chunk-fastest,
+  // whose CTAs spread over every plane at 512 KB strides).
   const unsigned lt = (unsigned)(T.t - tm.tile_start[T.b]);
   const unsigned nch = (unsigned)(T.G.L + TL - 1) / TL;
   const unsigned nwg = (unsigned)(T.G.nW + TW - 1) / TW;
   const unsigned q1 = (unsigned)((lt * T.B->tdiv[DIR][0]) >> 40);
   const unsigned q2 = (unsigned)((q1 * T.B->tdiv[DIR][1]) >> 40);
-  const int ch = (int)(lt - q1 * nch);
-  const int wg = (int)(q1 - q2 * nwg);
-  T.o = (int)q2;
+  int ch, wg;
+  if (DIR == 2) {
+    wg = (int)(lt - q1 * nwg);
+    T.o = (int)(q1 - q2 * (unsigned)T.G.nO);
+    ch = (int)q2;
+  } else {
+    ch = (int)(lt - q1 * nch);
+    wg = (int)(q1 - q2 * nwg);
+    T.o = (int)q2;
+  }
   T.c0 = ch * TL;
   T.cl = min(TL, T.G.L - T.c0);
   T.w0 = wg * TW;
@@ -667,23 +683,6 @@ __device__ __forceinline__ void reduce_eig(double emax, double *sRed, StepState 
 
 #include "sensor.cuh"
 
-// The five reconstructions of one boundary-scheme face, out of line: the hybrid sweep's
-// hot loop stays small.
-template <int DIR, int SCH>
-__device__ __noinline__ void edge_faces_of_line(const TileCtx &T, int f, int fl, int w,
-                                                const double *sF, double *sH) {
-  using M = TileSmem<DIR, SCH>;
-  constexpr int R = M::R, TW = M::TW, SP = M::SP, SH = M::SH;
-  for (int v = 0; v < 5; ++v) {
-    const double *rowP = sF + (v * TW + w) * SP + (R - T.c0);
-    const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - T.c0);
-    auto Pacc = [rowP](int c) { return rowP[c]; };
-    auto Nacc = [rowN](int c) { return rowN[c]; };
-    sH[(v * TW + w) * SH + fl] =
-        edge_face<SCH>(f, T.G.L, T.ts, T.physR, T.c0 - R, T.c0 - R + M::NP - 1, Pacc, Nacc);
-  }
-}
-
 // Explicit-scheme sweep: phases split -> faces -> cells in one CTA.  HYB: the hybrid
 // WENO-Z face loop of the throughput build (P.sensor set).
 template <int DIR, int SCH, bool HYB = false>
@@ -699,14 +698,25 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   double *sV = sH + 5 * TW * SH;            // [4][TW][SV]: viscous fluxes (NS)
   double *sQ = sV + (ns ? 4 * TW * SV : 0); // [5][TW][SQ]: stage state (zeta sweep)
   double *sRP = sQ + (DIR == 2 ? 5 * TW * M::SQ : 0);  // hybrid: [2][TW][SP] rho, p
+  // hybrid: the sensor's weights; plain: the staged RHS
+  SensorDev *sS = reinterpret_cast<SensorDev *>(sRP + (HYB ? 2 * TW * SP : 0));
+  unsigned char *sLin = reinterpret_cast<unsigned char *>(sS) + kSensorSmem;  // hybrid: [TW*(TL+1)]
+  double *sRst = reinterpret_cast<double *>(reinterpret_cast<char *>(sS) + (HYB ? kHybSmem : 0));
   __shared__ double sRed[kThreads / 32];
 
   const TileCtx T = decode_tile<DIR>(blocks, tm, P);
   const bool eig = (flags & SW_EIG) != 0;
   unsigned st = 0;
   double emax = 0.0;
-  // !HYB: sRP's place holds the staged RHS instead
-  double *sR = (!HYB && rhs_prefetch<DIR>(ns)) ? sRP : nullptr;
+  // (the hybrid sweep measured slower with the staged RHS: its tile is larger already)
+  double *sR = (!HYB && rhs_prefetch<DIR>(ns)) ? sRst : nullptr;
+  if constexpr (HYB) {
+    // the network's weights, read by every warp's inference: shared memory
+    static_assert(sizeof(SensorDev) % 4 == 0, "word copy");
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(P.sensor);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(sS);
+    for (int i = threadIdx.x; i < (int)(sizeof(SensorDev) / 4); i += kThreads) dst[i] = src[i];
+  }
   if (sR) {
     // each thread stages the RHS of the cells it finishes in phase_cells (same mapping),
     // so its own wait_all orders them; no barrier needed
@@ -737,60 +747,44 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   const int ei = TW * ni, e0 = (ei + 31) & ~31;
   const float rni = ni > 0 ? 1.0f / (float)ni : 0.0f, rne = ne > 0 ? 1.0f / (float)ne : 0.0f;
   if constexpr (HYB) {
-    // hybrid WENO-Z: the face sensor picks linear or nonlinear weights per interior face.
-    // The loop runs the same number of rounds in every thread: the sensor is warp-collective.
-    for (int base = 0; base < e0 + TW * ne; base += kThreads) {
+    // hybrid WENO-Z, pass 1: the face sensor's decision for every interior face item
+    // (linear weights or WENO-Z), into sLin.  Rounds are the same in every thread: the
+    // inference is warp-collective.  Pass 2 is the face loop below; keeping the network
+    // out of it keeps its registers out of the reconstructions' (measured 2x faster than
+    // one loop doing both).
+    // 1a: per-gap values (F+ differences, jumps) into sG, in sH's place (sH is written
+    // only in pass 2)
+    float *sG = reinterpret_cast<float *>(sH);
+    constexpr int NG = M::NP - 1;
+    static_assert(kSensorGapVals * TW * SP * sizeof(float) <= 5 * TW * SH * sizeof(double),
+                  "gap values fit in the face-flux tile");
+    for (int e = threadIdx.x; e < TW * NG; e += kThreads) {
+      const int w = e / NG, p = e - w * NG;
+      if (w >= T.nw) continue;
+      const double *rowF[5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) rowF[v] = sF + (v * TW + w) * SP;
+      sensor_gap(rowF, sRP + w * SP, sRP + (TW + w) * SP, p, sG + w * SP + p, TW * SP);
+    }
+    __syncthreads();
+    // 1b: features, network, decision
+    for (int base = 0; base < ei; base += kThreads) {
       const int e = base + threadIdx.x;
       int w = 0, fl = 0;
-      bool edge = false, valid = true;
       if (e < ei) {
         w = __float2int_rz(((float)e + 0.5f) * rni);
         fl = lo + (e - w * ni);
-      } else if (e >= e0 && e < e0 + TW * ne) {
-        const int j = e - e0;
-        w = __float2int_rz(((float)j + 0.5f) * rne);
-        const int k = j - w * ne;
-        fl = k < nl ? k : hi + (k - nl);
-        edge = true;
-      } else {
-        valid = false;
       }
-      valid = valid && w < T.nw;
+      const bool valid = e < ei && w < T.nw;
       uint32_t xr[10];
 #pragma unroll
       for (int i = 0; i < 10; ++i) xr[i] = 0u;
-      if (valid && !edge) {
-        const double *rows[5];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) rows[v] = sF + (v * TW + w) * SP + (R + fl);
-        sensor_features_packed(rows, sRP + w * SP + (R + fl), sRP + (TW + w) * SP + (R + fl), xr);
-      }
-      const float logit = sensor_logit(P.sensor, xr);
-      if (!valid) continue;
-      const int f = T.c0 + fl;
-      if (!edge && logit < P.sensor_threshold) {
-#pragma unroll 1
-        for (int v = 0; v < 5; ++v) {
-          const double *rowP = sF + (v * TW + w) * SP + (R + fl);
-          const double *rowN = sF + ((5 + v) * TW + w) * SP + (R + fl);
-          sH[(v * TW + w) * SH + fl] = weno5_linear(rowP[-3], rowP[-2], rowP[-1], rowP[0], rowP[1]) +
-                                       weno5_linear(rowN[2], rowN[1], rowN[0], rowN[-1], rowN[-2]);
-        }
-      } else if (!edge) {
-        const bool cz = compat && f >= T.ts && f <= T.G.L - T.ts;
-#pragma unroll 1
-        for (int v = 0; v < 5; ++v) {
-          const double *rowP = sF + (v * TW + w) * SP + (R + fl);
-          const double *rowN = sF + ((5 + v) * TW + w) * SP + (R + fl);
-          auto Pacc = [rowP](int c) { return rowP[c]; };
-          auto Nacc = [rowN](int c) { return rowN[c]; };
-          sH[(v * TW + w) * SH + fl] = recon_pos_in<SCH>(0, cz, Pacc) + recon_neg_in<SCH>(0, Nacc);
-        }
-      } else {
-        edge_faces_of_line<DIR, SCH>(T, f, fl, w, sF, sH);
-      }
+      if (valid) sensor_features_gaps(sG + w * SP + (R + fl - 3), TW * SP, xr);
+      const float logit = sensor_logit(sS, xr);
+      if (valid) sLin[e] = logit < P.sensor_threshold ? 1 : 0;
     }
-  } else
+    __syncthreads();
+  }
   for (int e = threadIdx.x; e < e0 + TW * ne; e += kThreads) {
     // w = e / ni by a float reciprocal: exact, since (e + 1/2) / ni stays at least
     // 1/(2 ni) away from an integer and e < 2^9.
@@ -811,7 +805,16 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     }
     if (w >= T.nw) continue;
     const int f = T.c0 + fl;
-    if (!edge) {
+    if (HYB && !edge && sLin[e]) {
+      // hybrid: a face the sensor calls smooth takes the linear weights (0.1, 0.6, 0.3)
+#pragma unroll 1
+      for (int v = 0; v < 5; ++v) {
+        const double *rowP = sF + (v * TW + w) * SP + (R + fl);
+        const double *rowN = sF + ((5 + v) * TW + w) * SP + (R + fl);
+        sH[(v * TW + w) * SH + fl] = weno5_linear(rowP[-3], rowP[-2], rowP[-1], rowP[0], rowP[1]) +
+                                     weno5_linear(rowN[2], rowN[1], rowN[0], rowN[-1], rowN[-2]);
+      }
+    } else if (!edge) {
       const bool cz = compat && f >= T.ts && f <= T.G.L - T.ts;
 #pragma unroll 2  // two variables per iteration: measured 3% faster than none, and than five
       for (int v = 0; v < 5; ++v) {
@@ -1478,7 +1481,8 @@ metrics_kernel(const double *__restrict__ x, const double *__restrict__ y,
 // Shared memory of the hybrid sweep: the plain sweep's plus rho and p per position.
 template <int DIR, int SCH>
 __host__ __device__ inline size_t hybrid_smem_bytes(bool ns) {
-  return sweep_smem_bytes<DIR, SCH>(ns) + (size_t)2 * kTW * TileSmem<DIR, SCH>::SP * sizeof(double);
+  return sweep_smem_bytes<DIR, SCH>(ns) + (size_t)2 * kTW * TileSmem<DIR, SCH>::SP * sizeof(double) +
+         kHybSmem;
 }
 
 template <int DIR, int SCH>
@@ -1634,9 +1638,10 @@ template <int DIR, int SCH>
 inline cudaError_t configure_t() {
 #if NUC3D_FAST
   if constexpr (SCH == SCH_WENO5Z) {
+    const size_t he = hybrid_smem_bytes<DIR, SCH>(false), hn = hybrid_smem_bytes<DIR, SCH>(true);
     const cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIR, SCH, true>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)hybrid_smem_bytes<DIR, SCH>(true));
+                                               (int)(he > hn ? he : hn));
     if (e != cudaSuccess) return e;
   }
 #endif

@@ -860,6 +860,7 @@ int nuc3d_set_sensor(nuc3d_ctx *c, const float *params, float logit_threshold) {
   h.b3 = bf16_value(params[1728]);
   if (!c->d_sensor) CUDA_TRY(cudaMalloc(&c->d_sensor, sizeof(SensorDev)));
   CUDA_TRY(cudaMemcpy(c->d_sensor, &h, sizeof(SensorDev), cudaMemcpyHostToDevice));
+  CUDA_TRY(nuc3d::fast::run_sensor_zero(c->d_sensor, c->stream));
   c->P.sensor = c->L.P.sensor = c->d_sensor;
   c->P.sensor_threshold = c->L.P.sensor_threshold = logit_threshold;
   return NUC3D_OK;

@@ -161,12 +161,15 @@ __device__ __forceinline__ uint32_t gather_pair(const uint32_t xr[10], int base,
   return v;
 }
 
-// The logit of this lane's face.  xr: the lane's 19 features as BF16 pairs (pair 9 holds
-// feature 18 and a zero).
-__device__ __forceinline__ float sensor_logit(const SensorDev *__restrict__ S, const uint32_t xr[10]) {
+// The logit of this lane's face by the network.  xr: the lane's 19 features as BF16 pairs
+// (pair 9 holds feature 18 and a zero).  S may point to global or shared memory: generic
+// loads only (no __ldg, whose non-coherent global path cannot read shared memory).  The
+// two m-tiles run unrolled: their independent chains overlap (the unrolled form measured
+// 25% off the hybrid step at 256^3).
+__device__ __forceinline__ float sensor_logit_net(const SensorDev *S, const uint32_t xr[10]) {
   const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
   float mine = 0.0f;
-#pragma unroll 1
+#pragma unroll
   for (int mt = 0; mt < 2; ++mt) {
     const int r0 = mt * 16 + g, r8 = r0 + 8;  // owner lanes of fragment rows g, g+8
     float c[4][4];
@@ -181,7 +184,7 @@ __device__ __forceinline__ float sensor_logit(const SensorDev *__restrict__ S, c
       const uint32_t a2 = gather_pair(xr, ks * 8 + 4, q, r0), a3 = gather_pair(xr, ks * 8 + 4, q, r8);
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt) {
-        const uint2 bw = __ldg(reinterpret_cast<const uint2 *>(S->w1[ks][nt][lane]));
+        const uint2 bw = *reinterpret_cast<const uint2 *>(S->w1[ks][nt][lane]);
         mma_bf16(c[nt], a0, a1, a2, a3, bw.x, bw.y);
       }
     }
@@ -201,7 +204,7 @@ __device__ __forceinline__ float sensor_logit(const SensorDev *__restrict__ S, c
       float d[4] = {S->b2[n0], S->b2[n0 + 1], S->b2[n0], S->b2[n0 + 1]};
 #pragma unroll
       for (int ks = 0; ks < 2; ++ks) {
-        const uint2 bw = __ldg(reinterpret_cast<const uint2 *>(S->w2[ks][nt][lane]));
+        const uint2 bw = *reinterpret_cast<const uint2 *>(S->w2[ks][nt][lane]);
         mma_bf16(d, h[ks][0], h[ks][1], h[ks][2], h[ks][3], bw.x, bw.y);
       }
       pg += bf16_round(fmaxf(d[0], 0.0f)) * S->w3[n0] + bf16_round(fmaxf(d[1], 0.0f)) * S->w3[n0 + 1];
@@ -219,21 +222,64 @@ __device__ __forceinline__ float sensor_logit(const SensorDev *__restrict__ S, c
   return mine;
 }
 
-// The 19 features of one face, packed as BF16 pairs, for the inference: the stencil
-// differences in FP64 (they cancel), everything after them in FP32 with fast reciprocals
-// (the network reads BF16).  rowP[v]: F+ of variable v at line position face + c;
-// rr, pp: density and pressure likewise.
-__device__ __forceinline__ void sensor_features_packed(const double *const rowP[5],
-                                                       const double *rr, const double *pp,
-                                                       uint32_t xr[10]) {
+// The logit of this lane's face.  A warp whose 32 faces all have zero features (inside a
+// uniform region) takes the network's precomputed output for zero input: each output
+// row of the mma depends on its own row of features only, so this is the value the
+// network would return for them.
+__device__ __forceinline__ float sensor_logit(const SensorDev *S, const uint32_t xr[10]) {
+  uint32_t any = 0u;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) any |= xr[i];
+  if (__all_sync(0xffffffffu, any == 0u)) return S->zero_logit;
+  return sensor_logit_net(S, xr);
+}
+
+__global__ void sensor_zero_kernel(SensorDev *S) {
+  uint32_t xr[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) xr[i] = 0u;
+  const float z = sensor_logit_net(S, xr);
+  if (threadIdx.x == 0) S->zero_logit = z;
+}
+
+cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st) {
+  sensor_zero_kernel<<<1, 32, 0, st>>>(S);
+  return cudaGetLastError();
+}
+
+// The sweep's features are built from per-gap values that neighbouring faces share.
+// Gap p of a line joins tile positions p and p+1; sG holds, per gap, the first
+// differences of the 5 variables' F+ (FP64 subtraction, then FP32) and the relative
+// density and pressure jumps: sG[k][w][p], k = 0..4 differences, 5 density, 6 pressure.
+constexpr int kSensorGapVals = 7;
+
+__device__ __forceinline__ float rel_jump_f(float a, float b) {
+  return fabsf(b - a) * __frcp_rn(fabsf(a) + fabsf(b) + 1e-30f);
+}
+
+// Gap p of line w: rowF[v] = F+ of variable v at position 0 of the line, rr/pp = density
+// and pressure likewise; out[k] is sG[k][w] (stride gs floats between k).
+__device__ __forceinline__ void sensor_gap(const double *const rowF[5], const double *rr,
+                                           const double *pp, int p, float *out, int gs) {
+#pragma unroll
+  for (int v = 0; v < 5; ++v) out[v * gs] = (float)(rowF[v][p + 1] - rowF[v][p]);
+  out[5 * gs] = rel_jump_f((float)rr[p], (float)rr[p + 1]);
+  out[6 * gs] = rel_jump_f((float)pp[p], (float)pp[p + 1]);
+}
+
+// The 19 features of one face from the gaps g = first gap of its stencil (cells f-3, f-2)
+// .. g+4, packed as BF16 pairs: the WENO5 smoothness indicators of F+ rewritten on first
+// differences D0..D3 of the stencil f-3..f+1 (d = second difference, e = the indicator's
+// first-derivative term), normalised by their sum + 1e-6, then the jumps across the face
+// and their maxima over the stencil, as in sensor_data_kernel.
+__device__ __forceinline__ void sensor_features_gaps(const float *g, int gs, uint32_t xr[10]) {
   float x[kSensorIn];
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
-    const double *r = rowP[v];
-    const double f0 = r[-3], f1 = r[-2], f2 = r[-1], f3 = r[0], f4 = r[1];
-    const float d0 = (float)(f0 - 2.0 * f1 + f2), e0 = (float)(f0 - 4.0 * f1 + 3.0 * f2);
-    const float d1 = (float)(f1 - 2.0 * f2 + f3), e1 = (float)(f1 - f3);
-    const float d2 = (float)(f2 - 2.0 * f3 + f4), e2 = (float)(3.0 * f2 - 4.0 * f3 + f4);
+    const float D0 = g[v * gs], D1 = g[v * gs + 1], D2 = g[v * gs + 2], D3 = g[v * gs + 3];
+    const float d0 = D1 - D0, e0 = 3.0f * D1 - D0;
+    const float d1 = D2 - D1, e1 = D1 + D2;
+    const float d2 = D3 - D2, e2 = D3 - 3.0f * D2;
     const float b0 = (13.0f / 12.0f) * d0 * d0 + 0.25f * e0 * e0;
     const float b1 = (13.0f / 12.0f) * d1 * d1 + 0.25f * e1 * e1;
     const float b2 = (13.0f / 12.0f) * d2 * d2 + 0.25f * e2 * e2;
@@ -242,20 +288,14 @@ __device__ __forceinline__ void sensor_features_packed(const double *const rowP[
     x[3 * v + 1] = b1 * inv;
     x[3 * v + 2] = b2 * inv;
   }
-  float rho[6], pr[6];
+  const float *jr = g + 5 * gs, *jp = g + 6 * gs;
+  x[15] = jr[2];
+  x[16] = jp[2];
+  float mr = jr[0], mp = jp[0];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    rho[c] = (float)rr[c - 3];
-    pr[c] = (float)pp[c - 3];
-  }
-  auto jump = [](float a, float b) { return fabsf(b - a) * __frcp_rn(fabsf(a) + fabsf(b) + 1e-30f); };
-  x[15] = jump(rho[2], rho[3]);
-  x[16] = jump(pr[2], pr[3]);
-  float mr = 0.0f, mp = 0.0f;
-#pragma unroll
-  for (int c = 0; c < 5; ++c) {
-    mr = fmaxf(mr, jump(rho[c], rho[c + 1]));
-    mp = fmaxf(mp, jump(pr[c], pr[c + 1]));
+  for (int c = 1; c < 5; ++c) {
+    mr = fmaxf(mr, jr[c]);
+    mp = fmaxf(mp, jp[c]);
   }
   x[17] = mr;
   x[18] = mp;
