@@ -750,8 +750,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     // hybrid WENO-Z, pass 1: the face sensor's decision for every interior face item
     // (linear weights or WENO-Z), into sLin.  Rounds are the same in every thread: the
     // inference is warp-collective.  Pass 2 is the face loop below; keeping the network
-    // out of it keeps its registers out of the reconstructions' (measured 2x faster than
-    // one loop doing both).
+    // out of it keeps its registers out of the reconstructions'.
     // 1a: per-gap values (F+ differences, jumps) into sG, in sH's place (sH is written
     // only in pass 2)
     float *sG = reinterpret_cast<float *>(sH);
