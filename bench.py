@@ -284,6 +284,8 @@ def ours(args):
     stream = torch.cuda.Stream(device=dev)
     s.set_stream(stream.cuda_stream)
     s.set_q(b, q0)
+    # sweep tile shapes per direction, timed on this grid (outside every timed region)
+    tiles = s.autotune(reps=3)["shape"]
 
     def barrier():
         if dist is not None:
@@ -349,6 +351,7 @@ def ours(args):
         rho_plain = s.get_q(b)[0]
         s.set_q(b, q0)
         s.set_sensor(SENS.load_weights(), SENS.DEFAULT_THRESHOLD)
+        htiles = s.autotune(reps=3)["shape"]
         s.step(warm)  # includes the capture of the hybrid step graph
         barrier()
         ev4, ev5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -360,12 +363,13 @@ def ours(args):
         hms = max_over_ranks(ev4.elapsed_time(ev5))
         rho_h = s.get_q(b)[0]
         s.set_sensor(None)
+        s.set_tiles(tiles)
         hv = whole_job_rate(world, cells, args.steps, hms)
         hybrid = {"value": hv, "unit": "Mcell-RK3-steps/s", "ms_per_step": hms / args.steps,
                   "vs_plain": hv / value, "logit_threshold": SENS.DEFAULT_THRESHOLD,
                   "l1_density_error_vs_plain": float(np.abs(rho_h - rho_plain).sum() /
                                                      np.abs(rho_plain).sum()),
-                  "steps_compared": warm + args.steps}
+                  "steps_compared": warm + args.steps, "tile_shapes": list(htiles)}
 
     # ---- roofline of the dominant kernel ----
     s.set_q(b, q0)
@@ -407,6 +411,7 @@ def ours(args):
                    "arith": "reference-order (no FMA)" if args.exact else "fast (FMA, 1 div/face)",
                    "l2": "no flush: 3 state buffers of 671 MB + RHS + metrics = 4 GB > 126 MB L2",
                    "parallelism": f"replicas x{world} (one independent block per GPU)",
+                   "tile_shapes": list(tiles),
                    "status_bits": status},
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "Mcell-RK3-steps/s",

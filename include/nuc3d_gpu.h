@@ -196,6 +196,23 @@ int nuc3d_sensor_adam(float *params, const float *grad, float *m, float *v, floa
    NULL to return to plain WENO-Z. */
 int nuc3d_set_sensor(nuc3d_ctx *ctx, const float *params, float logit_threshold);
 
+/* ---- Sweep tile shapes (after nuc3d_finalize) ----------------------------------------
+   No counterpart in the reference.  Each direction's sweep runs tiles of one of
+   NUC3D_TILE_SHAPES shapes (lines x cells along them): 0 = 4 x 64 (default), 1 = 8 x 32,
+   2 = 2 x 128; compact-scheme directions run shape 0.  The results do not depend on the
+   shape (same arithmetic), only the speed does. */
+#define NUC3D_TILE_SHAPES 3
+int nuc3d_set_tiles(nuc3d_ctx *ctx, const int shape[3]);
+int nuc3d_get_tiles(nuc3d_ctx *ctx, int shape[3]);
+/* Time every shape of every explicit-scheme direction's right-hand-side sweep on the
+   current state (reps launches each; the state and the status word are left as they
+   were, the RHS array is overwritten) and keep the fastest per direction.  The choice is cached in the process per grid (block
+   extents, schemes, model, build, hybrid or plain): a later context of the same grid takes
+   it without timing.  shape_out (may be NULL): the shapes chosen; ms_out (may be NULL):
+   9 doubles, ms per launch of direction d with shape s at [3d + s], -1 where not timed
+   (a cached choice, a compact direction). */
+int nuc3d_autotune(nuc3d_ctx *ctx, int reps, int shape_out[3], double ms_out[9]);
+
 /* Kernels one nuc3d_step(ctx, 1) launches (after nuc3d_finalize): per RK stage the BC
    ghost pass (when a block has a physical face), the NS primitive and gradient passes,
    and one sweep per direction (three kernels for a compact-scheme direction).  No

@@ -39,7 +39,8 @@ EXPORTED = (
     "nuc3d_use_graph", "nuc3d_block_get_prim", "nuc3d_block_get_vis", "nuc3d_profile_sweep",
     "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step", "nuc3d_diagnostics", "nuc3d_block_get_diag",
     "nuc3d_block_set_nodes", "nuc3d_block_get_metrics", "nuc3d_sensor_record",
-    "nuc3d_sensor_loss_grad", "nuc3d_sensor_adam", "nuc3d_set_sensor",
+    "nuc3d_sensor_loss_grad", "nuc3d_sensor_adam", "nuc3d_set_sensor", "nuc3d_set_tiles",
+    "nuc3d_get_tiles", "nuc3d_autotune",
 )
 
 
@@ -103,6 +104,9 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_block_get_rhs.argtypes = [P, I, PD]
     lib.nuc3d_step.argtypes = [P, I]
     lib.nuc3d_solve_host.argtypes = [P, ctypes.POINTER(P), I]
+    lib.nuc3d_set_tiles.argtypes = [P, ctypes.POINTER(I)]
+    lib.nuc3d_get_tiles.argtypes = [P, ctypes.POINTER(I)]
+    lib.nuc3d_autotune.argtypes = [P, I, ctypes.POINTER(I), PD]
     lib.nuc3d_sync.argtypes = [P]
     lib.nuc3d_get_time.argtypes = [P, PD, PD]
     lib.nuc3d_set_time.argtypes = [P, D]
@@ -369,6 +373,26 @@ class Solver:
         self._sensor_keep = p
         _check(self.lib.nuc3d_set_sensor(self._ctx, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                          float(logit_threshold)))
+
+    def set_tiles(self, shape) -> None:
+        """Sweep tile shape per direction: 0 = 4 x 64, 1 = 8 x 32, 2 = 2 x 128."""
+        arr = (ctypes.c_int * 3)(*[int(x) for x in shape])
+        _check(self.lib.nuc3d_set_tiles(self._ctx, arr))
+
+    def get_tiles(self) -> tuple:
+        arr = (ctypes.c_int * 3)()
+        _check(self.lib.nuc3d_get_tiles(self._ctx, arr))
+        return tuple(arr)
+
+    def autotune(self, reps: int = 3) -> dict:
+        """Time every tile shape of each direction's sweep on the current state and keep the
+        fastest (cached per grid in this process).  Returns {"shape": (s0, s1, s2),
+        "ms": [[ms of shape 0, 1, 2] per direction] (None where not timed)}."""
+        shp = (ctypes.c_int * 3)()
+        ms = (ctypes.c_double * 9)()
+        _check(self.lib.nuc3d_autotune(self._ctx, int(reps), shp, ms))
+        t = [[(ms[3 * d + k] if ms[3 * d + k] >= 0 else None) for k in range(3)] for d in range(3)]
+        return {"shape": tuple(shp), "ms": t}
 
     def kernels_per_step(self) -> int:
         """Kernels one step launches (the library's own count of its launches)."""

@@ -67,24 +67,24 @@ struct BlockDev {
   unsigned long long tdiv[3][2];
 };
 
-// Sweep tiles: kTileW lines x kTileL cells along one direction.
-#ifndef NUC3D_TILE_W
-#define NUC3D_TILE_W 4
-#endif
-#ifndef NUC3D_TILE_L
-#define NUC3D_TILE_L 64
-#endif
-constexpr int kTileW = NUC3D_TILE_W, kTileL = NUC3D_TILE_L;
+// Sweep tile shapes, chosen per direction (nuc3d_autotune): shape s is tile_w(s) lines x
+// tile_l(s) cells along them; 0: 4 x 64, 1: 8 x 32, 2: 2 x 128.  All hold 256 cells, so
+// every sweep CTA has the same 288 threads.  Compact schemes use shape 0.
+constexpr int kTileShapes = 3;
+__host__ __device__ constexpr int tile_w(int s) { return s == 1 ? 8 : (s == 2 ? 2 : 4); }
+__host__ __device__ constexpr int tile_l(int s) { return s == 1 ? 32 : (s == 2 ? 128 : 64); }
 
-// Fills BlockDev::tdiv from n[]: the two radices of the tile index decode (decode_tile),
-// chunks and line groups for xi and eta, line groups and outer lines for zeta.
-// q = (x * tdiv) >> 40 equals x / k exactly for x < 2^24 (the tile count of a block of
-// fewer than 2^32 cells) and k < 2^16.
-inline void set_tile_divisors(BlockDev &b) {
+// Fills BlockDev::tdiv from n[] and the directions' tile shapes: the two radices of the
+// tile index decode (decode_tile), chunks and line groups for xi and eta, line groups and
+// outer lines for zeta.  q = (x * tdiv) >> 40 equals x / k exactly for x < 2^24 (the tile
+// count of a block of fewer than 2^32 cells) and k < 2^16.
+inline void set_tile_divisors(BlockDev &b, const int shape[3]) {
   for (int d = 0; d < 3; ++d) {
     const unsigned long long L = (unsigned long long)b.n[d];
     const unsigned long long nW = (unsigned long long)(d == 0 ? b.n[1] : b.n[0]);
-    const unsigned long long nch = (L + kTileL - 1) / kTileL, nwg = (nW + kTileW - 1) / kTileW;
+    const unsigned long long TL = (unsigned long long)tile_l(shape[d]),
+                             TW = (unsigned long long)tile_w(shape[d]);
+    const unsigned long long nch = (L + TL - 1) / TL, nwg = (nW + TW - 1) / TW;
     const unsigned long long k[2] = {d == 2 ? nwg : nch, d == 2 ? (unsigned long long)b.n[1] : nwg};
     for (int j = 0; j < 2; ++j) b.tdiv[d][j] = ((1ull << 40) + k[j] - 1) / k[j];
   }
@@ -154,6 +154,7 @@ struct Launch {
   const FaceJobs *d_jobs;  // device copy
   int bc_tiles;            // CTAs of the BC ghost pass (0: no physical faces)
   cudaStream_t stream;
+  int shape[3];            // sweep tile shape per direction (tile_w / tile_l)
 };
 
 // Diagnostics workspace of one block (postproc::solveQ, src/postproc.cpp:743-848):
@@ -173,7 +174,7 @@ void set_error_message(const char *msg);
 
 // configure(): one-time kernel attributes (dynamic shared memory opt-in).
 // run_sensor_zero(): fills S->zero_logit (one warp).
-// tile_count(): CTAs of the dir-sweep over one block of n cells.
+// tile_count(): CTAs of the dir-sweep over one block of n cells with tile shape `shape`.
 // run_metrics(): block::getJacobians of an nx x ny x nz block from its node coordinates
 // ((n+1) per axis, device arrays); *bad gets 1 for a negative Jacobian.
 // run_diag(): the solveQ diagnostics of state q[0] of every block into dd[b] and the
@@ -189,7 +190,7 @@ cudaError_t run_metrics(const double *x, const double *y, const double *z, const
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 cudaError_t configure();
-int tile_count(int dir, const int n[3]);
+int tile_count(int dir, const int n[3], int shape);
 }
 namespace fast {
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
@@ -201,7 +202,7 @@ cudaError_t run_metrics(const double *x, const double *y, const double *z, const
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 cudaError_t configure();
-int tile_count(int dir, const int n[3]);
+int tile_count(int dir, const int n[3], int shape);
 }
 
 }  // namespace nuc3d

@@ -25,11 +25,11 @@
 namespace nuc3d {
 namespace NUC3D_NS {
 
-// Tile of one sweep CTA: TW lines side by side, TL cells along each line.  xi lines
-// are contiguous in memory; eta/zeta tiles put TW consecutive i in a row (one 32-byte
-// sector).  kThreads = TW*TL + 32 makes every phase a single round: TW*(TL+2R) <= 288
-// split fluxes, TW*(TL+1) faces, TW*TL cells, so no warp idles at a barrier waiting
-// for a one-lane tail.
+// Tile of one sweep CTA: TW lines side by side, TL cells along each line, TW*TL = 256
+// in every shape (tile_w / tile_l).  xi lines are contiguous in memory; eta/zeta tiles
+// put TW consecutive i in a row (shape 0: one 32-byte sector).  kThreads = 256 + 32 makes
+// every phase of shape 0 a single round: TW*(TL+2R) <= 288 split fluxes, TW*(TL+1)
+// faces, TW*TL cells, so no warp idles at a barrier waiting for a one-lane tail.
 #ifndef NUC3D_SWEEP_MINB
 #define NUC3D_SWEEP_MINB 4  // resident sweep CTAs per SM the register budget is cut for (measured best)
 #endif
@@ -39,9 +39,11 @@ namespace NUC3D_NS {
 #ifndef NUC3D_RHS_PREFETCH_Z
 #define NUC3D_RHS_PREFETCH_Z 0
 #endif
-constexpr int kTW = kTileW, kTL = kTileL;
-constexpr int kThreads = kTW * kTL + 32;
-template <int DIR> struct Tile { static constexpr int TW = kTW, TL = kTL; };
+constexpr int kThreads = 256 + 32;
+template <int SHP> struct Tile {
+  static constexpr int TW = tile_w(SHP), TL = tile_l(SHP);
+  static_assert(TW * TL == 256, "every tile shape holds 256 cells");
+};
 
 template <int SCH> struct Halo {
   static constexpr int R = (SCH == SCH_WENO7JS || SCH == SCH_HCCS) ? 4
@@ -72,16 +74,15 @@ __host__ __device__ inline Geo make_geo(int dir, const int n[3]) {
   return g;
 }
 
-template <int DIR>
-__host__ __device__ inline int sweep_tiles(const int n[3]) {
-  Geo g = make_geo(DIR, n);
-  return ((g.L + Tile<DIR>::TL - 1) / Tile<DIR>::TL) * ((g.nW + Tile<DIR>::TW - 1) / Tile<DIR>::TW) *
-         g.nO;
+__host__ __device__ inline int sweep_tiles(int dir, const int n[3], int shape) {
+  Geo g = make_geo(dir, n);
+  const int TL = tile_l(shape), TW = tile_w(shape);
+  return ((g.L + TL - 1) / TL) * ((g.nW + TW - 1) / TW) * g.nO;
 }
 
-template <int DIR, int SCH>
+template <int DIR, int SCH, int SHP = 0>
 __host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
-  constexpr int R = Halo<SCH>::R, TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
+  constexpr int R = Halo<SCH>::R, TW = Tile<SHP>::TW, TL = Tile<SHP>::TL;
   size_t n = (size_t)10 * TW * pad_row(TL + 2 * R) + (size_t)5 * TW * pad_row(TL + 1);
   if (ns) n += (size_t)4 * TW * pad_row(TL + 2 * kVisHalo);
   if (DIR == 2) n += (size_t)5 * TW * pad_row(TL);
@@ -103,13 +104,15 @@ __host__ __device__ constexpr bool rhs_prefetch(bool ns) {
 }
 template <int DIR>
 __host__ __device__ inline size_t rhs_stage_bytes(bool ns) {
-  return rhs_prefetch<DIR>(ns) ? (size_t)5 * Tile<DIR>::TW * Tile<DIR>::TL * sizeof(double) : 0;
+  return rhs_prefetch<DIR>(ns) ? (size_t)5 * 256 * sizeof(double) : 0;
 }
 
 // Shared memory of the hybrid sweep: its copy of the sensor weights, then one decision
 // byte per face item of the tile (16-byte multiples).
 constexpr size_t kSensorSmem = ((sizeof(SensorDev) + 15) / 16) * 16;
-constexpr size_t kHybSmem = kSensorSmem + ((size_t)(kTW * (kTL + 1)) + 15) / 16 * 16;
+constexpr int kMaxFaceItems = 8 * (32 + 1);  // TW * (TL + 1), largest over the shapes
+static_assert(kMaxFaceItems >= 4 * (64 + 1) && kMaxFaceItems >= 2 * (128 + 1), "face items");
+constexpr size_t kHybSmem = kSensorSmem + ((size_t)kMaxFaceItems + 15) / 16 * 16;
 
 __device__ __forceinline__ void cp_async8(double *dst_smem, const double *src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
@@ -408,10 +411,10 @@ struct TileCtx {
   bool physL, physR;
 };
 
-template <int DIR>
+template <int DIR, int SHP = 0>
 __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ blocks, const TileMap &tm,
                                                const SolverParams &P) {
-  constexpr int TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
+  constexpr int TW = Tile<SHP>::TW, TL = Tile<SHP>::TL;
   TileCtx T;
   T.t = blockIdx.x;
   T.b = find_block(tm, T.t);
@@ -449,8 +452,8 @@ __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ bloc
 }
 
 // Shared-memory row strides of a sweep tile.
-template <int DIR, int SCH> struct TileSmem {
-  static constexpr int R = Halo<SCH>::R, TW = Tile<DIR>::TW, TL = Tile<DIR>::TL;
+template <int DIR, int SCH, int SHP = 0> struct TileSmem {
+  static constexpr int R = Halo<SCH>::R, TW = Tile<SHP>::TW, TL = Tile<SHP>::TL;
   static constexpr int NP = TL + 2 * R, SP = pad_row(NP);
   static constexpr int NV = TL + 2 * kVisHalo, SV = pad_row(NV);
   static constexpr int SH = pad_row(TL + 1), SQ = pad_row(TL);
@@ -459,12 +462,12 @@ template <int DIR, int SCH> struct TileSmem {
 // Phase 1: split fluxes F+/F- of the tile's line positions c0-R .. c0+cl+R-1 into sF
 // ([10][TW][SP]); own cells of the zeta tile also leave their state in sQ; eig reduces
 // max(|U|+c|grad xi|) over the three directions.
-template <int DIR, int SCH, bool RHOP = false>
+template <int DIR, int SCH, bool RHOP = false, int SHP = 0>
 __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks, const TileCtx &T,
                                             const SolverParams &P, int stage, bool eig, double *sF,
                                             double *sQ, unsigned &st, double &emax,
                                             double *sRP = nullptr) {
-  using M = TileSmem<DIR, SCH>;
+  using M = TileSmem<DIR, SCH, SHP>;
   constexpr int R = M::R, TW = M::TW, NP = M::NP, SP = M::SP, SQ = M::SQ;
   const BlockDev &B = *T.B;
   const Geo &G = T.G;
@@ -531,10 +534,10 @@ __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks,
 }
 
 // Viscous fluxes of the tile's line positions c0-4 .. c0+cl+3 into sV ([4][TW][SV]).
-template <int DIR, int SCH>
+template <int DIR, int SCH, int SHP = 0>
 __device__ __forceinline__ void phase_vis(const BlockDev *__restrict__ blocks, const TileCtx &T,
                                           const SolverParams &P, double *sV) {
-  using M = TileSmem<DIR, SCH>;
+  using M = TileSmem<DIR, SCH, SHP>;
   constexpr int TW = M::TW, NV = M::NV, SV = M::SV;
   const BlockDev &B = *T.B;
   const Geo &G = T.G;
@@ -575,12 +578,12 @@ __device__ __forceinline__ void phase_vis(const BlockDev *__restrict__ blocks, c
 // Phase 3: per cell, dF from the face fluxes in sH, RHS accumulation (src/euler3d.cpp:368-427,
 // src/NaiverStokes3d.cpp:401-513), and on the zeta sweep the TVD-RK3 stage.
 // sR: the tile's RHS staged at the start of the sweep ([5][TL][TW]), or null.
-template <int DIR, int SCH>
+template <int DIR, int SCH, int SHP = 0>
 __device__ __forceinline__ void phase_cells(const TileCtx &T, const SolverParams &P, StepState *S,
                                             int stage, int flags, const double *sH, const double *sV,
                                             const double *sQ, unsigned &st,
                                             const double *sR = nullptr) {
-  using M = TileSmem<DIR, SCH>;
+  using M = TileSmem<DIR, SCH, SHP>;
   constexpr int TW = M::TW, TL = M::TL, SV = M::SV, SH = M::SH, SQ = M::SQ;
   const BlockDev &B = *T.B;
   const Geo &G = T.G;
@@ -685,11 +688,11 @@ __device__ __forceinline__ void reduce_eig(double emax, double *sRed, StepState 
 
 // Explicit-scheme sweep: phases split -> faces -> cells in one CTA.  HYB: the hybrid
 // WENO-Z face loop of the throughput build (P.sensor set).
-template <int DIR, int SCH, bool HYB = false>
+template <int DIR, int SCH, bool HYB = false, int SHP = 0>
 __global__ void __launch_bounds__(kThreads, DIR == 2 ? NUC3D_SWEEP_MINB_Z : NUC3D_SWEEP_MINB)
 sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
              int stage, int flags) {
-  using M = TileSmem<DIR, SCH>;
+  using M = TileSmem<DIR, SCH, SHP>;
   constexpr int R = M::R, TW = M::TW, SP = M::SP, SV = M::SV, SH = M::SH;
   extern __shared__ double smem[];
   double *sF = smem;                        // [10][TW][SP]: F+ vars 0..4, F- vars 5..9
@@ -704,7 +707,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   double *sRst = reinterpret_cast<double *>(reinterpret_cast<char *>(sS) + (HYB ? kHybSmem : 0));
   __shared__ double sRed[kThreads / 32];
 
-  const TileCtx T = decode_tile<DIR>(blocks, tm, P);
+  const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P);
   const bool eig = (flags & SW_EIG) != 0;
   unsigned st = 0;
   double emax = 0.0;
@@ -729,8 +732,8 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       for (int v = 0; v < 5; ++v) cp_async8(sR + (v * TL + c) * TW + w, T.B->rhs + v * T.N + idx);
     }
   }
-  phase_split<DIR, SCH, HYB>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st, emax, sRP);
-  if (ns) phase_vis<DIR, SCH>(blocks, T, P, sV);
+  phase_split<DIR, SCH, HYB, SHP>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st, emax, sRP);
+  if (ns) phase_vis<DIR, SCH, SHP>(blocks, T, P, sV);
   __syncthreads();
 
   // ---- faces c0 .. c0+cl: the ten reconstructions of each face ----
@@ -845,7 +848,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   }
   __syncthreads();
   if (sR) cp_async_wait_all();
-  phase_cells<DIR, SCH>(T, P, S, stage, flags, sH, sV, sQ, st, sR);
+  phase_cells<DIR, SCH, SHP>(T, P, S, stage, flags, sH, sV, sQ, st, sR);
   if (eig) reduce_eig(emax, sRed, S);
   if (st) atomicOr(&S->status, st);
 }
@@ -1478,29 +1481,39 @@ metrics_kernel(const double *__restrict__ x, const double *__restrict__ y,
 // Host-side launchers (called by the C-ABI layer).
 // ---------------------------------------------------------------------------------
 // Shared memory of the hybrid sweep: the plain sweep's plus rho and p per position.
-template <int DIR, int SCH>
+template <int DIR, int SCH, int SHP = 0>
 __host__ __device__ inline size_t hybrid_smem_bytes(bool ns) {
-  return sweep_smem_bytes<DIR, SCH>(ns) + (size_t)2 * kTW * TileSmem<DIR, SCH>::SP * sizeof(double) +
-         kHybSmem;
+  using M = TileSmem<DIR, SCH, SHP>;
+  return sweep_smem_bytes<DIR, SCH, SHP>(ns) + (size_t)2 * M::TW * M::SP * sizeof(double) + kHybSmem;
 }
 
-template <int DIR, int SCH>
-inline cudaError_t launch_sweep_t(const Launch &L, int stage, int flags) {
+template <int DIR, int SCH, int SHP>
+inline cudaError_t launch_sweep_s(const Launch &L, int stage, int flags) {
   const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
   const bool ns = (flags & SW_NS) != 0;
 #if NUC3D_FAST
   if constexpr (SCH == SCH_WENO5Z) {
     if (L.P.sensor) {
-      sweep_kernel<DIR, SCH, true><<<ntiles, kThreads, hybrid_smem_bytes<DIR, SCH>(ns), L.stream>>>(
+      sweep_kernel<DIR, SCH, true, SHP><<<ntiles, kThreads, hybrid_smem_bytes<DIR, SCH, SHP>(ns), L.stream>>>(
           L.d_blocks, L.tm_dir[DIR], L.P, L.d_state, stage, flags);
       return cudaGetLastError();
     }
   }
 #endif
-  const size_t smem = sweep_smem_bytes<DIR, SCH>(ns) + rhs_stage_bytes<DIR>(ns);
-  sweep_kernel<DIR, SCH><<<ntiles, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[DIR], L.P,
+  const size_t smem = sweep_smem_bytes<DIR, SCH, SHP>(ns) + rhs_stage_bytes<DIR>(ns);
+  sweep_kernel<DIR, SCH, false, SHP><<<ntiles, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[DIR], L.P,
                                                                L.d_state, stage, flags);
   return cudaGetLastError();
+}
+
+template <int DIR, int SCH>
+inline cudaError_t launch_sweep_t(const Launch &L, int stage, int flags) {
+  switch (L.shape[DIR]) {
+    case 0: return launch_sweep_s<DIR, SCH, 0>(L, stage, flags);
+    case 1: return launch_sweep_s<DIR, SCH, 1>(L, stage, flags);
+    case 2: return launch_sweep_s<DIR, SCH, 2>(L, stage, flags);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <int DIR, int SCH>
@@ -1585,21 +1598,37 @@ cudaError_t run_metrics(const double *x, const double *y, const double *z, const
   return cudaGetLastError();
 }
 
+template <int DIR, int SHP>
+inline cudaError_t launch_sensor_data(const Launch &L, float *feat, unsigned char *label,
+                                      long long *where, unsigned long long *count,
+                                      unsigned long long cap) {
+  const int nt = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
+  using M = TileSmem<DIR, SCH_WENO5Z, SHP>;
+  const size_t smem = (size_t)12 * M::TW * M::SP * sizeof(double);
+  sensor_data_kernel<DIR, SHP><<<nt, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[DIR], L.P,
+                                                                  L.d_state, 0, feat, label,
+                                                                  where, count, cap);
+  return cudaGetLastError();
+}
+
+template <int DIR>
+inline cudaError_t launch_sensor_data_d(const Launch &L, float *feat, unsigned char *label,
+                                        long long *where, unsigned long long *count,
+                                        unsigned long long cap) {
+  switch (L.shape[DIR]) {
+    case 0: return launch_sensor_data<DIR, 0>(L, feat, label, where, count, cap);
+    case 1: return launch_sensor_data<DIR, 1>(L, feat, label, where, count, cap);
+    case 2: return launch_sensor_data<DIR, 2>(L, feat, label, where, count, cap);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
                             long long *where, unsigned long long *count, unsigned long long cap) {
   if (L.P.scheme[dir] != SCH_WENO5Z) return cudaErrorInvalidValue;
-  const int nt = L.tm_dir[dir].tile_start[L.tm_dir[dir].nblocks];
-  const size_t smem = (size_t)12 * kTW * TileSmem<0, SCH_WENO5Z>::SP * sizeof(double);
-  if (dir == 0)
-    sensor_data_kernel<0><<<nt, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[0], L.P, L.d_state,
-                                                            0, feat, label, where, count, cap);
-  else if (dir == 1)
-    sensor_data_kernel<1><<<nt, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[1], L.P, L.d_state,
-                                                            0, feat, label, where, count, cap);
-  else
-    sensor_data_kernel<2><<<nt, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[2], L.P, L.d_state,
-                                                            0, feat, label, where, count, cap);
-  return cudaGetLastError();
+  if (dir == 0) return launch_sensor_data_d<0>(L, feat, label, where, count, cap);
+  if (dir == 1) return launch_sensor_data_d<1>(L, feat, label, where, count, cap);
+  return launch_sensor_data_d<2>(L, feat, label, where, count, cap);
 }
 
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts) {
@@ -1633,21 +1662,29 @@ cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags) {
   return launch_sweep<2>(L, stage, f & ~SW_RK);
 }
 
-template <int DIR, int SCH>
-inline cudaError_t configure_t() {
+template <int DIR, int SCH, int SHP>
+inline cudaError_t configure_s() {
 #if NUC3D_FAST
   if constexpr (SCH == SCH_WENO5Z) {
-    const size_t he = hybrid_smem_bytes<DIR, SCH>(false), hn = hybrid_smem_bytes<DIR, SCH>(true);
-    const cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIR, SCH, true>,
+    const size_t he = hybrid_smem_bytes<DIR, SCH, SHP>(false), hn = hybrid_smem_bytes<DIR, SCH, SHP>(true);
+    const cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIR, SCH, true, SHP>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)(he > hn ? he : hn));
     if (e != cudaSuccess) return e;
   }
 #endif
-  const size_t euler = sweep_smem_bytes<DIR, SCH>(false) + rhs_stage_bytes<DIR>(false);
-  const size_t ns = sweep_smem_bytes<DIR, SCH>(true) + rhs_stage_bytes<DIR>(true);
-  return cudaFuncSetAttribute(sweep_kernel<DIR, SCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const size_t euler = sweep_smem_bytes<DIR, SCH, SHP>(false) + rhs_stage_bytes<DIR>(false);
+  const size_t ns = sweep_smem_bytes<DIR, SCH, SHP>(true) + rhs_stage_bytes<DIR>(true);
+  return cudaFuncSetAttribute(sweep_kernel<DIR, SCH, false, SHP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(euler > ns ? euler : ns));
+}
+
+template <int DIR, int SCH>
+inline cudaError_t configure_t() {
+  cudaError_t e;
+  if ((e = configure_s<DIR, SCH, 0>()) != cudaSuccess) return e;
+  if ((e = configure_s<DIR, SCH, 1>()) != cudaSuccess) return e;
+  return configure_s<DIR, SCH, 2>();
 }
 
 template <int DIR, int SCH>
@@ -1686,9 +1723,7 @@ cudaError_t configure() {
   return configure_dir<2>();
 }
 
-int tile_count(int dir, const int n[3]) {
-  return dir == 0 ? sweep_tiles<0>(n) : (dir == 1 ? sweep_tiles<1>(n) : sweep_tiles<2>(n));
-}
+int tile_count(int dir, const int n[3], int shape) { return sweep_tiles(dir, n, shape); }
 
 }  // namespace NUC3D_NS
 }  // namespace nuc3d

@@ -7,6 +7,9 @@
 // global eigenvalue maximum (src/PDEData3d.cpp:152-170), time += dt.  A step is
 // captured once as a CUDA graph and replayed.
 #include <algorithm>
+#include <array>
+#include <map>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -103,6 +106,7 @@ struct nuc3d_ctx {
   DiagDev *d_diag = nullptr;
   double *d_dsums = nullptr, *d_dparts = nullptr;
   SensorDev *d_sensor = nullptr;  // hybrid WENO-Z face sensor (nuc3d_set_sensor)
+  std::vector<BlockDev> hdesc;  // host copy of the block descriptors (tile divisors change)
   // nuc3d_solve_host: copy streams and events, created by its first call
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t ev_start = nullptr, ev_h2d = nullptr, ev_step = nullptr, ev_end = nullptr;
@@ -457,8 +461,9 @@ int nuc3d_finalize(nuc3d_ctx *c) {
       d.face[f].id = b.bc_id[f];
       for (int v = 0; v < 5; ++v) d.face[f].bcv[v] = b.bcv[f][v];
     }
-    set_tile_divisors(d);
+    set_tile_divisors(d, c->L.shape);
   }
+  c->hdesc = hb;
   cudaSetDevice(c->device);
   CUDA_TRY(cudaMalloc(&c->d_blocks, nbk * sizeof(BlockDev)));
   CUDA_TRY(cudaMemcpy(c->d_blocks, hb.data(), nbk * sizeof(BlockDev), cudaMemcpyHostToDevice));
@@ -478,7 +483,8 @@ int nuc3d_finalize(nuc3d_ctx *c) {
   for (int bi = 0; bi < nbk; ++bi) {
     const HostBlock &b = c->blocks[bi];
     for (int d = 0; d < 3; ++d) {
-      L.tm_dir[d].tile_start[bi + 1] = L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, b.n);
+      L.tm_dir[d].tile_start[bi + 1] =
+          L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, b.n, L.shape[d]);
       const long long nsys = 10 * (b.N / b.n[d]);
       L.tm_sys[d].tile_start[bi + 1] = L.tm_sys[d].tile_start[bi] + (int)((nsys + 255) / 256);
     }
@@ -664,6 +670,117 @@ int nuc3d_solve_host(nuc3d_ctx *c, double *const *q_host, int nsteps) {
   CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_end, 0));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return check_status(c);
+}
+
+// Tile shapes of the sweeps: tile divisors of every block (device descriptors) and the
+// per-direction tile maps; the captured step graph holds the old launches, so it goes.
+static int apply_shapes(nuc3d_ctx *c, const int shape[3]) {
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const int nbk = (int)c->blocks.size();
+  for (int d = 0; d < 3; ++d) c->L.shape[d] = shape[d];
+  for (int bi = 0; bi < nbk; ++bi) set_tile_divisors(c->hdesc[bi], c->L.shape);
+  CUDA_TRY(cudaMemcpy(c->d_blocks, c->hdesc.data(), nbk * sizeof(BlockDev), cudaMemcpyHostToDevice));
+  for (int bi = 0; bi < nbk; ++bi)
+    for (int d = 0; d < 3; ++d)
+      c->L.tm_dir[d].tile_start[bi + 1] =
+          c->L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, c->blocks[bi].n, shape[d]);
+  c->drop_graph();
+  return NUC3D_OK;
+}
+
+static bool compact_scheme(int s) { return s == SCH_CRWENO5 || s == SCH_HCCS || s == SCH_HCCS77; }
+
+int nuc3d_set_tiles(nuc3d_ctx *c, const int shape[3]) {
+  if (!c || !shape) return fail(NUC3D_EINVAL, "null argument");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  for (int d = 0; d < 3; ++d) {
+    if (shape[d] < 0 || shape[d] >= kTileShapes)
+      return fail(NUC3D_EINVAL, "direction %d: tile shape %d not in 0..%d", d, shape[d], kTileShapes - 1);
+    if (compact_scheme(c->P.scheme[d]) && shape[d] != 0)
+      return fail(NUC3D_EINVAL, "direction %d: compact schemes run tile shape 0", d);
+  }
+  return apply_shapes(c, shape);
+}
+
+int nuc3d_get_tiles(nuc3d_ctx *c, int shape[3]) {
+  if (!c || !shape) return fail(NUC3D_EINVAL, "null argument");
+  for (int d = 0; d < 3; ++d) shape[d] = c->L.shape[d];
+  return NUC3D_OK;
+}
+
+namespace {
+// Tile shapes chosen by nuc3d_autotune, per grid: block extents, schemes, model, build.
+std::mutex g_tune_mutex;
+std::map<std::string, std::array<int, 3>> g_tune_cache;
+
+std::string tune_key(const nuc3d_ctx *c) {
+  std::string k = c->exact ? "x" : "f";
+  k += c->P.model == MODEL_NS ? "ns" : "eu";
+  k += c->P.sensor ? "h" : "p";
+  for (int d = 0; d < 3; ++d) k += ":" + std::to_string(c->P.scheme[d]) + "." + std::to_string(c->P.vis[d]);
+  for (const HostBlock &b : c->blocks)
+    k += "|" + std::to_string(b.n[0]) + "x" + std::to_string(b.n[1]) + "x" + std::to_string(b.n[2]);
+  return k;
+}
+}  // namespace
+
+int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  if (reps < 1) reps = 3;
+  const std::string key = tune_key(c);
+  std::array<int, 3> best = {0, 0, 0};
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) { best = it->second; cached = true; }
+  }
+  if (ms_out)
+    for (int i = 0; i < 9; ++i) ms_out[i] = -1.0;
+  if (!cached) {
+    cudaSetDevice(c->device);
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    unsigned status0 = 0;  // the timing sweeps must not leave status bits behind
+    CUDA_TRY(cudaMemcpy(&status0, &c->d_state->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    int cur[3] = {c->L.shape[0], c->L.shape[1], c->L.shape[2]};
+    for (int d = 0; d < 3; ++d) {
+      if (compact_scheme(c->P.scheme[d])) { best[d] = 0; continue; }
+      double tbest = 1e300;
+      for (int sh = 0; sh < kTileShapes; ++sh) {
+        cur[d] = sh;
+        if (int r = apply_shapes(c, cur)) return r;
+        auto sweep = [&]() {
+          return c->exact ? nuc3d::exact::run_sweep(c->L, d, 0, 0) : nuc3d::fast::run_sweep(c->L, d, 0, 0);
+        };
+        CUDA_TRY(sweep());  // warm-up
+        CUDA_TRY(cudaEventRecord(e0, c->stream));
+        for (int r = 0; r < reps; ++r) CUDA_TRY(sweep());
+        CUDA_TRY(cudaEventRecord(e1, c->stream));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float t = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+        const double ms = (double)t / reps;
+        if (ms_out) ms_out[3 * d + sh] = ms;
+        if (ms < tbest) { tbest = ms; best[d] = sh; }
+      }
+      cur[d] = best[d];
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CUDA_TRY(cudaMemcpy(&c->d_state->status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice));
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    g_tune_cache[key] = best;
+  }
+  const int shp[3] = {best[0], best[1], best[2]};
+  if (int r = apply_shapes(c, shp)) return r;
+  if (shape_out)
+    for (int d = 0; d < 3; ++d) shape_out[d] = best[d];
+  return NUC3D_OK;
 }
 
 int nuc3d_sync(nuc3d_ctx *c) {

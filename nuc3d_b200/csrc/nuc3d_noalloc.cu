@@ -163,7 +163,8 @@ int nuc3d_rhs_noalloc(const nuc3d_config *cfg, int device, int nx, int ny, int n
     B.face[f].id = bc_id[f];
     for (int v = 0; v < 5; ++v) B.face[f].bcv[v] = bc_values ? bc_values[f * 5 + v] : 0.0;
   }
-  set_tile_divisors(B);
+  const int shape0[3] = {0, 0, 0};  // default tile shape in every direction
+  set_tile_divisors(B, shape0);
   static thread_local FaceJobs J;  // host staging only
   std::memset(&J, 0, sizeof(J));
   for (int f = 0; f < 6; ++f) {
@@ -193,7 +194,7 @@ int nuc3d_rhs_noalloc(const nuc3d_config *cfg, int device, int nx, int ny, int n
   for (int d = 0; d < 3; ++d) {
     L.tm_dir[d].nblocks = 1;
     L.tm_dir[d].tile_start[0] = 0;
-    L.tm_dir[d].tile_start[1] = nuc3d::exact::tile_count(d, n);
+    L.tm_dir[d].tile_start[1] = nuc3d::exact::tile_count(d, n, 0);
   }
   L.tm_cells.nblocks = 1;
   L.tm_cells.tile_start[1] = (int)((B.N + 255) / 256);

@@ -61,21 +61,21 @@ __device__ __forceinline__ double weno5z_deviation(double f0, double f1, double 
 // sweep, then one thread per face.  Faces are appended at *count (order unspecified);
 // at most cap are written.  where (may be null) gets each face's index in the block's
 // face grid of direction DIR: faces along DIR have extent n[DIR] + 1, i fastest.
-template <int DIR>
+template <int DIR, int SHP>
 __global__ void __launch_bounds__(kThreads, NUC3D_SWEEP_MINB)
 sensor_data_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
                    int stage, float *__restrict__ feat, unsigned char *__restrict__ label,
                    long long *__restrict__ where, unsigned long long *count,
                    unsigned long long cap) {
-  using M = TileSmem<DIR, SCH_WENO5Z>;
+  using M = TileSmem<DIR, SCH_WENO5Z, SHP>;
   constexpr int R = M::R, TW = M::TW, TL = M::TL, SP = M::SP;
   extern __shared__ double smem[];
   double *sF = smem;                 // [10][TW][SP]
   double *sRP = sF + 10 * TW * SP;   // [2][TW][SP]: rho, p
-  const TileCtx T = decode_tile<DIR>(blocks, tm, P);
+  const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P);
   unsigned st = 0;
   double emax = 0.0;
-  phase_split<DIR, SCH_WENO5Z, true>(blocks, T, P, stage, false, sF, nullptr, st, emax, sRP);
+  phase_split<DIR, SCH_WENO5Z, true, SHP>(blocks, T, P, stage, false, sF, nullptr, st, emax, sRP);
   __syncthreads();
   const bool compat = P.weno5z_compat != 0;
   for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {

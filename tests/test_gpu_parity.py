@@ -230,3 +230,58 @@ def test_solve_host_chunked_equals_device_steps():
     assert s1.time_dt() == s2.time_dt()
     s1.close()
     s2.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tgv_ns_weno5js_lf", "sphere_euler_weno5z_ausm_outlet",
+                                  "bc_ns_weno7js_ausmp", "mixed_low_order_ausmp",
+                                  "ns_cd2_weno5z_bc"])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 2, 2), (2, 0, 1)])
+def test_tile_shapes_bitwise(name, shape):
+    """Every sweep tile shape gives the reference's RHS and steps bit for bit: the shape
+    changes which CTA computes a face, never the arithmetic."""
+    g = G.load(name)
+    s = G.solver(g, exact=True)
+    s.set_tiles(shape)
+    assert s.get_tiles() == shape
+    assert s.rhs() == g.dt_local[0]
+    assert np.array_equal(s.get_rhs(0), g.rhs)
+    s.step(int(g.cfg["nsteps"]))
+    assert np.array_equal(s.get_q(0), g.qn)
+
+
+@pytest.mark.gpu
+def test_tile_shapes_two_blocks_bitwise():
+    name = G.multi_names()[0]
+    g = G.load(name)
+    s, mr = _two_rank_solver(g, exact=True)
+    s.set_tiles((0, 1, 0))  # hccs77 directions keep shape 0
+    s.step(int(mr["nsteps"][0]))
+    q = np.concatenate([s.get_q(0), s.get_q(1)], axis=3)
+    assert np.array_equal(q, mr["qn"])
+
+
+@pytest.mark.gpu
+def test_autotune_picks_and_caches():
+    """nuc3d_autotune times each shape of each explicit direction, keeps the fastest, leaves
+    the state and the results unchanged, and a second context of the same grid takes the
+    cached choice without timing; compact directions stay on shape 0."""
+    import nuc3d_b200 as nb
+    g = G.load("tgv_ns_weno5js_lf")
+    s = G.solver(g, exact=True)
+    r = s.autotune(reps=2)
+    assert all(0 <= x < 3 for x in r["shape"]) and s.get_tiles() == r["shape"]
+    assert all(t is not None and t > 0 for row in r["ms"] for t in row)
+    assert r["shape"] == tuple(min(range(3), key=lambda k: row[k]) for row in r["ms"])
+    assert s.status() == 0
+    s.step(int(g.cfg["nsteps"]))
+    assert np.array_equal(s.get_q(0), g.qn)
+    s2 = G.solver(g, exact=True)
+    r2 = s2.autotune()
+    assert r2["shape"] == r["shape"] and all(t is None for row in r2["ms"] for t in row)
+    c = G.load("mixed_compact_ausmp")
+    s3 = G.solver(c, exact=True)
+    r3 = s3.autotune(reps=1)
+    assert r3["shape"][0] == 0 and r3["shape"][1] == 0 and r3["ms"][0] == [None] * 3
+    with pytest.raises(nb.Nuc3dError):
+        s3.set_tiles((1, 0, 0))
