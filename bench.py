@@ -2,6 +2,7 @@
 """Throughput of NUC3d's per-block RHS + TVD-RK3 update on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --workload turbulence24      (the 24-block Navier-Stokes grid)
 
 Workload (one per GPU): the shock-dominated FP64 Euler case -- a 256^3 block on
 [0,1]^3 with extrapolation (outlet) faces, spherical discontinuity rho,p = 1,10
@@ -442,6 +443,91 @@ def ours(args):
     return 0
 
 
+TURB_WORKLOAD = ("decaying isotropic turbulence, 2pi periodic box in 24 uneven blocks (per-axis "
+                 "sizes from {48,64,96,128,160}, seed 99), 40.1M cells, FP64 Navier-Stokes, "
+                 "WENO5-Z, AUSM, cd6, Mt 0.6, Re_lambda 100, TVD-RK3 CFL 0.5")
+
+
+def turbulence24(args):
+    """The batched multi-block Navier-Stokes workload on one GPU: every block of the grid in
+    one context (on-device ghost copies), one launch per sweep over all blocks, the step a
+    CUDA graph, tile shapes from nuc3d_autotune."""
+    import torch
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+
+    torch.cuda.set_device(0)
+    parts = C.uneven_blocks(seed=99)
+    n = [sum(p) for p in parts]
+    prim, re = C.isotropic_turbulence(tuple(n), seed=7)
+    types, ids = C.block_topology(parts)
+    off = [np.concatenate([[0], np.cumsum(p)]) for p in parts]
+    h = [2 * math.pi / n[d] for d in range(3)]
+    s = nb.Solver(nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="NavierStokes3d",
+                            reynolds=re, mach=0.6, cfl=0.5, exact=args.exact))
+    boxes = [((a, b, c), (parts[0][a], parts[1][b], parts[2][c]))
+             for c in range(len(parts[2])) for b in range(len(parts[1])) for a in range(len(parts[0]))]
+    for r, (_, sh) in enumerate(boxes):
+        s.add_block(*sh, types[r], ids[r])
+    mets = [C.uniform_metrics(sh, lo=(0, 0, 0), hi=tuple(h[d] * sh[d] for d in range(3)))
+            for _, sh in boxes]
+    for r, m in enumerate(mets):
+        s.set_metrics(r, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
+    s.finalize()
+    qs = []
+    for r, ((a, b, c), sh) in enumerate(boxes):
+        sl = (slice(None), slice(off[2][c], off[2][c + 1]), slice(off[1][b], off[1][b + 1]),
+              slice(off[0][a], off[0][a + 1]))
+        qs.append(np.ascontiguousarray(C.prim_to_q(prim[sl], mets[r]["jac"], 1.4)))
+        s.set_q(r, qs[r])
+    cells = int(np.prod(n))
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    tiles = s.autotune(reps=2)["shape"]
+    s.step(args.warmup)
+    s.sync()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        s.step(args.steps, sync=False)
+        ev1.record(stream)
+        ev1.synchronize()
+    s.sync()
+    ms = ev0.elapsed_time(ev1)
+    # end to end: every block's Q from pinned host arrays and back, every step
+    host = [torch.empty(q.size, dtype=torch.float64, pin_memory=True) for q in qs]
+    for hq, q in zip(host, qs):
+        hq.numpy()[:] = q.reshape(-1)
+    e2e_steps = max(3, min(args.steps, 10))
+    s.solve_host([hq.data_ptr() for hq in host], 1)
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    s.solve_host([hq.data_ptr() for hq in host], e2e_steps)
+    ev3.record(stream)
+    ev3.synchronize()
+    e2e_ms = ev2.elapsed_time(ev3)
+    per = [s.profile_sweep(d, reps=3) for d in range(3)]
+    line = {
+        "metric": "Mcell-RK3-steps/s", "value": whole_job_rate(1, cells, args.steps, ms),
+        "unit": "Mcell-RK3-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": TURB_WORKLOAD, "cells_per_gpu": cells, "blocks": len(boxes),
+                   "tile_shapes": list(tiles), "status_bits": s.status(),
+                   "l2": "no flush: 40.1M cells x 5 doubles = 1.6 GB per state buffer > 126 MB L2"},
+        "clocks": clk.summary(),
+        "e2e": {"value": whole_job_rate(1, cells, e2e_steps, e2e_ms), "unit": "Mcell-RK3-steps/s",
+                "h2d_bytes_per_step": 5 * cells * 8, "d2h_bytes_per_step": 5 * cells * 8,
+                "steps": e2e_steps, "api": "nuc3d_solve_host (24 host arrays in place, every step)"},
+        "gpu_launches": s.kernels_per_step() * args.steps,
+        "sweep_ms_per_launch": per,
+        "roofline": None, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+    s.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,9 +536,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--exact", action="store_true", help="reference-order arithmetic")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="sphere256", choices=["sphere256", "turbulence24"],
+                    help="turbulence24: the 24-block Navier-Stokes grid on one GPU (our arm only)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.workload == "turbulence24":
+        if args.impl == "reference" or args.gpus > 1:
+            print(json.dumps({"impl": args.impl, "unavailable": "turbulence24 runs our arm on one GPU only"}))
+            return 0
+        return turbulence24(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours(args)
