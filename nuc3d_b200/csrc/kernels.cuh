@@ -1132,11 +1132,28 @@ __global__ void __launch_bounds__(kCellTile)
 grad_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P) {
   const int b = find_block(tm, blockIdx.x);
   const BlockDev &B = blocks[b];
-  const long long idx = (long long)(blockIdx.x - tm.tile_start[b]) * kCellTile + threadIdx.x;
-  if (idx >= B.N) return;
+  const long long t = (long long)(blockIdx.x - tm.tile_start[b]) * kCellTile + threadIdx.x;
+  if (t >= B.N) return;
   const long long N = B.N;
   const int nx = B.n[0], ny = B.n[1];
-  const int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((long long)nx * ny));
+  // Threads take the cells whose xi stencil stays inside the block first (row by row), then
+  // the E cells at each end of every xi row, so that a warp's lanes take the same xi
+  // branch below (cell by cell in order, 3 lanes of every other warp took the edge path).
+  const int E = P.ts[0], ni = nx - 2 * E;  // nx >= 2 bfsize + 2 > 2 E
+  const long long nint = (long long)ni * ny * B.n[2];
+  long long row;
+  int i;
+  if (t < nint) {
+    row = t / ni;
+    i = E + (int)(t - row * ni);
+  } else {
+    const long long e = t - nint;
+    row = e / (2 * E);
+    const int c = (int)(e - row * 2 * E);
+    i = c < E ? c : nx - 2 * E + c;
+  }
+  const int j = (int)(row % ny), k = (int)(row / ny);
+  const long long idx = row * nx + i;
   const int pos[3] = {i, j, k};
   const long long stride[3] = {1, nx, (long long)nx * ny};
   double gr[4][3];  // [u,v,w,T][xi,eta,zeta]
