@@ -285,8 +285,13 @@ def ours(args):
     stream = torch.cuda.Stream(device=dev)
     s.set_stream(stream.cuda_stream)
     s.set_q(b, q0)
-    # sweep tile shapes per direction, timed on this grid (outside every timed region)
-    tiles = s.autotune(reps=3)["shape"]
+    # sweep tile shapes per direction, timed on this grid (outside every timed region);
+    # --tiles pins them instead (profiler runs, whose timings would mislead the autotuner)
+    if args.tiles:
+        s.set_tiles(args.tiles)
+        tiles = s.get_tiles()
+    else:
+        tiles = s.autotune(reps=3)["shape"]
 
     def barrier():
         if dist is not None:
@@ -352,7 +357,7 @@ def ours(args):
         rho_plain = s.get_q(b)[0]
         s.set_q(b, q0)
         s.set_sensor(SENS.load_weights(), SENS.DEFAULT_THRESHOLD)
-        htiles = s.autotune(reps=3)["shape"]
+        htiles = s.get_tiles() if args.tiles else s.autotune(reps=3)["shape"]
         s.step(warm)  # includes the capture of the hybrid step graph
         barrier()
         ev4, ev5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -483,7 +488,11 @@ def turbulence24(args):
     cells = int(np.prod(n))
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
-    tiles = s.autotune(reps=2)["shape"]
+    if args.tiles:
+        s.set_tiles(args.tiles)
+        tiles = s.get_tiles()
+    else:
+        tiles = s.autotune(reps=2)["shape"]
     s.step(args.warmup)
     s.sync()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -536,6 +545,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--exact", action="store_true", help="reference-order arithmetic")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tiles", type=lambda x: tuple(int(v) for v in x.split(",")), default=None,
+                    help="sweep tile shapes per direction, e.g. 2,0,0 (default: nuc3d_autotune)")
     ap.add_argument("--workload", default="sphere256", choices=["sphere256", "turbulence24"],
                     help="turbulence24: the 24-block Navier-Stokes grid on one GPU (our arm only)")
     args = ap.parse_args()

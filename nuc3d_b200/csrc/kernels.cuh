@@ -1128,7 +1128,10 @@ __device__ __forceinline__ double diff_inner(const double *__restrict__ f, long 
 
 // NaiverStokesData3d::solveGrads + solveViscousFlux (src/NaiverStokes3d.cpp:63-326)
 // with physicsModel::sutherland (src/physicsModel.cpp:199-234).
-__global__ void __launch_bounds__(kCellTile)
+#ifndef NUC3D_GRAD_MINB
+#define NUC3D_GRAD_MINB 4  // resident CTAs per SM the gradient kernel's registers are cut for:
+#endif                     // 64 registers, 7% faster than 80 (3 CTAs) despite spills
+__global__ void __launch_bounds__(kCellTile, NUC3D_GRAD_MINB)
 grad_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P) {
   const int b = find_block(tm, blockIdx.x);
   const BlockDev &B = blocks[b];
