@@ -42,7 +42,7 @@ WORKLOAD = ("spherical Riemann 256^3, FP64 Euler, WENO5-Z (reference :80 stencil
             "outlet faces, TVD-RK3 CFL 0.5")
 
 # Algorithmic FP64 operations per cell, counted from the reference's expressions
-# (add/sub/mul/div/sqrt = 1, abs = 0, pow(x,2) = 1).  Derivation in DESIGN.md.
+# (add/sub/mul/div/sqrt = 1, abs = 0, pow(x,2) = 1), per the cited reference lines.
 FLOPS = {
     "con2prim": 46,        # src/physicsModel.cpp:315-353, :1000-1054
     "AUSM": 82,            # src/physicsModel.cpp:557-597 + RiemannAUSM :762-850, per direction
