@@ -612,6 +612,15 @@ int nuc3d_step(nuc3d_ctx *c, int nsteps) {
   return NUC3D_OK;
 }
 
+// Two timing events, destroyed on every way out of the scope that made them.
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
 // Copy chunks of nuc3d_solve_host: small enough that the upload of chunk j (next step)
 // trails the download of chunk j (this step) by little, large enough that each copy runs
 // at full PCIe speed.
@@ -744,9 +753,10 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     unsigned status0 = 0;  // the timing sweeps must not leave status bits behind
     CUDA_TRY(cudaMemcpy(&status0, &c->d_state->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    cudaEvent_t e0, e1;
-    CUDA_TRY(cudaEventCreate(&e0));
-    CUDA_TRY(cudaEventCreate(&e1));
+    EventPair ev;
+    CUDA_TRY(cudaEventCreate(&ev.a));
+    CUDA_TRY(cudaEventCreate(&ev.b));
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     int cur[3] = {c->L.shape[0], c->L.shape[1], c->L.shape[2]};
     for (int d = 0; d < 3; ++d) {
       if (compact_scheme(c->P.scheme[d])) { best[d] = 0; continue; }
@@ -770,8 +780,6 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
       }
       cur[d] = best[d];
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     CUDA_TRY(cudaMemcpy(&c->d_state->status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice));
     std::lock_guard<std::mutex> g(g_tune_mutex);
     g_tune_cache[key] = best;
@@ -842,17 +850,16 @@ int nuc3d_profile_sweep(nuc3d_ctx *c, int dir, int reps, double *ms) {
     return c->exact ? nuc3d::exact::run_sweep(c->L, dir, 0, 0) : nuc3d::fast::run_sweep(c->L, dir, 0, 0);
   };
   CUDA_TRY(sweep());  // warm-up
-  cudaEvent_t e0, e1;
-  CUDA_TRY(cudaEventCreate(&e0));
-  CUDA_TRY(cudaEventCreate(&e1));
+  EventPair ev;
+  CUDA_TRY(cudaEventCreate(&ev.a));
+  CUDA_TRY(cudaEventCreate(&ev.b));
+  cudaEvent_t e0 = ev.a, e1 = ev.b;
   CUDA_TRY(cudaEventRecord(e0, c->stream));
   for (int r = 0; r < reps; ++r) CUDA_TRY(sweep());
   CUDA_TRY(cudaEventRecord(e1, c->stream));
   CUDA_TRY(cudaEventSynchronize(e1));
   float t = 0.0f;
   CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   *ms = (double)t / reps;
   return check_status(c);
 }
