@@ -757,16 +757,18 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     // 1a: per-gap values (F+ differences, jumps) into sG, in sH's place (sH is written
     // only in pass 2)
     float *sG = reinterpret_cast<float *>(sH);
+    unsigned char *sZ = reinterpret_cast<unsigned char *>(sG + kSensorGapVals * TW * SP);
     constexpr int NG = M::NP - 1;
-    static_assert(kSensorGapVals * TW * SP * sizeof(float) <= 5 * TW * SH * sizeof(double),
-                  "gap values fit in the face-flux tile");
+    static_assert(kSensorGapVals * TW * SP * sizeof(float) + TW * SP <= 5 * TW * SH * sizeof(double),
+                  "gap values and zero flags fit in the face-flux tile");
     for (int e = threadIdx.x; e < TW * NG; e += kThreads) {
       const int w = e / NG, p = e - w * NG;
       if (w >= T.nw) continue;
       const double *rowF[5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) rowF[v] = sF + (v * TW + w) * SP;
-      sensor_gap(rowF, sRP + w * SP, sRP + (TW + w) * SP, p, sG + w * SP + p, TW * SP);
+      sZ[w * SP + p] =
+          sensor_gap(rowF, sRP + w * SP, sRP + (TW + w) * SP, p, sG + w * SP + p, TW * SP) ? 1 : 0;
     }
     __syncthreads();
     // 1b: features, network, decision
@@ -781,7 +783,12 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       uint32_t xr[10];
 #pragma unroll
       for (int i = 0; i < 10; ++i) xr[i] = 0u;
-      if (valid) sensor_features_gaps(sG + w * SP + (R + fl - 3), TW * SP, xr);
+      if (valid) {
+        // a face whose five stencil gaps are all zero has all-zero features: skip them
+        const unsigned char *z = sZ + w * SP + (R + fl - 3);
+        if (!(z[0] & z[1] & z[2] & z[3] & z[4]))
+          sensor_features_gaps(sG + w * SP + (R + fl - 3), TW * SP, xr);
+      }
       const float logit = sensor_logit(sS, xr);
       if (valid) sLin[e] = logit < P.sensor_threshold ? 1 : 0;
     }

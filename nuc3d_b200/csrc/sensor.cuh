@@ -258,13 +258,22 @@ __device__ __forceinline__ float rel_jump_f(float a, float b) {
 }
 
 // Gap p of line w: rowF[v] = F+ of variable v at position 0 of the line, rr/pp = density
-// and pressure likewise; out[k] is sG[k][w] (stride gs floats between k).
-__device__ __forceinline__ void sensor_gap(const double *const rowF[5], const double *rr,
+// and pressure likewise; out[k] is sG[k][w] (stride gs floats between k).  Returns whether
+// all seven values are zero (a gap inside a uniform region).
+__device__ __forceinline__ bool sensor_gap(const double *const rowF[5], const double *rr,
                                            const double *pp, int p, float *out, int gs) {
+  bool zero = true;
 #pragma unroll
-  for (int v = 0; v < 5; ++v) out[v * gs] = (float)(rowF[v][p + 1] - rowF[v][p]);
-  out[5 * gs] = rel_jump_f((float)rr[p], (float)rr[p + 1]);
-  out[6 * gs] = rel_jump_f((float)pp[p], (float)pp[p + 1]);
+  for (int v = 0; v < 5; ++v) {
+    const float d = (float)(rowF[v][p + 1] - rowF[v][p]);
+    out[v * gs] = d;
+    zero = zero && d == 0.0f;
+  }
+  const float jr = rel_jump_f((float)rr[p], (float)rr[p + 1]);
+  const float jp = rel_jump_f((float)pp[p], (float)pp[p + 1]);
+  out[5 * gs] = jr;
+  out[6 * gs] = jp;
+  return zero && jr == 0.0f && jp == 0.0f;
 }
 
 // The 19 features of one face from the gaps g = first gap of its stencil (cells f-3, f-2)
