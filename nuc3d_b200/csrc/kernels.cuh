@@ -98,6 +98,9 @@ __host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
 #ifndef NUC3D_RHS_PREFETCH
 #define NUC3D_RHS_PREFETCH 1
 #endif
+#ifndef NUC3D_HYB_PREFETCH
+#define NUC3D_HYB_PREFETCH 0  // the same staging in the hybrid eta sweep (measured 2% slower)
+#endif
 template <int DIR>
 __host__ __device__ constexpr bool rhs_prefetch(bool ns) {
   return NUC3D_RHS_PREFETCH && (DIR == 1 || (DIR == 2 && NUC3D_RHS_PREFETCH_Z)) && !ns;
@@ -712,7 +715,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   unsigned st = 0;
   double emax = 0.0;
   // (the hybrid sweep measured slower with the staged RHS: its tile is larger already)
-  double *sR = (!HYB && rhs_prefetch<DIR>(ns)) ? sRst : nullptr;
+  double *sR = ((!HYB || NUC3D_HYB_PREFETCH) && rhs_prefetch<DIR>(ns)) ? sRst : nullptr;
   if constexpr (HYB) {
     // the network's weights, read by every warp's inference: shared memory
     static_assert(sizeof(SensorDev) % 4 == 0, "word copy");
@@ -1511,7 +1514,8 @@ metrics_kernel(const double *__restrict__ x, const double *__restrict__ y,
 template <int DIR, int SCH, int SHP = 0>
 __host__ __device__ inline size_t hybrid_smem_bytes(bool ns) {
   using M = TileSmem<DIR, SCH, SHP>;
-  return sweep_smem_bytes<DIR, SCH, SHP>(ns) + (size_t)2 * M::TW * M::SP * sizeof(double) + kHybSmem;
+  return sweep_smem_bytes<DIR, SCH, SHP>(ns) + (size_t)2 * M::TW * M::SP * sizeof(double) + kHybSmem +
+         (NUC3D_HYB_PREFETCH ? rhs_stage_bytes<DIR>(ns) : 0);
 }
 
 template <int DIR, int SCH, int SHP>
