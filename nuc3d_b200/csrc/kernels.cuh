@@ -752,6 +752,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   const int ne = nf - ni;                     // edge faces per line
   const int ei = TW * ni, e0 = (ei + 31) & ~31;
   const float rni = ni > 0 ? 1.0f / (float)ni : 0.0f, rne = ne > 0 ? 1.0f / (float)ne : 0.0f;
+  bool hyb_any = true, hyb_lin0 = false;  // hybrid: some gap of the tile nonzero; decision at zero
   if constexpr (HYB) {
     // hybrid WENO-Z, pass 1: the face sensor's decision for every interior face item
     // (linear weights or WENO-Z), into sLin.  Rounds are the same in every thread: the
@@ -764,17 +765,24 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     constexpr int NG = M::NP - 1;
     static_assert(kSensorGapVals * TW * SP * sizeof(float) + TW * SP <= 5 * TW * SH * sizeof(double),
                   "gap values and zero flags fit in the face-flux tile");
+    int nonzero = 0;
     for (int e = threadIdx.x; e < TW * NG; e += kThreads) {
       const int w = e / NG, p = e - w * NG;
       if (w >= T.nw) continue;
       const double *rowF[5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) rowF[v] = sF + (v * TW + w) * SP;
-      sZ[w * SP + p] =
-          sensor_gap(rowF, sRP + w * SP, sRP + (TW + w) * SP, p, sG + w * SP + p, TW * SP) ? 1 : 0;
+      const bool zero =
+          sensor_gap(rowF, sRP + w * SP, sRP + (TW + w) * SP, p, sG + w * SP + p, TW * SP);
+      sZ[w * SP + p] = zero ? 1 : 0;
+      nonzero |= zero ? 0 : 1;
     }
-    __syncthreads();
+    // A tile whose every gap is zero (inside a uniform region) has all-zero features on
+    // every face: each face's decision is the network's zero-input one, and 1b is skipped.
+    hyb_any = __syncthreads_or(nonzero) != 0;
+    hyb_lin0 = sS->zero_logit < P.sensor_threshold;
     // 1b: features, network, decision
+    if (hyb_any)
     for (int base = 0; base < ei; base += kThreads) {
       const int e = base + threadIdx.x;
       int w = 0, fl = 0;
@@ -795,7 +803,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       const float logit = sensor_logit(sS, xr);
       if (valid) sLin[e] = logit < P.sensor_threshold ? 1 : 0;
     }
-    __syncthreads();
+    if (hyb_any) __syncthreads();
   }
   for (int e = threadIdx.x; e < e0 + TW * ne; e += kThreads) {
     // w = e / ni by a float reciprocal: exact, since (e + 1/2) / ni stays at least
@@ -817,7 +825,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
     }
     if (w >= T.nw) continue;
     const int f = T.c0 + fl;
-    if (HYB && !edge && sLin[e]) {
+    if (HYB && !edge && (hyb_any ? sLin[e] != 0 : hyb_lin0)) {
       // hybrid: a face the sensor calls smooth takes the linear weights (0.1, 0.6, 0.3)
 #pragma unroll 1
       for (int v = 0; v < 5; ++v) {
