@@ -101,9 +101,13 @@ __host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
 #ifndef NUC3D_HYB_PREFETCH
 #define NUC3D_HYB_PREFETCH 0  // the same staging in the hybrid eta sweep (measured 2% slower)
 #endif
+#ifndef NUC3D_RHS_PREFETCH_NS
+#define NUC3D_RHS_PREFETCH_NS 0  // the same staging in the Navier-Stokes eta sweep (measured
+#endif                           // 2% slower on the 24-block grid: 3 CTAs per SM with 8x32)
 template <int DIR>
 __host__ __device__ constexpr bool rhs_prefetch(bool ns) {
-  return NUC3D_RHS_PREFETCH && (DIR == 1 || (DIR == 2 && NUC3D_RHS_PREFETCH_Z)) && !ns;
+  return NUC3D_RHS_PREFETCH && (DIR == 1 || (DIR == 2 && NUC3D_RHS_PREFETCH_Z)) &&
+         (!ns || NUC3D_RHS_PREFETCH_NS);
 }
 template <int DIR>
 __host__ __device__ inline size_t rhs_stage_bytes(bool ns) {
