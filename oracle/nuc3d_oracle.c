@@ -21,12 +21,15 @@
  *   RHS sum, dt                        src/euler3d.cpp:368-435, src/NaiverStokes3d.cpp:401-513
  *   TVD-RK3                            src/PDEData3d.cpp:152-170, src/TVD-RK3.cpp:16-137
  * Arithmetic is written in the reference's operand order; build with
- * -ffp-contract=off (oracle/Makefile).  pow(x, 2) is x*x and pow(T, 1.5) uses
- * the correctly rounded sequence of oracle/pow_cr.c.
+ * -ffp-contract=off (oracle/Makefile).  pow(x, 2) is x*x, pow(T, 1.5) uses
+ * the correctly rounded sequence of oracle/pow_cr.c, and the energy reset's
+ * pow(rho, gamma) the double-double pow of oracle/cr_pow.h.
  */
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+
+#include "cr_pow.h"
 
 enum { S_WENO5JS = 0, S_WENO5Z = 1, S_WENO7JS = 2, S_CRWENO5 = 3, S_HCCS = 4, S_WENO3JS = 5, S_UPWIND1 = 6,
        S_HCCS77 = 7 };
@@ -73,6 +76,14 @@ static double cr_pow15(double x) {
   double hi = x * s, lo = fma(x, s, -hi), t = x * e;
   return hi + (lo + t);
 }
+
+/* pow for the energy reset (src/physicsModel.cpp:329): cr_pow.h, libm outside its domain */
+static double oc_pow(double x, double y) {
+  const double r = nuc3d_cr_pow(x, y);
+  return r == r ? r : pow(x, y);
+}
+/* exported for the tests: the oracle's pow(x, y) */
+double oc_cr_pow(double x, double y) { return oc_pow(x, y); }
 
 static const double A5[3][3] = {{1.0 / 3.0, -7.0 / 6.0, 11.0 / 6.0},
                                 {-1.0 / 6.0, 5.0 / 6.0, 1.0 / 3.0},
@@ -201,7 +212,7 @@ static void con2prim(const oc_config *c, double *q4, double q0, double q1, doubl
   double E = *q4 * jac;
   double e0 = E - 0.5 * rho * (u * u + v * v + w * w);
   if (e0 < 0.0) {
-    E = (pow(rho, g) / ((g * m * m) * (g - 1.0)) + 0.5 * rho * (u * u + v * v + w * w));
+    E = (oc_pow(rho, g) / ((g * m * m) * (g - 1.0)) + 0.5 * rho * (u * u + v * v + w * w));
     *q4 = E / jac;
   }
   double p = (E - 0.5 * rho * (u * u + v * v + w * w)) * (g - 1.0);
@@ -798,9 +809,15 @@ int oc_rhs(const oc_config *c, int nb, oc_block *blocks, double *dt_local) {
 }
 
 /* nsteps TVD-RK3 steps (block::solve); dt[s] and the accumulated *time are returned */
-int oc_step(const oc_config *c, int nb, oc_block *blocks, int nsteps, double *dt, double *time) {
+/* nsteps TVD-RK3 steps; dt[s], *time, and res[s] (may be NULL): the residual of step s,
+   PDEData3d::setRES (src/PDEData3d.cpp:90-122) per block in its loop order, the maximum
+   over blocks; res_last is per block (a function-static per rank in the reference), from
+   0 at the first step of this call. */
+int oc_step(const oc_config *c, int nb, oc_block *blocks, int nsteps, double *dt, double *time,
+            double *res) {
   work_t *W = alloc_work(c, nb, blocks);
   double **qn = malloc(sizeof(double *) * nb);
+  double *res_last = calloc(nb, sizeof(double));
   for (int bi = 0; bi < nb; ++bi) qn[bi] = malloc(sizeof(double) * 5 * W[bi].N);
   for (int s = 0; s < nsteps; ++s) {
     double dtg = 0.0;
@@ -824,8 +841,23 @@ int oc_step(const oc_config *c, int nb, oc_block *blocks, int nsteps, double *dt
     }
     if (dt) dt[s] = dtg;
     if (time) *time = *time + dtg;
+    double rmax = 0.0;
+    for (int bi = 0; bi < nb; ++bi) {
+      long n5 = 5 * W[bi].N;
+      double sum = 0.0;
+      for (long x = 0; x < n5; ++x) {
+        double d = blocks[bi].q[x] - qn[bi][x];
+        sum += sq(d);
+      }
+      double r = sqrt(sum / (double)((unsigned long)n5));
+      double rl = fabs(r - res_last[bi]) / (dtg * dtg);
+      res_last[bi] = r;
+      if (rl > rmax) rmax = rl;
+    }
+    if (res) res[s] = rmax;
   }
   for (int bi = 0; bi < nb; ++bi) free(qn[bi]);
+  free(res_last);
   free(qn);
   free_work(nb, W);
   return 0;

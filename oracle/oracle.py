@@ -45,12 +45,19 @@ def lib() -> ctypes.CDLL:
                                 ctypes.POINTER(ctypes.c_double)]
         _lib.oc_step.argtypes = [ctypes.POINTER(OcConfig), ctypes.c_int, ctypes.POINTER(OcBlock),
                                  ctypes.c_int, ctypes.POINTER(ctypes.c_double),
-                                 ctypes.POINTER(ctypes.c_double)]
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         _lib.oc_metrics.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 8
         _lib.oc_diag.argtypes = [ctypes.POINTER(OcConfig), ctypes.c_int, ctypes.POINTER(OcBlock),
                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                  ctypes.POINTER(ctypes.c_void_p)]
+        _lib.oc_cr_pow.restype = ctypes.c_double
+        _lib.oc_cr_pow.argtypes = [ctypes.c_double, ctypes.c_double]
     return _lib
+
+
+def cr_pow(x: float, y: float) -> float:
+    """The oracle's pow for the energy reset (oracle/cr_pow.h)."""
+    return lib().oc_cr_pow(x, y)
 
 
 def _ptr(a):
@@ -119,10 +126,13 @@ class Run:
         return dt.value, [k[2].copy() for k in self._keep]
 
     def step(self, n):
+        """n steps: (dt per step, time); self.res gets the residual of each step."""
         arr = self._arr()
         dts = (ctypes.c_double * n)()
+        res = (ctypes.c_double * n)()
         t = ctypes.c_double(0.0)
-        lib().oc_step(ctypes.byref(self.cfg), len(self.blocks), arr, n, dts, ctypes.byref(t))
+        lib().oc_step(ctypes.byref(self.cfg), len(self.blocks), arr, n, dts, ctypes.byref(t), res)
+        self.res = np.array(res[:])
         return np.array(dts[:]), t.value
 
     def q(self, b):

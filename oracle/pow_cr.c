@@ -1,5 +1,5 @@
 /*
- * pow_cr.c -- correctly rounded pow(x, 2) and pow(x, 1.5) for the oracle build.
+ * pow_cr.c -- correctly rounded pow for the oracle build.
  *
  * TEST INFRASTRUCTURE ONLY.  The NUC3d reference evaluates squares through
  * std::pow with a run-time exponent p = 2.0 (src/weno5js.cpp:7-8,97-99,
@@ -10,8 +10,11 @@
  * binary interposes `pow` so that
  *   pow(x, 2.0) == x*x                (the correctly rounded square), and
  *   pow(x, 1.5) == cr_pow15(x) below  (x*sqrt(x) with an exact-residual fix),
- * while every other exponent still goes to libm.  The GPU kernels evaluate the
- * same two formulas, so the reference, the C restatement and the CUDA path can
+ *   pow(x, y) == nuc3d_cr_pow(x, y)   (cr_pow.h) for every other exponent and
+ *                                      x > 0, which serves the energy reset's
+ *                                      pow(rho, gamma) (src/physicsModel.cpp:329);
+ * arguments outside cr_pow.h's domain still go to libm.  The GPU kernels evaluate
+ * the same formulas, so the reference, the C restatement and the CUDA path can
  * be compared bit for bit.  The stock-libm reference build is kept beside this
  * one and the tests bound the difference between the two to round-off.
  *
@@ -26,6 +29,8 @@
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
+
+#include "cr_pow.h"
 
 static double (*libm_pow)(double, double) = 0;
 
@@ -42,6 +47,10 @@ double nuc3d_cr_pow15(double x) {
 double pow(double x, double y) {
   if (y == 2.0) return x * x;
   if (y == 1.5 && x > 0.0 && x < 1.0e300 && x > 1.0e-300) return nuc3d_cr_pow15(x);
+  if (x > 0.0) {
+    const double r = nuc3d_cr_pow(x, y);
+    if (r == r) return r;
+  }
   if (!libm_pow) {
     libm_pow = (double (*)(double, double))dlsym(RTLD_NEXT, "pow");
     if (!libm_pow) {

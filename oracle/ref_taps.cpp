@@ -11,7 +11,8 @@
 //   nuc3d_ref_taps init  OUT   metrics + Q after block::initial (src/block.cpp:31-100)
 //   nuc3d_ref_taps rhs   OUT   one right-hand side: EulerData3D::solve or its NS override
 //                              (src/euler3d.cpp:248-262, src/NaiverStokes3d.cpp:36-49)
-//   nuc3d_ref_taps steps N OUT  N TVD-RK3 steps of block::solve (src/block.cpp:569-594)
+//   nuc3d_ref_taps steps N OUT  N TVD-RK3 steps of block::solve (src/block.cpp:569-594):
+//                              Q, and per step dt, time and the residual block::RES
 //   nuc3d_ref_taps time  N W    W untimed + N timed steps; prints the reference's own
 //                              per-step wall time (src/block.cpp:576-584) as JSON
 //   nuc3d_ref_taps post  N OUT  N steps, then block::Post (src/block.cpp:601-618), whose
@@ -214,17 +215,19 @@ int main(int argc, char **argv) {
     } else if (mode == "steps") {
       if (argc < 4) return 2;
       int n = std::atoi(argv[2]);
-      std::vector<double> dts, times;
+      std::vector<double> dts, times, res;
       for (int s = 0; s < n; ++s) {
         h.myBlock.solve(h.myOperator, h.myPhys, h.myMPI, h.myBC, h.myIO);
         dts.push_back(h.myBlock.dt);
         times.push_back(h.myBlock.time);
+        res.push_back(h.myBlock.RES);  // PDEData3d::setRES via block::solve (src/block.cpp:593)
       }
       Writer w(ranked(argv[3], rank));
       w.fields("Q", h.myBlock.myPDE.getQ());
       if (n > 0) {
         w.rec("dt", {(long long)n}, dts.data());
         w.rec("time", {(long long)n}, times.data());
+        w.rec("res", {(long long)n}, res.data());
       }
     } else if (mode == "post") {
       if (argc < 4) return 2;

@@ -136,8 +136,9 @@ def stack(d: dict, name: str, n: int) -> np.ndarray:
 
 
 def run(case: Case, mode: str, *args, binary: str = "nuc3d_ref_taps", keep: Path | None = None,
-        timeout: float = 3600.0) -> list:
-    """Run the taps harness; returns one dict of arrays per rank."""
+        timeout: float = 3600.0, stdout: list | None = None) -> list:
+    """Run the taps harness; returns one dict of arrays per rank.  stdout (a list), if
+    given, receives the reference's standard output (all ranks)."""
     tmp = Path(keep) if keep else Path(tempfile.mkdtemp(prefix="nuc3d_ref_"))
     try:
         write_case(case, tmp)
@@ -151,6 +152,8 @@ def run(case: Case, mode: str, *args, binary: str = "nuc3d_ref_taps", keep: Path
         if p.returncode != 0:
             raise RuntimeError(f"reference failed ({p.returncode}):\n{p.stdout[-2000:]}\n"
                                f"{p.stderr[-2000:]}")
+        if stdout is not None:
+            stdout.append(p.stdout)
         if mode == "time":
             return [p.stdout]
         return [read_nuct(Path(f"{out}.r{r}")) for r in range(case.nranks)]
@@ -206,6 +209,12 @@ def prim_to_q(prim, jac, gamma):
     rho, u, v, w, p = prim
     rhoe = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
     return np.stack([rho / jac, (rho * u) / jac, (rho * v) / jac, (rho * w) / jac, rhoe / jac])
+
+
+def reset_lines(text: str) -> int:
+    """Cells whose energy the reference's con2prim reset: it prints one "negative pressure
+    at<rank>:i,j,k" line per cell and right-hand side (src/physicsModel.cpp:324-332)."""
+    return text.count("negative pressure at")
 
 
 def spherical_riemann_prim(xc, yc, zc, radius=0.2, centre=(0.5, 0.5, 0.5)):

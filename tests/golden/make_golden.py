@@ -9,7 +9,8 @@ Each fixture <name>.npz holds one case:
   q0              Q = U/J at t = 0 (5, nz, ny, nx)
   rhs, dt_local   one right-hand side at q0 (EulerData3D::solve / its NS override)
   q1, qn          Q after 1 and after `nsteps` TVD-RK3 steps (block::solve)
-  dt, time        per-step dt and accumulated time of those nsteps
+  dt, time, res   per-step dt, accumulated time and residual (block::RES) of those nsteps
+  reset_cells     con2prim energy resets over the nsteps (its printed lines)
   metrics_*       (only in the first fixture) the reference's metrics, to pin the
                   host metric computation
 multi/<name>.2ranks.npz the same case run as two ranks (cases marked ranks2), and
@@ -132,6 +133,14 @@ def case_defs():
              init="sphere",
              params=dict(Reynolds=1000.0, Mach=1.0, Pt=0.72, Gamma=1.4, T_ref=110.4,
                          T_inf=288.0, T_wall=1.0), nsteps=3, ranks2=True),
+        # con2prim's energy reset (src/physicsModel.cpp:324-332): the blast trips it at stages
+        # 1 and 2 of the first step, and cells planted with negative internal energy trip it
+        # at stage 0, where the reset state is what Q_Euler keeps (src/PDEData3d.cpp:74-76)
+        dict(name="sphere_reset_euler_weno5z_ausm", model="Euler3d", riemann="AUSM",
+             schemes=("weno5z",) * 3, shape=(24, 24, 24), lo=(0, 0, 0), hi=(1, 1, 1),
+             wavy=0.0, faces=["outlet"] * 6, init="sphere_reset",
+             params=dict(Reynolds=1000.0, Mach=1.0, Pt=0.72, Gamma=1.4, T_ref=110.4,
+                         T_inf=288.0, T_wall=1.0), nsteps=3, diag=False),
         dict(name="mixed_compact_ausmp", model="Euler3d", riemann="AUSMp",
              schemes=("crweno5", "hccs", "weno5z"), shape=(12, 16, 12), lo=(0, 0, 0),
              hi=(1.0, 1.5, 1.0), wavy=0.2,
@@ -150,6 +159,18 @@ def initial_prim(kind, xc, yc, zc, p):
     g, m = p["Gamma"], p["Mach"]
     if kind == "sphere":
         return R.spherical_riemann_prim(xc, yc, zc)
+    if kind == "sphere_reset":
+        # the blast, plus moving cells with negative pressure (so negative internal energy)
+        # on a sparse lattice outside the sphere
+        prim = R.spherical_riemann_prim(xc, yc, zc)
+        n = xc.shape
+        k, j, i = np.meshgrid(*(np.arange(m) for m in n), indexing="ij")
+        plant = ((i % 11 == 3) & (j % 13 == 5) & (k % 7 == 2))
+        plant &= (xc - 0.5) ** 2 + (yc - 0.5) ** 2 + (zc - 0.5) ** 2 > 0.3 ** 2
+        prim[1] = np.where(plant, 0.5, prim[1])
+        prim[3] = np.where(plant, -0.25, prim[3])
+        prim[4] = np.where(plant, -0.01, prim[4])
+        return prim
     if kind == "smooth":
         rho = 1.0 + 0.2 * np.sin(2.0 * math.pi * xc) * np.cos(math.pi * yc)
         u = 0.3 + 0.1 * np.cos(math.pi * zc)
@@ -193,11 +214,15 @@ def generate(cd):
         q0 = R.stack(init, "Q", 5)
     rhs = R.run(case, "rhs")[0]
     s1 = R.run(case, "steps", 1)[0]
-    sn = R.run(case, "steps", cd["nsteps"])[0]
+    printed = []
+    sn = R.run(case, "steps", cd["nsteps"], stdout=printed)[0]
     out = dict(
         config=json.dumps({k: v for k, v in cd.items()}),
         q0=q0, rhs=R.stack(rhs, "RHS", 5), dt_local=rhs["dt_local"],
         q1=R.stack(s1, "Q", 5), qn=R.stack(sn, "Q", 5), dt=sn["dt"], time=sn["time"],
+        res=sn["res"],  # block::RES after each step (PDEData3d::setRES)
+        # cells whose energy con2prim reset over the n steps (one printed line each)
+        reset_cells=np.array([R.reset_lines(printed[0])]),
     )
     if cd.get("metrics"):
         out["metrics_jac"] = init["jac"]
@@ -234,7 +259,7 @@ def generate_two_ranks(cd, q0):
     MULTI.mkdir(exist_ok=True)
     res = dict(nsteps=np.array([cd["nsteps"]]), q0=q0,
                qn=np.concatenate([R.stack(o, "Q", 5) for o in out], axis=-1),
-               dt=out[0]["dt"], time=out[0]["time"])
+               dt=out[0]["dt"], time=out[0]["time"], res=out[0]["res"])
     np.savez_compressed(MULTI / f"{cd['name']}.2ranks.npz", **res)
     return res
 
@@ -304,6 +329,8 @@ def main(names=None, diag_only=False):
             if cd.get("ranks2"):
                 t = generate_two_ranks(cd, o["q0"])
                 print(f"{cd['name']} 2 ranks: dt={t['dt']}")
+        if not cd.get("diag", True):
+            continue
         if not diag_defined(cd):
             print(f"{cd['name']} diag: skipped (the reference's difference reads past its tile)")
             continue

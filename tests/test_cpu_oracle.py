@@ -44,6 +44,7 @@ def test_oracle_steps_bitwise(name):
     dt, t = r.step(n)
     assert np.array_equal(r.q(0), g.qn), np.max(np.abs(r.q(0) - g.qn))
     assert np.array_equal(dt, g.dt) and t == g.time[-1]
+    assert np.array_equal(r.res, g.res), (r.res, g.res)  # block::RES after each step
 
 
 @pytest.mark.parametrize("name", G.diag_names())
@@ -92,6 +93,7 @@ def test_oracle_two_ranks_bitwise(name):
     assert np.array_equal(dt, mr["dt"]) and t == mr["time"][-1]
     q = np.concatenate([r.q(0), r.q(1)], axis=-1)
     assert np.array_equal(q, mr["qn"]), np.max(np.abs(q - mr["qn"]))
+    assert np.array_equal(r.res, mr["res"])  # MPI_Allreduce MAX of the ranks' residuals
     assert not np.array_equal(q, g.qn)
 
 
