@@ -3,6 +3,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --workload turbulence24      (the 24-block Navier-Stokes grid)
+    python bench.py --profile-case --shape 192 --sweeps 2 [--steps N] [--ns] [--hybrid]
+                                                 (untimed: the command ncu captures)
 
 Workload (one per GPU): the shock-dominated FP64 Euler case -- a 256^3 block on
 [0,1]^3 with extrapolation (outlet) faces, spherical discontinuity rho,p = 1,10
@@ -62,7 +64,7 @@ FLOPS = {
 SWEEP_BYTES = {0: 72 + 40, 1: 72 + 80, 2: 72 + 80}
 # DRAM bytes per cell the same launches moved under ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of a 192^3 block, whose every array is larger than L2, divided by
-# its cells; a launch's traffic grows with its cells): profiles/sweep_kernel_sphere_fast.md.
+# its cells; a launch's traffic grows with its cells).
 SWEEP_TRAFFIC = {0: 108.1, 1: 152.1, 2: 150.8}
 
 
@@ -276,11 +278,12 @@ def ours(args):
 
     cfg = nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="Euler3d", mach=1.0,
                     gamma=1.4, cfl=0.5, exact=args.exact, weno5z_compat=True)
-    q0, m = C.spherical_riemann(SHAPE)
+    q0, _ = C.spherical_riemann(SHAPE)
     cells = int(np.prod(SHAPE))
     s = nb.Solver(cfg, device=local)
     b = s.add_block(*SHAPE, *C.outlet_faces())
-    s.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
+    # metrics by block::getJacobians from the unit-box nodes on the GPU: the reference's own
+    s.set_nodes(b, *C.unit_box_nodes(SHAPE))
     s.finalize()
     stream = torch.cuda.Stream(device=dev)
     s.set_stream(stream.cuda_stream)
@@ -315,6 +318,7 @@ def ours(args):
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     s.sync()
     status = s.status()
+    resets = s.energy_resets()  # over the warm-up and timed steps
     value = whole_job_rate(world, cells, args.steps, ms)
 
     # ---- end to end through the public API with pinned host buffers ----
@@ -418,7 +422,12 @@ def ours(args):
                    "l2": "no flush: 3 state buffers of 671 MB + RHS + metrics = 4 GB > 126 MB L2",
                    "parallelism": f"replicas x{world} (one independent block per GPU)",
                    "tile_shapes": list(tiles),
-                   "status_bits": status},
+                   "status_bits": status,
+                   "energy_reset_cells": resets,
+                   "energy_reset_note": "cells whose energy con2prim reset (e < 0, "
+                                        "src/physicsModel.cpp:324-332), once per cell and "
+                                        "right-hand side, over the warm-up and timed steps",
+                   "metrics": "block::getJacobians of the unit-box nodes (the reference's)"},
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "Mcell-RK3-steps/s",
                 "h2d_bytes_per_step": 5 * cells * 8, "d2h_bytes_per_step": 5 * cells * 8,
@@ -537,6 +546,45 @@ def turbulence24(args):
     return 0
 
 
+def profile_case(args):
+    """--profile-case: the workload at a chosen size, untimed -- the command ncu captures.
+    Euler: the spherical Riemann problem (this file's workload); --ns: the Navier-Stokes
+    Taylor-Green vortex (WENO5-JS, LF, periodic).  --sweeps R launches each direction's
+    right-hand-side sweep 1 + R times (the launches the roofline times) instead of stepping;
+    --hybrid sets the learned face sensor."""
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+    shape = (args.shape,) * 3
+    if args.ns:
+        cfg = nb.Config(scheme_ivs=("weno5js",) * 3, riemann="LF", model="NavierStokes3d",
+                        mach=0.1, reynolds=1600.0, exact=args.exact)
+        q, m = C.taylor_green(shape)
+        faces = C.periodic_faces()
+    else:
+        cfg = nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="Euler3d", mach=1.0,
+                        exact=args.exact, weno5z_compat=True)
+        q, m = C.spherical_riemann(shape)
+        faces = C.outlet_faces()
+    s = nb.Solver(cfg)
+    b = s.add_block(*shape, *faces)
+    s.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
+    s.finalize()
+    s.set_q(b, q)
+    if args.tiles:
+        s.set_tiles(args.tiles)
+    if args.hybrid:
+        from nuc3d_b200 import sensor
+        s.set_sensor(sensor.load_weights(), sensor.DEFAULT_THRESHOLD)
+    if args.sweeps > 0:
+        print([s.profile_sweep(d, args.sweeps) for d in range(3)])
+    else:
+        s.step(args.steps)
+        t, dt = s.time_dt()
+        print(f"{shape} steps={args.steps} time={t:.6g} dt={dt:.6g} status={s.status()}")
+    s.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -549,7 +597,15 @@ def main():
                     help="sweep tile shapes per direction, e.g. 2,0,0 (default: nuc3d_autotune)")
     ap.add_argument("--workload", default="sphere256", choices=["sphere256", "turbulence24"],
                     help="turbulence24: the 24-block Navier-Stokes grid on one GPU (our arm only)")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="untimed run of the workload at --shape (the target of ncu captures)")
+    ap.add_argument("--shape", type=int, default=128, help="--profile-case: cells per axis")
+    ap.add_argument("--sweeps", type=int, default=0, help="--profile-case: sweep launches")
+    ap.add_argument("--ns", action="store_true", help="--profile-case: NS Taylor-Green")
+    ap.add_argument("--hybrid", action="store_true", help="--profile-case: learned sensor")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.workload == "turbulence24":

@@ -144,6 +144,12 @@ int nuc3d_sync(nuc3d_ctx *ctx);
 int nuc3d_get_time(nuc3d_ctx *ctx, double *time, double *dt);
 int nuc3d_set_time(nuc3d_ctx *ctx, double time);
 int nuc3d_get_status(nuc3d_ctx *ctx, unsigned *status);
+/* Cells whose energy con2prim reset because their internal energy was negative
+   (physicsModel::con2prim, src/physicsModel.cpp:324-332), counted once per cell and
+   right-hand-side evaluation and summed since the context was created: the number of
+   "negative pressure at" lines the reference prints for the same evaluations.  Profiling
+   and autotuning sweeps leave it unchanged. */
+int nuc3d_get_energy_resets(nuc3d_ctx *ctx, unsigned long long *cells);
 
 /* CUDA stream (cudaStream_t) the context launches on; NULL = its own stream. */
 int nuc3d_set_stream(nuc3d_ctx *ctx, void *stream);
@@ -226,21 +232,26 @@ int nuc3d_block_get_vis(nuc3d_ctx *ctx, int block, double *vis);
 
 /* ---- Allocation-free right-hand side -------------------------------------------
    No counterpart in the reference: it exists for callers that cannot allocate device
-   memory where they evaluate the right-hand side (inside a CUDA stream capture that
-   must not allocate, under a host framework that owns all device memory, in loops
-   where an allocation would stall).  One Euler3d block: all array arguments are
-   DEVICE pointers owned by the caller (q, metrics as in nuc3d_block_set_metrics, and
-   the output rhs, 5N); bc_type[f] is -1 (physical) or 0 (the block is its own
-   neighbour, i.e. periodic).  It calls no cudaMalloc/cudaFree: its working memory
-   (block descriptor, step state, face list, 40 bytes per cell of every physical face)
-   is a static device array of NUC3D_NOALLOC_SCRATCH_BYTES that every GPU loading the
-   library keeps until the process exits; larger blocks are rejected with NUC3D_EINVAL.
-   The first call on a device looks up that array's device address and sets kernel
-   attributes, so make the first call before any stream capture.  All calls share the
-   array: calls that overlap on the GPU (different streams, or threads without
-   ordering) race and must be serialised by the caller.  With dt_local non-NULL the
-   call waits for the stream and returns 1/max eigenvalue; with NULL it is
-   asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream). */
+   memory where they evaluate the right-hand side (a host framework that owns every
+   device buffer and forbids allocations by libraries, a loop where an allocation could
+   stall).  One Euler3d block.  Device pointers, owned by the caller: q (5N), jac (N),
+   xi_xyz, eta_xyz, zeta_xyz (3N each, as in nuc3d_block_set_metrics), dxyz (9N; only
+   read by symmetry faces, may be NULL otherwise) and the output rhs (5N).  Host
+   pointers: bc_type and bc_id (6 ints; bc_type[f] is -1 for a physical face or 0 for a
+   face joined to the block itself, i.e. periodic), bc_values (NULL, or 6 x 5 doubles
+   rho, u, v, w, p per face, read for inlet faces) and dt_local (NULL or one double).
+   It calls no cudaMalloc/cudaFree: its working memory (block descriptor, step state,
+   face list, 40 bytes per cell of every physical face) is a static device array of
+   NUC3D_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until the process
+   exits; blocks whose physical faces need more are rejected with NUC3D_EINVAL.  The first
+   call on a device looks up that array's device address and sets kernel attributes, so
+   make that first call before any stream capture.  All calls share the array and each
+   call overwrites it: calls that overlap on the GPU (different streams, or threads
+   without ordering) race and must be serialised by the caller.  With dt_local non-NULL
+   the call waits for the stream, returns 1/max eigenvalue in *dt_local and reports
+   negative pressure or non-finite values as NUC3D_ENUMERIC; with NULL it only queues the
+   work on `stream` (a cudaStream_t, NULL = legacy default stream) and reports no numeric
+   status.  The calling thread's current device is the same on return as on entry. */
 #define NUC3D_NOALLOC_SCRATCH_BYTES (8u << 20)
 int nuc3d_rhs_noalloc(const nuc3d_config *cfg, int device, int nx, int ny, int nz,
                       const int bc_type[6], const int bc_id[6], const double *bc_values,

@@ -40,7 +40,7 @@ EXPORTED = (
     "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step", "nuc3d_diagnostics", "nuc3d_block_get_diag",
     "nuc3d_block_set_nodes", "nuc3d_block_get_metrics", "nuc3d_sensor_record",
     "nuc3d_sensor_loss_grad", "nuc3d_sensor_adam", "nuc3d_set_sensor", "nuc3d_set_tiles",
-    "nuc3d_get_tiles", "nuc3d_autotune",
+    "nuc3d_get_tiles", "nuc3d_autotune", "nuc3d_get_energy_resets",
 )
 
 
@@ -111,6 +111,7 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_get_time.argtypes = [P, PD, PD]
     lib.nuc3d_set_time.argtypes = [P, D]
     lib.nuc3d_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint)]
+    lib.nuc3d_get_energy_resets.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong)]
     lib.nuc3d_set_stream.argtypes = [P, P]
     lib.nuc3d_use_graph.argtypes = [P, I]
     lib.nuc3d_block_get_prim.argtypes = [P, I, PD]
@@ -331,6 +332,13 @@ class Solver:
         s = ctypes.c_uint()
         _check(self.lib.nuc3d_get_status(self._ctx, ctypes.byref(s)))
         return s.value
+
+    def energy_resets(self) -> int:
+        """Cells whose energy con2prim reset, once per cell and right-hand side, since the
+        context was created (the reference prints one "negative pressure at" line each)."""
+        n = ctypes.c_ulonglong()
+        _check(self.lib.nuc3d_get_energy_resets(self._ctx, ctypes.byref(n)))
+        return n.value
 
     def profile_sweep(self, direction: int, reps: int = 10) -> float:
         """Mean device milliseconds of one launch of the direction sweep kernel."""

@@ -50,6 +50,16 @@ def prim_to_q(prim, jac, gamma):
     return np.stack([rho / jac, (rho * u) / jac, (rho * v) / jac, (rho * w) / jac, rhoe / jac])
 
 
+def unit_box_nodes(shape):
+    """Node coordinates (x, y, z), each (nz+1, ny+1, nx+1), of the unit box: i/nx, j/ny,
+    k/nz, the mesh the reference reads for the shock-dominated workload.  Metrics taken from
+    them by block::getJacobians (nuc3d_block_set_nodes) are the reference's own, bit for bit;
+    the analytic uniform_metrics differ from those in the last bits."""
+    xs = [np.arange(n + 1, dtype=np.float64) / n for n in shape]
+    Z, Y, X = np.meshgrid(xs[2], xs[1], xs[0], indexing="ij")
+    return X, Y, Z
+
+
 def spherical_riemann(shape, gamma=1.4, radius=0.2):
     X, Y, Z = centres(shape)
     r2 = (X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2

@@ -141,6 +141,9 @@ struct StepState {
   double time;                      // accumulated time
   unsigned status;                  // StatusBits
   unsigned pad_;
+  unsigned long long reset_cells;   // cells whose energy con2prim reset (src/physicsModel.cpp:
+                                    // 324-332), once per cell and right-hand side; the
+                                    // reference prints one "negative pressure at" line for each
 };
 
 // What the host hands to a stage launch.

@@ -468,12 +468,13 @@ template <int DIR, int SCH, int SHP = 0> struct TileSmem {
 
 // Phase 1: split fluxes F+/F- of the tile's line positions c0-R .. c0+cl+R-1 into sF
 // ([10][TW][SP]); own cells of the zeta tile also leave their state in sQ; eig reduces
-// max(|U|+c|grad xi|) over the three directions.
+// max(|U|+c|grad xi|) over the three directions; nres (xi sweeps) counts the own cells
+// whose energy con2prim reset.
 template <int DIR, int SCH, bool RHOP = false, int SHP = 0>
 __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks, const TileCtx &T,
                                             const SolverParams &P, int stage, bool eig, double *sF,
                                             double *sQ, unsigned &st, double &emax,
-                                            double *sRP = nullptr) {
+                                            double *sRP = nullptr, unsigned *nres = nullptr) {
   using M = TileSmem<DIR, SCH, SHP>;
   constexpr int R = M::R, TW = M::TW, NP = M::NP, SP = M::SP, SQ = M::SQ;
   const BlockDev &B = *T.B;
@@ -503,6 +504,7 @@ __device__ __forceinline__ void phase_split(const BlockDev *__restrict__ blocks,
           sRP[w * SP + p] = s.rho;
           sRP[(TW + w) * SP + p] = s.p;
         }
+        if (DIR == 0 && nres && own && s.reset && g >= T.c0 && g < T.c0 + T.cl) ++*nres;
         if (own && eig && g >= T.c0 && g < T.c0 + T.cl) {
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
@@ -660,11 +662,22 @@ __device__ __forceinline__ void phase_cells(const TileCtx &T, const SolverParams
       if (flags & SW_RK) {
         double *__restrict__ qo = B.q[(stage + 1) % 3];
         const double *__restrict__ qn = B.q[0];
+        // u_n: the state stage 0 started from, with con2prim's energy reset applied, as
+        // the reference's Q_Euler = Q_work copy takes it after stage 0's right-hand side
+        // wrote the reset into Q_work (src/physicsModel.cpp:324-332, src/PDEData3d.cpp:74-76)
+        double un[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        if (stage != 0) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) un[v] = qn[v * N + idx];
+          CellPrim sn;
+          unsigned stn = 0;
+          con2prim(un, __ldg(B.jac + idx), P.gamma, P.mach, sn, stn);
+          un[4] = sn.q4;
+        }
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
           const double ui = sQ[(v * TW + w) * SQ + c];
-          const double un = stage == 0 ? 0.0 : qn[v * N + idx];
-          const double x = rk3_update(stage, r[v], ui, un, dt);
+          const double x = rk3_update(stage, r[v], ui, un[v], dt);
           if (!isfinite(x)) st |= ST_NONFINITE;
           qo[v * N + idx] = x;
         }
@@ -739,7 +752,9 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       for (int v = 0; v < 5; ++v) cp_async8(sR + (v * TL + c) * TW + w, T.B->rhs + v * T.N + idx);
     }
   }
-  phase_split<DIR, SCH, HYB, SHP>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st, emax, sRP);
+  unsigned nres = 0;
+  phase_split<DIR, SCH, HYB, SHP>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st, emax, sRP,
+                                  DIR == 0 ? &nres : nullptr);
   if (ns) phase_vis<DIR, SCH, SHP>(blocks, T, P, sV);
   __syncthreads();
 
@@ -873,6 +888,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   phase_cells<DIR, SCH, SHP>(T, P, S, stage, flags, sH, sV, sQ, st, sR);
   if (eig) reduce_eig(emax, sRed, S);
   if (st) atomicOr(&S->status, st);
+  if (nres) atomicAdd(&S->reset_cells, (unsigned long long)nres);
 }
 
 // ---------------------------------------------------------------------------------
@@ -912,7 +928,9 @@ compact_rows_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParam
   const bool eig = (flags & SW_EIG) != 0;
   unsigned st = 0;
   double emax = 0.0;
-  phase_split<DIR, SCH>(blocks, T, P, stage, eig, sF, nullptr, st, emax);
+  unsigned nres = 0;
+  phase_split<DIR, SCH>(blocks, T, P, stage, eig, sF, nullptr, st, emax, nullptr,
+                        DIR == 0 ? &nres : nullptr);
   __syncthreads();
   const BlockDev &B = *T.B;
   const int L = T.G.L, ts = T.ts, f0 = WHOLE ? 0 : ts, m = L - 2 * f0 + 1;
@@ -960,6 +978,7 @@ compact_rows_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParam
   }
   if (eig) reduce_eig(emax, sRed, S);
   if (st) atomicOr(&S->status, st);
+  if (nres) atomicAdd(&S->reset_cells, (unsigned long long)nres);
 }
 
 // One thread per (line, variable, split) system of one direction.

@@ -754,8 +754,10 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
   if (!cached) {
     cudaSetDevice(c->device);
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    unsigned status0 = 0;  // the timing sweeps must not leave status bits behind
+    unsigned status0 = 0;  // the timing sweeps must not leave status bits or resets behind
+    unsigned long long resets0 = 0;
     CUDA_TRY(cudaMemcpy(&status0, &c->d_state->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&resets0, &c->d_state->reset_cells, sizeof(resets0), cudaMemcpyDeviceToHost));
     EventPair ev;
     CUDA_TRY(cudaEventCreate(&ev.a));
     CUDA_TRY(cudaEventCreate(&ev.b));
@@ -784,6 +786,7 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
       cur[d] = best[d];
     }
     CUDA_TRY(cudaMemcpy(&c->d_state->status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(&c->d_state->reset_cells, &resets0, sizeof(resets0), cudaMemcpyHostToDevice));
     std::lock_guard<std::mutex> g(g_tune_mutex);
     g_tune_cache[key] = best;
   }
@@ -828,6 +831,15 @@ int nuc3d_get_status(nuc3d_ctx *c, unsigned *status) {
   return NUC3D_OK;
 }
 
+int nuc3d_get_energy_resets(nuc3d_ctx *c, unsigned long long *cells) {
+  if (!c || !cells) return fail(NUC3D_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(cells, &c->d_state->reset_cells, sizeof(unsigned long long),
+                      cudaMemcpyDeviceToHost));
+  return NUC3D_OK;
+}
+
 int nuc3d_set_stream(nuc3d_ctx *c, void *stream) {
   if (!c) return fail(NUC3D_EINVAL, "null context");
   cudaSetDevice(c->device);
@@ -852,6 +864,9 @@ int nuc3d_profile_sweep(nuc3d_ctx *c, int dir, int reps, double *ms) {
   auto sweep = [&]() {
     return c->exact ? nuc3d::exact::run_sweep(c->L, dir, 0, 0) : nuc3d::fast::run_sweep(c->L, dir, 0, 0);
   };
+  unsigned long long resets0 = 0;  // profiling sweeps leave the reset count as it was
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(&resets0, &c->d_state->reset_cells, sizeof(resets0), cudaMemcpyDeviceToHost));
   CUDA_TRY(sweep());  // warm-up
   EventPair ev;
   CUDA_TRY(cudaEventCreate(&ev.a));
@@ -864,6 +879,7 @@ int nuc3d_profile_sweep(nuc3d_ctx *c, int dir, int reps, double *ms) {
   float t = 0.0f;
   CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
   *ms = (double)t / reps;
+  CUDA_TRY(cudaMemcpy(&c->d_state->reset_cells, &resets0, sizeof(resets0), cudaMemcpyHostToDevice));
   return check_status(c);
 }
 

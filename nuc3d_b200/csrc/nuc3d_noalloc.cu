@@ -2,10 +2,9 @@
 // with every byte of working memory taken from a fixed static device array.
 //
 // Who needs it: callers that cannot call cudaMalloc at the point where they evaluate
-// the right-hand side -- code running inside a CUDA stream capture that must not
-// allocate, host frameworks with their own memory pool that forbid foreign
-// allocations, or real-time loops where an allocation could stall.  They bring their
-// own device buffers for the inputs (state, metrics) and the output (RHS); the
+// the right-hand side -- host frameworks with their own memory pool that forbid
+// foreign allocations, or real-time loops where an allocation could stall.  They bring
+// their own device buffers for the inputs (state, metrics) and the output (RHS); the
 // library's working memory is the file-scope array below.
 //
 // The array holds the block descriptor, the step state (eigenvalue maximum and
@@ -14,6 +13,8 @@
 // by every GPU that loads the library until the process exits.  Its host-side name is
 // only a stand-in: host code takes the device address with cudaGetSymbolAddress, once
 // per device, with that device current, and passes that address to the kernels.
+// The descriptors reach the array through the arguments of a one-thread kernel
+// (noalloc_setup), so nothing is copied from host memory.
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -41,6 +42,40 @@ int nfail(int code, const char *msg) {
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// The physical faces of the one block (at most six), passed by value to noalloc_setup.
+struct NoallocFaces {
+  int njobs;
+  unsigned char face[6];
+  int start[7];
+};
+
+// Writes the block descriptor and the face list into the static array and clears the
+// step state (eigenvalue maximum, status, counters): the call's set-up, on the GPU.
+__global__ void noalloc_setup(BlockDev B, NoallocFaces F, BlockDev *dB, StepState *dS,
+                              FaceJobs *dJ) {
+  *dB = B;
+  StepState z;
+  memset(&z, 0, sizeof(z));
+  *dS = z;
+  dJ->njobs = F.njobs;
+  for (int j = 0; j < 6; ++j) {
+    dJ->block[j] = 0;
+    dJ->face[j] = F.face[j];
+  }
+  for (int j = 0; j < 7; ++j) dJ->start[j] = F.start[j];
+}
+
+// Restores the calling thread's current device on every way out of the entry point.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 int scheme_id(const char *s, int *out) {
   if (!s) return 1;
@@ -124,6 +159,7 @@ int nuc3d_rhs_noalloc(const nuc3d_config *cfg, int device, int nx, int ny, int n
   if (device < 0 || device >= kMaxDevices) return nfail(NUC3D_EINVAL, "bad device index");
 
   // ---- one-time set-up on this device: the array's device address, kernel attributes ----
+  DeviceGuard keep_device;  // the caller's current device is restored on return
   if (cudaSetDevice(device) != cudaSuccess) return nfail(NUC3D_ECUDA, "cudaSetDevice failed");
   const int mode = cfg->exact ? 0 : 1;
   {
@@ -144,7 +180,7 @@ int nuc3d_rhs_noalloc(const nuc3d_config *cfg, int device, int nx, int ny, int n
   unsigned char *base = static_cast<unsigned char *>(g_scratch_dev[device]);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-  // ---- descriptors, built on the host and copied into the static array ----
+  // ---- descriptors, built on the host and written into the static array by a kernel ----
   BlockDev B;
   std::memset(&B, 0, sizeof(B));
   for (int d = 0; d < 3; ++d) B.n[d] = n[d];
@@ -165,23 +201,20 @@ int nuc3d_rhs_noalloc(const nuc3d_config *cfg, int device, int nx, int ny, int n
   }
   const int shape0[3] = {0, 0, 0};  // default tile shape in every direction
   set_tile_divisors(B, shape0);
-  static thread_local FaceJobs J;  // host staging only
+  NoallocFaces J;
   std::memset(&J, 0, sizeof(J));
   for (int f = 0; f < 6; ++f) {
     if (bc_type[f] != -1) continue;
     const int d = f >> 1;
     const long long area = d == 0 ? (long long)ny * nz : (d == 1 ? (long long)nz * nx : (long long)nx * ny);
-    J.block[J.njobs] = 0;
     J.face[J.njobs] = (unsigned char)f;
     J.start[J.njobs + 1] = J.start[J.njobs] + (int)((area + 255) / 256);
     ++J.njobs;
   }
-  StepState S0;
-  std::memset(&S0, 0, sizeof(S0));  // the eigenvalue maximum and status start at zero
-  if (cudaMemcpyAsync(base, &B, sizeof(B), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemcpyAsync(base + off_state, &S0, sizeof(S0), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemcpyAsync(base + off_jobs, &J, sizeof(J), cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return nfail(NUC3D_ECUDA, "descriptor upload failed");
+  noalloc_setup<<<1, 1, 0, st>>>(B, J, reinterpret_cast<BlockDev *>(base),
+                                 reinterpret_cast<StepState *>(base + off_state),
+                                 reinterpret_cast<FaceJobs *>(base + off_jobs));
+  if (cudaGetLastError() != cudaSuccess) return nfail(NUC3D_ECUDA, "descriptor set-up launch failed");
 
   Launch L;
   std::memset(&L, 0, sizeof(L));

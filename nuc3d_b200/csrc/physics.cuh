@@ -46,9 +46,98 @@ __device__ __forceinline__ double pow15(double x) {
   return hi + (lo + t);
 }
 
+// ---- pow(x, y) for the energy reset's pow(rho, gamma) (src/physicsModel.cpp:329) ----
+// Double-double arithmetic (Dekker 1971; Knuth's TwoSum; the add, multiply and divide of
+// Hida, Li & Bailey's QD library, 2001), every operation an explicit IEEE intrinsic so that
+// neither build contracts or reorders it:
+//   log x = e ln2 + log m, x = m 2^e, m in [sqrt(1/2), sqrt(2)),
+//   log m = 2 s (1 + z/3 + z^2/5 + ... + z^21/45), s = (m-1)/(m+1), z = s^2,
+//   exp P = 2^k exp r, k = rint(P/ln2), r = P - k ln2, |r| <= 0.347, with
+//   exp r = 1 + r(1 + r/2(1 + r/3(... (1 + r/24)))) (the Taylor sum to r^24/24!),
+// with ln2 as the double-double (0x1.62e42fefa39efp-1, 0x1.abc9e3b39803fp-56).  The
+// result is the correctly rounded x^y unless x^y lies within about 2^-100 of a rounding
+// midpoint; the oracle evaluates the same operation sequence in C, so both return the same
+// bits.  Out of line: it runs only in the rare reset branch.
+struct DD {
+  double hi, lo;
+};
+__device__ __forceinline__ DD dd_two_sum(double a, double b) {
+  const double s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  return {s, __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb))};
+}
+__device__ __forceinline__ DD dd_fast_two_sum(double a, double b) {
+  const double s = __dadd_rn(a, b);
+  return {s, __dsub_rn(b, __dsub_rn(s, a))};
+}
+__device__ __forceinline__ DD dd_two_prod(double a, double b) {
+  const double p = __dmul_rn(a, b);
+  return {p, __fma_rn(a, b, -p)};
+}
+__device__ __forceinline__ DD dd_add(DD x, DD y) {
+  DD s = dd_two_sum(x.hi, y.hi);
+  const DD t = dd_two_sum(x.lo, y.lo);
+  double e = __dadd_rn(s.lo, t.hi);
+  s = dd_fast_two_sum(s.hi, e);
+  e = __dadd_rn(s.lo, t.lo);
+  return dd_fast_two_sum(s.hi, e);
+}
+__device__ __forceinline__ DD dd_neg(DD x) { return {-x.hi, -x.lo}; }
+__device__ __forceinline__ DD dd_mul(DD x, DD y) {
+  const DD p = dd_two_prod(x.hi, y.hi);
+  const double c = __dmul_rn(x.hi, y.lo), d = __dmul_rn(x.lo, y.hi);
+  return dd_fast_two_sum(p.hi, __dadd_rn(p.lo, __dadd_rn(c, d)));
+}
+__device__ __forceinline__ DD dd_mul_d(DD x, double b) {
+  const DD p = dd_two_prod(x.hi, b);
+  return dd_fast_two_sum(p.hi, __dadd_rn(p.lo, __dmul_rn(x.lo, b)));
+}
+__device__ __forceinline__ DD dd_div_d(DD x, double b) {
+  const double q1 = __ddiv_rn(x.hi, b);
+  const DD p = dd_two_prod(q1, b);
+  const double r = __dadd_rn(__dsub_rn(__dsub_rn(x.hi, p.hi), p.lo), x.lo);
+  return dd_fast_two_sum(q1, __ddiv_rn(r, b));
+}
+__device__ __forceinline__ DD dd_div(DD x, DD y) {
+  const double q1 = __ddiv_rn(x.hi, y.hi);
+  DD r = dd_add(x, dd_neg(dd_mul_d(y, q1)));
+  const double q2 = __ddiv_rn(r.hi, y.hi);
+  r = dd_add(r, dd_neg(dd_mul_d(y, q2)));
+  const double q3 = __ddiv_rn(r.hi, y.hi);
+  return dd_add(dd_fast_two_sum(q1, q2), DD{q3, 0.0});
+}
+
+__device__ __noinline__ double cr_pow(double x, double y) {
+  if (!(x > 0x1p-1000 && x < 0x1p1000) || !(fabs(y) < 0x1p20)) return pow(x, y);
+  if (x == 1.0 || y == 0.0) return 1.0;
+  const DD ln2 = {0x1.62e42fefa39efp-1, 0x1.abc9e3b39803fp-56};
+  int e;
+  double m = frexp(x, &e);
+  if (m < 0x1.6a09e667f3bcdp-1) {
+    m = __dmul_rn(m, 2.0);
+    e = e - 1;
+  }
+  const DD s = dd_div(DD{__dsub_rn(m, 1.0), 0.0}, dd_two_sum(m, 1.0));
+  const DD z = dd_mul(s, s);
+  DD t = dd_div_d(DD{1.0, 0.0}, 45.0);
+#pragma unroll 1
+  for (int k = 20; k >= 0; --k)
+    t = dd_add(dd_div_d(DD{1.0, 0.0}, __dadd_rn(__dmul_rn(2.0, (double)k), 3.0)), dd_mul(z, t));
+  const DD lm = dd_mul_d(dd_mul(s, dd_add(DD{1.0, 0.0}, dd_mul(z, t))), 2.0);
+  const DD P = dd_mul_d(dd_add(dd_mul_d(ln2, (double)e), lm), y);
+  if (!(fabs(P.hi) < 700.0)) return pow(x, y);
+  const double k = rint(__ddiv_rn(P.hi, ln2.hi));
+  const DD r = dd_add(P, dd_neg(dd_mul_d(ln2, k)));
+  DD sum = {1.0, 0.0};
+#pragma unroll 1
+  for (int n = 24; n >= 1; --n) sum = dd_add(DD{1.0, 0.0}, dd_mul(dd_div_d(r, (double)n), sum));
+  return ldexp(sum.hi, (int)k);
+}
+
 struct CellPrim {
   double rho, u, v, w, E, p, alpha;
-  double q4;  // energy component of Q actually used (after the reset of :324-332)
+  double q4;   // energy component of Q actually used (after the reset of :324-332)
+  bool reset;  // the reset fired for this cell
 };
 
 // physicsModel::con2prim (src/physicsModel.cpp:307-356) with EoSIdealGasFWD (:981-1054).
@@ -70,8 +159,9 @@ __device__ __forceinline__ void con2prim(const double q[5], double jac, double g
   double E = q[4] * jac;
   double e0 = E - 0.5 * rho * (u * u + v * v + w * w);
   s.q4 = q[4];
+  s.reset = e0 < 0.0;
   if (e0 < 0.0) {
-    E = (pow(rho, gamma) / ((gamma * mach * mach) * (gamma - 1.0)) + 0.5 * rho * (u * u + v * v + w * w));
+    E = (cr_pow(rho, gamma) / ((gamma * mach * mach) * (gamma - 1.0)) + 0.5 * rho * (u * u + v * v + w * w));
     s.q4 = E / jac;
     st |= ST_ENERGY_RESET;
   }

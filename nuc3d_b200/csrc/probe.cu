@@ -6,6 +6,8 @@
 //     several times over, timed with CUDA events.
 //   nuc3d_probe_qdiv         the throughput build's division next to IEEE division on
 //     the same operands, for the accuracy test of the former.
+//   nuc3d_probe_crpow        the energy reset's double-double pow (cr_pow), for the test
+//     that pins its bits to the oracle's.
 #include <cuda_runtime.h>
 
 #define NUC3D_NS fast
@@ -39,9 +41,31 @@ __global__ void qdiv_pairs(const double *a, const double *b, double *q_fast, dou
   }
 }
 
+__global__ void crpow_pairs(const double *x, const double *y, double *r, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    r[i] = nuc3d::fast::cr_pow(x[i], y[i]);
+}
+
 }  // namespace
 
 extern "C" {
+
+// r[i] = cr_pow(x[i], y[i]) on the device; host arrays of n doubles.  Returns 0 or a CUDA
+// error code.
+int nuc3d_probe_crpow(int device, const double *x, const double *y, double *r, long long n) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return (int)e;
+  double *d = nullptr;
+  const size_t bytes = (size_t)n * sizeof(double);
+  if ((e = cudaMalloc(&d, 3 * bytes)) != cudaSuccess) return (int)e;
+  cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+  cudaMemcpy(d + n, y, bytes, cudaMemcpyHostToDevice);
+  crpow_pairs<<<296, 256>>>(d, d + n, d + 2 * n, n);
+  e = cudaMemcpy(r, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return (int)e;
+}
 
 // q_fast[i] = the throughput build's a[i] / b[i], q_ieee[i] = IEEE a[i] / b[i]; host arrays
 // of n doubles.  Returns 0 or a CUDA error code.

@@ -1,8 +1,8 @@
 """nuc3d_rhs_noalloc: the right-hand side for callers that cannot allocate device memory.
 
-Some callers cannot call cudaMalloc where they evaluate the right-hand side: code
-recorded into a CUDA stream capture that must not allocate, host frameworks that own
-every device buffer, time-critical loops where an allocation could stall.  For them the
+Some callers cannot call cudaMalloc where they evaluate the right-hand side: host
+frameworks that own every device buffer, time-critical loops where an allocation could
+stall.  For them the
 library has one entry point that allocates nothing: the caller passes its own device
 buffers for the state, the metrics and the output, and the library's working memory is a
 fixed 8 MiB static device array.  These tests call it through the C ABI and check that it
