@@ -19,8 +19,10 @@
  *                           (src/euler3d.h:38-46)
  *   nuc3d_block_set_q/get_q PDEData3d::Q_work = U/J (src/PDEData3d.hpp:39-44),
  *                           restart read/write (src/block.cpp:754-855)
- *   nuc3d_rhs               EulerData3D::solve / NaiverStokesData3d::solve
+ *   nuc3d_rhs, nuc3d_rhs_stage  EulerData3D::solve / NaiverStokesData3d::solve
  *                           (src/euler3d.cpp:248-262, src/NaiverStokes3d.cpp:36-49) + getDt
+ *   nuc3d_rk_stage          tvdrk3rd::integrationAll (src/TVD-RK3.cpp:16-137)
+ *   nuc3d_get_residual      PDEData3d::setRES / getRes (src/PDEData3d.cpp:90-122)
  *   nuc3d_block_get_rhs     PDEData3d::RHS (src/PDEData3d.hpp:44)
  *   nuc3d_step              block::solve: 3 x (RHS; PDEData3d::solve -> tvdrk3rd)
  *                           (src/block.cpp:569-594, src/PDEData3d.cpp:152-170,
@@ -50,7 +52,9 @@ enum {
   NUC3D_ST_NEG_PRESSURE = 1, /* EoS pressure < 0: the reference exits (src/physicsModel.cpp:1009-1016) */
   NUC3D_ST_ENERGY_RESET = 2, /* internal energy < 0 was reset (src/physicsModel.cpp:324-332) */
   NUC3D_ST_NONFINITE = 4,    /* the RK update produced a NaN or Inf */
-  NUC3D_ST_BAD_LAUNCH = 8
+  NUC3D_ST_BAD_LAUNCH = 8,
+  NUC3D_ST_PIPE_TIMEOUT = 16 /* a pipelined sweep gave up waiting for its loads (2 s); the
+                                results of that evaluation are invalid (NUC3D_ECUDA) */
 };
 
 typedef struct nuc3d_ctx nuc3d_ctx;
@@ -128,6 +132,27 @@ int nuc3d_block_q_device(nuc3d_ctx *ctx, int block, double **dev_q);
    the reference's dt before the cfl factor (src/euler3d.cpp:429-435). */
 int nuc3d_rhs(nuc3d_ctx *ctx, double *dt_local);
 int nuc3d_block_get_rhs(nuc3d_ctx *ctx, int block, double *rhs);
+
+/* The stages of block::solve one call at a time, for a host that drives the reference's
+   loop itself (src/block.cpp:579-580: EulerData3D::solve, then PDEData3d::solve).
+   nuc3d_rhs_stage: the right-hand side of every block at the state of RK stage `stage`
+   (0: the step's state; 1, 2: the states nuc3d_rk_stage(stage - 1) produced), as
+   EulerData3D::solve / NaiverStokesData3d::solve evaluate it on Q_work; dt_local as in
+   nuc3d_rhs.  nuc3d_rhs(ctx, dt) is nuc3d_rhs_stage(ctx, 0, dt).
+   nuc3d_rk_stage: tvdrk3rd::integrationAll (src/TVD-RK3.cpp:16-137) for stage `stage` with
+   the step size dt the caller fixed at stage 0 (PDEData3d::solve, src/PDEData3d.cpp:70-88:
+   cfl times the minimum over ranks of dt_local), from the right-hand side the last
+   nuc3d_rhs_stage(stage) left; the stage state and the step's state enter with con2prim's
+   energy reset applied, as Q_work and Q_Euler hold them.  Stage 2 leaves the new state as
+   the block's current state, adds dt to the time and computes the residual. */
+int nuc3d_rhs_stage(nuc3d_ctx *ctx, int stage, double *dt_local);
+int nuc3d_rk_stage(nuc3d_ctx *ctx, int stage, double dt);
+/* The residual of the last step (PDEData3d::setRES, src/PDEData3d.cpp:90-122, which
+   block::printStatus prints: src/block.cpp:593-598): per block
+   |sqrt(sum over components and cells of (u - u_n)^2 / (5N)) - that root one step earlier|
+   / dt^2, the maximum over blocks.  The reference-order build sums in the reference's order
+   (bit for bit); the throughput build sums per tile (round-off apart). */
+int nuc3d_get_residual(nuc3d_ctx *ctx, double *res);
 
 /* nsteps TVD-RK3 steps (each: three stages; dt fixed at stage 0 as cfl/max eigenvalue).
    Asynchronous on the context's stream; nuc3d_sync waits and checks the status. */
@@ -219,10 +244,19 @@ int nuc3d_get_tiles(nuc3d_ctx *ctx, int shape[3]);
    (a cached choice, a compact direction). */
 int nuc3d_autotune(nuc3d_ctx *ctx, int reps, int shape_out[3], double ms_out[9]);
 
+/* Pipelined sweeps (after nuc3d_finalize; on by default).  No counterpart in the reference.
+   With it on, each explicit-scheme sweep is a persistent kernel (two CTAs per SM) whose
+   producer warp loads the next tiles' state, Jacobian and metric with tensor-map (TMA)
+   copies while the other warps compute; results are identical either way.  It applies to
+   Euler3d contexts whose blocks all have an even nx (16-byte rows); elsewhere, or with
+   on = 0, every sweep CTA loads its own tile.  nuc3d_get_pipeline: 1 if it is in use. */
+int nuc3d_set_pipeline(nuc3d_ctx *ctx, int on);
+int nuc3d_get_pipeline(nuc3d_ctx *ctx, int *on);
+
 /* Kernels one nuc3d_step(ctx, 1) launches (after nuc3d_finalize): per RK stage the BC
    ghost pass (when a block has a physical face), the NS primitive and gradient passes,
-   and one sweep per direction (three kernels for a compact-scheme direction).  No
-   counterpart in the reference. */
+   and one sweep per direction (three kernels for a compact-scheme direction); then the
+   residual kernel after the last stage.  No counterpart in the reference. */
 int nuc3d_kernels_per_step(nuc3d_ctx *ctx, int *kernels);
 
 /* Debug taps: NS primitives (u, v, w, T: 4N) and contravariant viscous fluxes

@@ -40,7 +40,8 @@ EXPORTED = (
     "nuc3d_rhs_noalloc", "nuc3d_kernels_per_step", "nuc3d_diagnostics", "nuc3d_block_get_diag",
     "nuc3d_block_set_nodes", "nuc3d_block_get_metrics", "nuc3d_sensor_record",
     "nuc3d_sensor_loss_grad", "nuc3d_sensor_adam", "nuc3d_set_sensor", "nuc3d_set_tiles",
-    "nuc3d_get_tiles", "nuc3d_autotune", "nuc3d_get_energy_resets",
+    "nuc3d_get_tiles", "nuc3d_autotune", "nuc3d_get_energy_resets", "nuc3d_set_pipeline",
+    "nuc3d_get_pipeline", "nuc3d_rhs_stage", "nuc3d_rk_stage", "nuc3d_get_residual",
 )
 
 
@@ -112,6 +113,11 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_set_time.argtypes = [P, D]
     lib.nuc3d_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_uint)]
     lib.nuc3d_get_energy_resets.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.nuc3d_set_pipeline.argtypes = [P, I]
+    lib.nuc3d_get_pipeline.argtypes = [P, ctypes.POINTER(I)]
+    lib.nuc3d_rhs_stage.argtypes = [P, I, PD]
+    lib.nuc3d_rk_stage.argtypes = [P, I, D]
+    lib.nuc3d_get_residual.argtypes = [P, PD]
     lib.nuc3d_set_stream.argtypes = [P, P]
     lib.nuc3d_use_graph.argtypes = [P, I]
     lib.nuc3d_block_get_prim.argtypes = [P, I, PD]
@@ -332,6 +338,32 @@ class Solver:
         s = ctypes.c_uint()
         _check(self.lib.nuc3d_get_status(self._ctx, ctypes.byref(s)))
         return s.value
+
+    def rhs_stage(self, stage: int) -> float:
+        """RHS of every block at the state of RK stage `stage`; returns dt_local."""
+        dt = ctypes.c_double()
+        _check(self.lib.nuc3d_rhs_stage(self._ctx, int(stage), ctypes.byref(dt)))
+        return dt.value
+
+    def rk_stage(self, stage: int, dt: float) -> None:
+        """TVD-RK3 stage `stage` from the last rhs_stage(stage), step size dt."""
+        _check(self.lib.nuc3d_rk_stage(self._ctx, int(stage), float(dt)))
+
+    def residual(self) -> float:
+        """The residual of the last step (PDEData3d::setRES), max over blocks."""
+        r = ctypes.c_double()
+        _check(self.lib.nuc3d_get_residual(self._ctx, ctypes.byref(r)))
+        return r.value
+
+    def set_pipeline(self, on: bool) -> None:
+        """Persistent TMA-fed sweeps on (default) or off; results are identical."""
+        _check(self.lib.nuc3d_set_pipeline(self._ctx, 1 if on else 0))
+
+    def pipeline(self) -> bool:
+        """Whether the sweeps run pipelined (Euler, even nx, switched on)."""
+        v = ctypes.c_int()
+        _check(self.lib.nuc3d_get_pipeline(self._ctx, ctypes.byref(v)))
+        return bool(v.value)
 
     def energy_resets(self) -> int:
         """Cells whose energy con2prim reset, once per cell and right-hand side, since the

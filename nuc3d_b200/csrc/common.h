@@ -8,6 +8,7 @@
 // materialised: each sweep kernel walks its own axis through strides.
 #pragma once
 #include <stdint.h>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace nuc3d {
@@ -28,6 +29,7 @@ enum StatusBits : unsigned {
   ST_ENERGY_RESET = 2u,    // internal energy < 0, E reset (src/physicsModel.cpp:324-332)
   ST_NONFINITE = 4u,       // a non-finite value was produced by the RK update
   ST_BAD_LAUNCH = 8u,      // a kernel found an inconsistent descriptor and skipped work
+  ST_PIPE_TIMEOUT = 16u,   // a pipelined sweep's wait for its copies gave up (results invalid)
 };
 
 // Reference bufferSize per scheme (src/fieldOperator.cpp:127-283).
@@ -61,6 +63,8 @@ struct BlockDev {
   long long goff[6];     // -1 for neighbour faces
   double *fh;            // compact schemes: face fluxes [sys][line][face] of one direction
   double *rows;          // compact schemes: tridiagonal rows [row][4][sys*lines + line]
+  double *dres;          // reference-order build: u - u_n of the last RK stage (5*N), summed
+                         // in the reference's order for the residual; null otherwise
   FaceDev face[6];
   // Per direction d, ceil(2^40 / k) for k = tile chunks per line and k = line groups:
   // the sweep kernels divide tile indices by multiply-and-shift (set_tile_divisors).
@@ -73,6 +77,24 @@ struct BlockDev {
 constexpr int kTileShapes = 3;
 __host__ __device__ constexpr int tile_w(int s) { return s == 1 ? 8 : (s == 2 ? 2 : 4); }
 __host__ __device__ constexpr int tile_l(int s) { return s == 1 ? 32 : (s == 2 ? 128 : 64); }
+
+// Boxes of the pipelined sweep's tensor-map loads (pipe_sweep_kernel), for direction d, a
+// tile of tw lines x tl cells and a scheme reaching r cells: the halo box covers line
+// positions c0-r .. c0+tl+r-1 of the tile's lanes (xi: from c0 - ra, ra = r rounded up to
+// even, and x extent rounded up to even, so that the box starts and spans whole 16-byte
+// units); the own box covers the tile's cells.  ext[0..2] = x, y, z extents.
+__host__ __device__ constexpr int pipe_ra(int r) { return (r + 1) & ~1; }
+__host__ __device__ inline void pipe_box(int d, int tw, int tl, int r, bool halo, int ext[3]) {
+  const int len = halo ? (d == 0 ? ((tl + r + pipe_ra(r) + 1) & ~1) : tl + 2 * r) : tl;
+  ext[0] = d == 0 ? len : tw;
+  ext[1] = d == 0 ? tw : (d == 1 ? len : 1);
+  ext[2] = d == 2 ? len : 1;
+}
+// Cells a scheme's reconstruction reaches past a face (the sweep's split halo).
+__host__ __device__ constexpr int scheme_halo(int s) {
+  return (s == SCH_WENO7JS || s == SCH_HCCS || s == SCH_HCCS77) ? 4
+         : s == SCH_WENO3JS ? 2 : s == SCH_UPWIND1 ? 1 : 3;
+}
 
 // Fills BlockDev::tdiv from n[] and the directions' tile shapes: the two radices of the
 // tile index decode (decode_tile), chunks and line groups for xi and eta, line groups and
@@ -125,6 +147,8 @@ struct SolverParams {
   double gamma, mach, reynolds, prandtl, t_ref, t_inf, t_wall, cfl;
   const SensorDev *sensor;  // hybrid WENO-Z: the face sensor, or null (plain WENO-Z)
   float sensor_threshold;   // logit below which a face takes the linear weights
+  double *res_part;         // throughput build: per-tile sums of (u - u_n)^2 of the step's
+                            // last stage, for the residual (Launch::d_res_part)
 };
 
 // Per-launch work list: tiles of every block, laid end to end.
@@ -137,6 +161,8 @@ struct TileMap {
 // Device-resident scalars of the time loop.
 struct StepState {
   unsigned long long max_eig_bits;  // max over blocks and directions of |U|+c|grad xi| (bits of a double >= 0)
+  unsigned long long res_bits;      // the step's residual (PDEData3d::setRES, src/PDEData3d.cpp:
+                                    // 90-122): max over blocks, bits of a double >= 0
   double dt;                        // cfl / max_eig, fixed at stage 0 of each step
   double time;                      // accumulated time
   unsigned status;                  // StatusBits
@@ -158,6 +184,13 @@ struct Launch {
   int bc_tiles;            // CTAs of the BC ghost pass (0: no physical faces)
   cudaStream_t stream;
   int shape[3];            // sweep tile shape per direction (tile_w / tile_l)
+  // pipelined sweeps (pipe_sweep_kernel): tensor maps [block][dir][PM_COUNT] in device
+  // memory and the persistent grid (CTAs); null / 0: the one-tile-per-CTA sweeps
+  const CUtensorMap *d_maps;
+  int pipe_grid;
+  // each block's residual root of the previous step (the reference's static res_last);
+  // null: no residual (nuc3d_rhs_noalloc)
+  double *d_res_last;
 };
 
 // Diagnostics workspace of one block (postproc::solveQ, src/postproc.cpp:743-848):
@@ -183,7 +216,13 @@ void set_error_message(const char *msg);
 // run_diag(): the solveQ diagnostics of state q[0] of every block into dd[b] and the
 // per-block totals sums[2b] (enstrophy), sums[2b+1] (kinetic energy); parts holds
 // 2 * kDiagParts doubles per block of scratch.
+// run_rk_stage(): the TVD-RK3 stage update alone (rk_stage_kernel), from the RHS array, dt
+// given; at stage 2 also time += dt and the residual.
+// run_residual(): the residual of the step just finished (after stage 2); cells: 1 when the
+// partial sums are per cell tile (rk_stage_kernel), 0 per zeta-sweep tile.
 namespace exact {
+cudaError_t run_rk_stage(const Launch &L, int stage, double dt);
+cudaError_t run_residual(const Launch &L, bool cells);
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
 cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
@@ -196,6 +235,8 @@ cudaError_t configure();
 int tile_count(int dir, const int n[3], int shape);
 }
 namespace fast {
+cudaError_t run_rk_stage(const Launch &L, int stage, double dt);
+cudaError_t run_residual(const Launch &L, bool cells);
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
 cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,

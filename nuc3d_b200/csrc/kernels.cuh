@@ -395,7 +395,41 @@ __device__ __forceinline__ double diff_at(int c, int L, int ts, bool physL, bool
   return cd6(V(c - 3), V(c - 2), V(c - 1), V(c + 1), V(c + 2), V(c + 3));
 }
 
-enum SweepFlags : int { SW_EIG = 1, SW_RK = 2, SW_NS = 4, SW_STORE_DVIS = 8 };
+enum SweepFlags : int { SW_EIG = 1, SW_RK = 2, SW_NS = 4, SW_STORE_DVIS = 8, SW_RES = 16 };
+
+// The residual's share of one value of the last RK stage (PDEData3d::setRES,
+// src/PDEData3d.cpp:90-122): the reference-order build keeps d = u - u_n per value for the
+// residual kernel's sum in the reference's order; the throughput build adds d^2 to the
+// thread's sum, which the CTA reduces per tile.
+__device__ __forceinline__ void res_value(const BlockDev &B, int v, long long idx, double x,
+                                          double un, double &acc) {
+  const double d = x - un;
+#if NUC3D_FAST
+  (void)B; (void)v; (void)idx;
+  acc = fma(d, d, acc);
+#else
+  (void)acc;
+  B.dres[v * B.N + idx] = d;
+#endif
+}
+
+// Sum of acc over the CTA's first nthreads threads (warp shuffles, then the warp sums in
+// order): thread 0 writes it to *out.  Every one of those threads calls it; sync is their
+// barrier.
+template <class Sync>
+__device__ __forceinline__ void cta_sum_to(double acc, double *sRed, int nthreads, double *out,
+                                           Sync sync) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) sRed[threadIdx.x >> 5] = acc;
+  sync();
+  if (threadIdx.x == 0) {
+    double t = sRed[0];
+    for (int i = 1; i < nthreads / 32; ++i) t += sRed[i];
+    *out = t;
+  }
+  sync();
+}
 
 // TVD-RK3 stage update of one value (src/TVD-RK3.cpp:57-136, coefficients src/TVD-RK3.h:9-12):
 // u_i is the stage state, u_n the state saved at stage 0, R the right-hand side.
@@ -420,10 +454,10 @@ struct TileCtx {
 
 template <int DIR, int SHP = 0>
 __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ blocks, const TileMap &tm,
-                                               const SolverParams &P) {
+                                               const SolverParams &P, int t) {
   constexpr int TW = Tile<SHP>::TW, TL = Tile<SHP>::TL;
   TileCtx T;
-  T.t = blockIdx.x;
+  T.t = t;
   T.b = find_block(tm, T.t);
   T.B = &blocks[T.b];
   for (int d = 0; d < 3; ++d) T.n[d] = T.B->n[d];
@@ -456,6 +490,12 @@ __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ bloc
   T.physL = T.B->face[2 * DIR].type < 0;
   T.physR = T.B->face[2 * DIR + 1].type < 0;
   return T;
+}
+// The tile of this CTA (one tile per CTA).
+template <int DIR, int SHP = 0>
+__device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ blocks, const TileMap &tm,
+                                               const SolverParams &P) {
+  return decode_tile<DIR, SHP>(blocks, tm, P, (int)blockIdx.x);
 }
 
 // Shared-memory row strides of a sweep tile.
@@ -590,7 +630,7 @@ __device__ __forceinline__ void phase_vis(const BlockDev *__restrict__ blocks, c
 template <int DIR, int SCH, int SHP = 0>
 __device__ __forceinline__ void phase_cells(const TileCtx &T, const SolverParams &P, StepState *S,
                                             int stage, int flags, const double *sH, const double *sV,
-                                            const double *sQ, unsigned &st,
+                                            const double *sQ, unsigned &st, double *sRed,
                                             const double *sR = nullptr) {
   using M = TileSmem<DIR, SCH, SHP>;
   constexpr int TW = M::TW, TL = M::TL, SV = M::SV, SH = M::SH, SQ = M::SQ;
@@ -611,6 +651,7 @@ __device__ __forceinline__ void phase_cells(const TileCtx &T, const SolverParams
     }
     if (stage == 2 && T.t == 0 && threadIdx.x == 0) S->time = S->time + dt;
   }
+  double racc = 0.0;  // the residual's sum of (u - u_n)^2 (SW_RES)
   for (int e = threadIdx.x; e < TW * TL; e += kThreads) {
     int c, w;
     if (DIR == 0) { c = e % TL; w = e / TL; } else { w = e % TW; c = e / TW; }
@@ -680,6 +721,7 @@ __device__ __forceinline__ void phase_cells(const TileCtx &T, const SolverParams
           const double x = rk3_update(stage, r[v], ui, un[v], dt);
           if (!isfinite(x)) st |= ST_NONFINITE;
           qo[v * N + idx] = x;
+          if (flags & SW_RES) res_value(B, v, idx, x, un[v], racc);
         }
       } else {
 #pragma unroll
@@ -687,6 +729,11 @@ __device__ __forceinline__ void phase_cells(const TileCtx &T, const SolverParams
       }
     }
   }
+#if NUC3D_FAST
+  if (flags & SW_RES) cta_sum_to(racc, sRed, kThreads, P.res_part + T.t, [] { __syncthreads(); });
+#else
+  (void)sRed;
+#endif
 }
 
 __device__ __forceinline__ void reduce_eig(double emax, double *sRed, StepState *S) {
@@ -705,6 +752,7 @@ __device__ __forceinline__ void reduce_eig(double emax, double *sRed, StepState 
 }
 
 #include "sensor.cuh"
+#include "sweep_pipe.cuh"
 
 // Explicit-scheme sweep: phases split -> faces -> cells in one CTA.  HYB: the hybrid
 // WENO-Z face loop of the throughput build (P.sensor set).
@@ -885,7 +933,7 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
   }
   __syncthreads();
   if (sR) cp_async_wait_all();
-  phase_cells<DIR, SCH, SHP>(T, P, S, stage, flags, sH, sV, sQ, st, sR);
+  phase_cells<DIR, SCH, SHP>(T, P, S, stage, flags, sH, sV, sQ, st, sRed, sR);
   if (eig) reduce_eig(emax, sRed, S);
   if (st) atomicOr(&S->status, st);
   if (nres) atomicAdd(&S->reset_cells, (unsigned long long)nres);
@@ -1026,6 +1074,7 @@ compact_finish_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverPar
   double *sV = sH + 5 * TW * SH;
   const bool ns = (flags & SW_NS) != 0;
   double *sQ = sV + (ns ? 4 * TW * SV : 0);
+  __shared__ double sRed[kThreads / 32];
   const TileCtx T = decode_tile<DIR>(blocks, tm, P);
   const BlockDev &B = *T.B;
   unsigned st = 0;
@@ -1060,7 +1109,7 @@ compact_finish_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverPar
     }
   }
   __syncthreads();
-  phase_cells<DIR, SCH>(T, P, S, stage, flags, sH, sV, sQ, st);
+  phase_cells<DIR, SCH>(T, P, S, stage, flags, sH, sV, sQ, st, sRed);
   if (st) atomicOr(&S->status, st);
 }
 
@@ -1105,6 +1154,111 @@ bc_ghost_kernel(const BlockDev *__restrict__ blocks, const FaceJobs *__restrict_
 // Navier-Stokes: primitives, then gradients and viscous fluxes per cell.
 // ---------------------------------------------------------------------------------
 constexpr int kCellTile = 256;
+constexpr int kDiagChunk = 2048;  // values a reference-order sum stages at a time
+
+// ---------------------------------------------------------------------------------
+// The TVD-RK3 stage alone (tvdrk3rd::integrationAll, src/TVD-RK3.cpp:16-137), one thread
+// per cell, from the right-hand side in B.rhs: q[(stage+1) mod 3] from u_i = q[stage] and
+// u_n = q[0], each with con2prim's energy reset applied (src/physicsModel.cpp:324-332), as
+// the reference's Q_work and Q_Euler hold them.  The fused path applies the same update in
+// the zeta sweep; this kernel serves nuc3d_rk_stage.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kCellTile)
+rk_stage_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
+                int stage, double dt, int flags) {
+  __shared__ double sRed[kCellTile / 32];
+  const int b = find_block(tm, blockIdx.x);
+  const BlockDev &B = blocks[b];
+  const long long idx = (long long)(blockIdx.x - tm.tile_start[b]) * kCellTile + threadIdx.x;
+  const long long N = B.N;
+  unsigned st = 0;
+  double racc = 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (stage == 0) S->dt = dt;
+    if (stage == 2) S->time = S->time + dt;
+  }
+  if (idx < N) {
+    const double jac = __ldg(B.jac + idx);
+    double ui[5], un[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    load_q(B.q[stage], N, idx, ui);
+    CellPrim s;
+    con2prim(ui, jac, P.gamma, P.mach, s, st);
+    ui[4] = s.q4;
+    if (stage != 0) {
+      load_q(B.q[0], N, idx, un);
+      CellPrim sn;
+      unsigned stn = 0;
+      con2prim(un, jac, P.gamma, P.mach, sn, stn);
+      un[4] = sn.q4;
+    }
+    double *__restrict__ qo = B.q[(stage + 1) % 3];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double x = rk3_update(stage, B.rhs[v * N + idx], ui[v], un[v], dt);
+      if (!isfinite(x)) st |= ST_NONFINITE;
+      qo[v * N + idx] = x;
+      if (flags & SW_RES) res_value(B, v, idx, x, un[v], racc);
+    }
+  }
+#if NUC3D_FAST
+  if (flags & SW_RES) cta_sum_to(racc, sRed, kCellTile, P.res_part + blockIdx.x, [] { __syncthreads(); });
+#endif
+  st &= ST_NONFINITE | ST_NEG_PRESSURE;  // the reset was reported by the right-hand side
+  if (st) atomicOr(&S->status, st);
+}
+
+// The step's residual from its last stage (PDEData3d::setRES, src/PDEData3d.cpp:90-122):
+// per block res = |sqrt(sum (u - u_n)^2 / (5 N)) - res_last| / dt^2, res_last = that root
+// (the reference keeps it in a function-static, one per rank, i.e. per block here), and
+// the maximum over blocks (MPI_Allreduce MAX, :121) into S->res_bits.
+__device__ __forceinline__ void residual_finish(const BlockDev &B, int b, double sum,
+                                                double *__restrict__ res_last, StepState *S) {
+  const double cnt = (double)((unsigned long long)B.N * 5ull);
+  const double r = sqrt(sum / cnt);
+  const double dt = S->dt;
+  const double res = fabs(r - res_last[b]) / (dt * dt);
+  res_last[b] = r;
+  atomicMax(&S->res_bits, (unsigned long long)__double_as_longlong(res));
+}
+
+// Reference order: one CTA per block stages 2048 values of u - u_n at a time and thread 0
+// adds their squares one by one, component by component, in cell order, as the
+// reference's loops over Q_work do (src/PDEData3d.cpp:103-116).
+__global__ void __launch_bounds__(256)
+residual_seq_kernel(const BlockDev *__restrict__ blocks, double *__restrict__ res_last, StepState *S) {
+  __shared__ double sd[kDiagChunk];
+  const int b = blockIdx.x;
+  const BlockDev &B = blocks[b];
+  const long long n = 5 * B.N;
+  double sum = 0.0;
+  for (long long c0 = 0; c0 < n; c0 += kDiagChunk) {
+    const int m = (int)min((long long)kDiagChunk, n - c0);
+    for (int t = threadIdx.x; t < m; t += blockDim.x) sd[t] = B.dres[c0 + t];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int t = 0; t < m; ++t) sum = sum + sd[t] * sd[t];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) residual_finish(B, b, sum, res_last, S);
+}
+
+// Throughput order: one CTA per block adds the block's per-tile sums (threads strided, then
+// a fixed tree).
+__global__ void __launch_bounds__(256)
+residual_part_kernel(const BlockDev *__restrict__ blocks, TileMap tm, const double *__restrict__ part,
+                     double *__restrict__ res_last, StepState *S) {
+  __shared__ double sr[256];
+  const int b = blockIdx.x;
+  double acc = 0.0;
+  for (int t = tm.tile_start[b] + threadIdx.x; t < tm.tile_start[b + 1]; t += blockDim.x) acc += part[t];
+  sr[threadIdx.x] = acc;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) sr[threadIdx.x] += sr[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) residual_finish(blocks[b], b, sr[0], res_last, S);
+}
 
 __global__ void __launch_bounds__(kCellTile)
 prim_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S, int stage) {
@@ -1386,7 +1540,6 @@ diag_kernel(const BlockDev *__restrict__ blocks, const DiagDev *__restrict__ dd,
 // Reference-order totals: one CTA per block stages 2048-cell chunks of both terms in
 // shared memory and thread 0 adds them one by one in cell order, as the reference's
 // k-j-i loop does.  Bitwise equal to the reference; about 2 ns per cell.
-constexpr int kDiagChunk = 2048;
 __global__ void __launch_bounds__(256)
 diag_sum_seq_kernel(const BlockDev *__restrict__ blocks, const DiagDev *__restrict__ dd,
                     double *__restrict__ sums) {
@@ -1562,6 +1715,13 @@ inline cudaError_t launch_sweep_s(const Launch &L, int stage, int flags) {
     }
   }
 #endif
+  if (L.d_maps && L.pipe_grid > 0 && !ns) {
+    // persistent sweep fed by tensor-map loads (sweep_pipe.cuh)
+    const int grid = ntiles < L.pipe_grid ? ntiles : L.pipe_grid;
+    pipe_sweep_kernel<DIR, SCH, SHP><<<grid, kPipeThreads, PipeSmem<DIR, SCH, SHP>::TOTAL, L.stream>>>(
+        L.d_blocks, L.d_maps, L.tm_dir[DIR], L.P, L.d_state, stage, flags);
+    return cudaGetLastError();
+  }
   const size_t smem = sweep_smem_bytes<DIR, SCH, SHP>(ns) + rhs_stage_bytes<DIR>(ns);
   sweep_kernel<DIR, SCH, false, SHP><<<ntiles, kThreads, smem, L.stream>>>(L.d_blocks, L.tm_dir[DIR], L.P,
                                                                L.d_state, stage, flags);
@@ -1626,6 +1786,8 @@ inline cudaError_t launch_sweep(const Launch &L, int stage, int flags) {
   }
 }
 
+cudaError_t run_residual(const Launch &L, bool cells);
+
 // One right-hand-side evaluation at stage `stage`; with rk, also the stage update.
 inline cudaError_t launch_stage(const Launch &L, int stage, bool rk, bool eig) {
   cudaError_t e;
@@ -1642,10 +1804,37 @@ inline cudaError_t launch_stage(const Launch &L, int stage, bool rk, bool eig) {
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   const int nsf = ns ? SW_NS : 0;
+  const bool res = rk && stage == 2 && L.d_res_last;  // the step's residual at its last stage
   if ((e = launch_sweep<0>(L, stage, nsf | (eig ? SW_EIG : 0))) != cudaSuccess) return e;
   if ((e = launch_sweep<1>(L, stage, nsf)) != cudaSuccess) return e;
-  if ((e = launch_sweep<2>(L, stage, nsf | (rk ? SW_RK : 0))) != cudaSuccess) return e;
+  if ((e = launch_sweep<2>(L, stage, nsf | (rk ? SW_RK : 0) | (res ? SW_RES : 0))) != cudaSuccess)
+    return e;
+  if (res) return run_residual(L, false);
   return cudaSuccess;
+}
+
+cudaError_t run_residual(const Launch &L, bool cells) {
+  const int nb = L.tm_cells.nblocks;
+  cudaError_t e = cudaMemsetAsync(&L.d_state->res_bits, 0, sizeof(unsigned long long), L.stream);
+  if (e != cudaSuccess) return e;
+#if NUC3D_FAST
+  residual_part_kernel<<<nb, 256, 0, L.stream>>>(L.d_blocks, cells ? L.tm_cells : L.tm_dir[2],
+                                                 L.P.res_part, L.d_res_last, L.d_state);
+#else
+  (void)cells;
+  residual_seq_kernel<<<nb, 256, 0, L.stream>>>(L.d_blocks, L.d_res_last, L.d_state);
+#endif
+  return cudaGetLastError();
+}
+
+cudaError_t run_rk_stage(const Launch &L, int stage, double dt) {
+  const bool res = stage == 2 && L.d_res_last;
+  const int nt = L.tm_cells.tile_start[L.tm_cells.nblocks];
+  rk_stage_kernel<<<nt, kCellTile, 0, L.stream>>>(L.d_blocks, L.tm_cells, L.P, L.d_state, stage, dt,
+                                                  res ? SW_RES : 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !res) return e;
+  return run_residual(L, true);
 }
 
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig) {
@@ -1737,6 +1926,10 @@ inline cudaError_t configure_s() {
 #endif
   const size_t euler = sweep_smem_bytes<DIR, SCH, SHP>(false) + rhs_stage_bytes<DIR>(false);
   const size_t ns = sweep_smem_bytes<DIR, SCH, SHP>(true) + rhs_stage_bytes<DIR>(true);
+  const cudaError_t e = cudaFuncSetAttribute(pipe_sweep_kernel<DIR, SCH, SHP>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)PipeSmem<DIR, SCH, SHP>::TOTAL);
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(sweep_kernel<DIR, SCH, false, SHP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(euler > ns ? euler : ns));
 }

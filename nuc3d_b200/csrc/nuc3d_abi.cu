@@ -16,10 +16,17 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "common.h"
 #include "nuc3d_gpu.h"
 
 using namespace nuc3d;
+
+// Tensor maps of the pipelined sweeps: [block][dir][kind] (the kinds of sweep_pipe.cuh).
+namespace nuc3d {
+enum : int { kMapQ0 = 0, kMapJac = 3, kMapMet = 4, kMapMetO = 5, kMapRhs = 6, kMapQn = 7, kMapKinds = 8 };
+}
 
 namespace {
 
@@ -50,6 +57,7 @@ struct HostBlock {
   double *rhs = nullptr, *jac = nullptr, *met = nullptr, *dxyz = nullptr;
   double *prim = nullptr, *vis = nullptr, *dvis = nullptr, *ghost = nullptr;
   double *fh = nullptr, *rows = nullptr;  // compact schemes
+  double *dres = nullptr;                 // reference-order build: u - u_n for the residual
   long long goff[6] = {-1, -1, -1, -1, -1, -1};
   bool metrics = false;
 };
@@ -107,6 +115,11 @@ struct nuc3d_ctx {
   double *d_dsums = nullptr, *d_dparts = nullptr;
   SensorDev *d_sensor = nullptr;  // hybrid WENO-Z face sensor (nuc3d_set_sensor)
   std::vector<BlockDev> hdesc;  // host copy of the block descriptors (tile divisors change)
+  // pipelined sweeps: tensor maps of every block and direction (built by build_maps)
+  bool use_pipe = true;
+  CUtensorMap *d_maps = nullptr;
+  // the residual of each step: per-tile partial sums, each block's previous residual root
+  double *d_res_part = nullptr, *d_res_last = nullptr;
   // nuc3d_solve_host: copy streams and events, created by its first call
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t ev_start = nullptr, ev_h2d = nullptr, ev_step = nullptr, ev_end = nullptr;
@@ -205,9 +218,12 @@ int nuc3d_destroy(nuc3d_ctx *c) {
   c->drop_graph();
   for (auto &b : c->blocks) {
     for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.dxyz, b.prim, b.vis, b.dvis,
-                   b.ghost, b.fh, b.rows})
+                   b.ghost, b.fh, b.rows, b.dres})
       if (p) cudaFree(p);
   }
+  for (auto p : {c->d_res_part, c->d_res_last})
+    if (p) cudaFree(p);
+  if (c->d_maps) cudaFree(c->d_maps);
   for (auto &d : c->diag)
     for (auto p : {d.prim, d.fields, d.dens})
       if (p) cudaFree(p);
@@ -312,11 +328,12 @@ int nuc3d_block_add(nuc3d_ctx *c, int nx, int ny, int nz, const int bc_type[6], 
     if (fh_n > 0 && e == cudaSuccess) e = cudaMalloc(&b.fh, fh_n * sizeof(double));
     if (rows_n > 0 && e == cudaSuccess) e = cudaMalloc(&b.rows, rows_n * sizeof(double));
   }
+  if (c->exact && e == cudaSuccess) e = cudaMalloc(&b.dres, 5 * nb);
   for (int s = 0; s < 3 && e == cudaSuccess; ++s) e = cudaMemset(b.q[s], 0, 5 * nb);
   if (e == cudaSuccess) e = cudaMemset(b.rhs, 0, 5 * nb);
   if (e != cudaSuccess) {
     for (auto p : {b.q[0], b.q[1], b.q[2], b.rhs, b.jac, b.met, b.prim, b.vis, b.dvis, b.ghost,
-                   b.fh, b.rows})
+                   b.fh, b.rows, b.dres})
       if (p) cudaFree(p);
     return fail(NUC3D_ECUDA, "block allocation (%lld cells): %s", b.N, cudaGetErrorString(e));
   }
@@ -402,6 +419,93 @@ int nuc3d_block_get_metrics(nuc3d_ctx *c, int bi, double *jac, double *xi_xyz, d
   return NUC3D_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled g_encode = nullptr;
+std::once_flag g_encode_once;
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+  std::call_once(g_encode_once, [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+  });
+  return g_encode;
+}
+
+bool explicit_scheme(int s) {
+  return s == SCH_WENO5JS || s == SCH_WENO5Z || s == SCH_WENO7JS || s == SCH_WENO3JS ||
+         s == SCH_UPWIND1;
+}
+
+// A 3D (ncomp = 0) or 4D tiled map over an [ncomp][nz][ny][nx] array of doubles.
+bool encode_map(CUtensorMap *m, const void *base, const int n[3], int ncomp, const int box[3],
+                int box_comp) {
+  const cuuint64_t dims[4] = {(cuuint64_t)n[0], (cuuint64_t)n[1], (cuuint64_t)n[2], (cuuint64_t)ncomp};
+  const cuuint64_t nx8 = (cuuint64_t)n[0] * 8;
+  const cuuint64_t strides[3] = {nx8, nx8 * n[1], nx8 * n[1] * n[2]};
+  const cuuint32_t bdim[4] = {(cuuint32_t)box[0], (cuuint32_t)box[1], (cuuint32_t)box[2],
+                              (cuuint32_t)box_comp};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = tensor_map_encoder()(
+      m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, ncomp ? 4 : 3, const_cast<void *>(base), dims, strides,
+      bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// Tensor maps of the pipelined sweeps for the current tile shapes, or pipelining off
+// (L.d_maps = null) where it does not apply: Navier-Stokes (its viscous tiles are not
+// staged), a block with an odd nx (TMA needs 16-byte row strides), or switched off.
+int build_maps(nuc3d_ctx *c) {
+  Launch &L = c->L;
+  L.d_maps = nullptr;
+  L.pipe_grid = 0;
+  bool ok = c->use_pipe && c->P.model == MODEL_EULER;
+  for (const HostBlock &b : c->blocks) ok = ok && b.n[0] % 2 == 0;
+  if (!ok) return NUC3D_OK;
+  if (!tensor_map_encoder()) return NUC3D_OK;  // no TMA encoder in this driver: plain sweeps
+  const int nbk = (int)c->blocks.size();
+  std::vector<CUtensorMap> h((size_t)nbk * 3 * kMapKinds);
+  std::memset(h.data(), 0, h.size() * sizeof(CUtensorMap));
+  for (int bi = 0; bi < nbk; ++bi) {
+    const HostBlock &b = c->blocks[bi];
+    for (int d = 0; d < 3; ++d) {
+      if (!explicit_scheme(c->P.scheme[d])) continue;
+      CUtensorMap *m = &h[((size_t)bi * 3 + d) * kMapKinds];
+      const int tw = tile_w(L.shape[d]), tl = tile_l(L.shape[d]), r = scheme_halo(c->P.scheme[d]);
+      int hb[3], ob[3];
+      pipe_box(d, tw, tl, r, true, hb);
+      pipe_box(d, tw, tl, r, false, ob);
+      bool e = true;
+      for (int s = 0; s < 3; ++s) e = e && encode_map(&m[kMapQ0 + s], b.q[s], b.n, 5, hb, 5);
+      e = e && encode_map(&m[kMapJac], b.jac, b.n, 0, hb, 0);
+      e = e && encode_map(&m[kMapMet], b.met, b.n, 9, hb, 3);
+      e = e && encode_map(&m[kMapMetO], b.met, b.n, 9, ob, 6);
+      e = e && encode_map(&m[kMapRhs], b.rhs, b.n, 5, ob, 5);
+      e = e && encode_map(&m[kMapQn], b.q[0], b.n, 5, ob, 5);
+      if (!e) return fail(NUC3D_ECUDA, "block %d direction %d: tensor map encoding failed", bi, d);
+    }
+  }
+  cudaSetDevice(c->device);
+  if (!c->d_maps) CUDA_TRY(cudaMalloc(&c->d_maps, h.size() * sizeof(CUtensorMap)));
+  CUDA_TRY(cudaMemcpy(c->d_maps, h.data(), h.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  L.d_maps = c->d_maps;
+  L.pipe_grid = 2 * sms;  // two persistent CTAs per SM
+  return NUC3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int nuc3d_finalize(nuc3d_ctx *c) {
   if (!c) return fail(NUC3D_EINVAL, "null context");
   if (c->finalized) return fail(NUC3D_ESTATE, "already finalized");
@@ -455,6 +559,7 @@ int nuc3d_finalize(nuc3d_ctx *c) {
     d.ghost = b.ghost;
     d.fh = b.fh;
     d.rows = b.rows;
+    d.dres = b.dres;
     for (int f = 0; f < 6; ++f) d.goff[f] = b.goff[f];
     for (int f = 0; f < 6; ++f) {
       d.face[f].type = b.bc_type[f];
@@ -511,6 +616,21 @@ int nuc3d_finalize(nuc3d_ctx *c) {
   CUDA_TRY(cudaMalloc(&c->d_jobs, sizeof(FaceJobs)));
   CUDA_TRY(cudaMemcpy(c->d_jobs, &J, sizeof(FaceJobs), cudaMemcpyHostToDevice));
   L.d_jobs = c->d_jobs;
+  // residual workspace: one partial sum per zeta tile (any tile shape) or per cell tile
+  {
+    long long nt = L.tm_cells.tile_start[nbk];
+    for (int sh = 0; sh < kTileShapes; ++sh) {
+      long long z = 0;
+      for (int bi = 0; bi < nbk; ++bi) z += nuc3d::exact::tile_count(2, c->blocks[bi].n, sh);
+      nt = std::max(nt, z);
+    }
+    CUDA_TRY(cudaMalloc(&c->d_res_part, nt * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&c->d_res_last, nbk * sizeof(double)));
+    CUDA_TRY(cudaMemset(c->d_res_last, 0, nbk * sizeof(double)));
+    c->P.res_part = L.P.res_part = c->d_res_part;
+    L.d_res_last = c->d_res_last;
+  }
+  if (int r = build_maps(c)) return r;
   c->finalized = true;
   return NUC3D_OK;
 }
@@ -566,17 +686,23 @@ int nuc3d_block_get_vis(nuc3d_ctx *c, int bi, double *vis) {
 static int check_status(nuc3d_ctx *c) {
   StepState s;
   CUDA_TRY(cudaMemcpy(&s, c->d_state, sizeof(s), cudaMemcpyDeviceToHost));
+  if (s.status & ST_PIPE_TIMEOUT)
+    return fail(NUC3D_ECUDA, "kernel status 0x%x: a pipelined sweep's wait for its loads gave up",
+                s.status);
   if (s.status & (ST_NEG_PRESSURE | ST_NONFINITE | ST_BAD_LAUNCH))
     return fail(NUC3D_ENUMERIC, "kernel status 0x%x (negative pressure / non-finite state)", s.status);
   return NUC3D_OK;
 }
 
-int nuc3d_rhs(nuc3d_ctx *c, double *dt_local) {
+int nuc3d_rhs(nuc3d_ctx *c, double *dt_local) { return nuc3d_rhs_stage(c, 0, dt_local); }
+
+int nuc3d_rhs_stage(nuc3d_ctx *c, int stage, double *dt_local) {
   if (!c) return fail(NUC3D_EINVAL, "null context");
   if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  if (stage < 0 || stage > 2) return fail(NUC3D_EINVAL, "stage %d not in 0..2", stage);
   cudaSetDevice(c->device);
   CUDA_TRY(cudaMemsetAsync(&c->d_state->max_eig_bits, 0, sizeof(unsigned long long), c->stream));
-  CUDA_TRY(c->stage(0, false, true));
+  CUDA_TRY(c->stage(stage, false, true));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   StepState s;
   CUDA_TRY(cudaMemcpy(&s, c->d_state, sizeof(s), cudaMemcpyDeviceToHost));
@@ -586,6 +712,27 @@ int nuc3d_rhs(nuc3d_ctx *c, double *dt_local) {
     *dt_local = 1.0 / me;
   }
   return check_status(c);
+}
+
+int nuc3d_rk_stage(nuc3d_ctx *c, int stage, double dt) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  if (stage < 0 || stage > 2) return fail(NUC3D_EINVAL, "stage %d not in 0..2", stage);
+  if (!(dt > 0.0)) return fail(NUC3D_EINVAL, "dt must be > 0");
+  cudaSetDevice(c->device);
+  CUDA_TRY(c->exact ? nuc3d::exact::run_rk_stage(c->L, stage, dt)
+                    : nuc3d::fast::run_rk_stage(c->L, stage, dt));
+  return NUC3D_OK;
+}
+
+int nuc3d_get_residual(nuc3d_ctx *c, double *res) {
+  if (!c || !res) return fail(NUC3D_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  unsigned long long bits = 0;
+  CUDA_TRY(cudaMemcpy(&bits, &c->d_state->res_bits, sizeof(bits), cudaMemcpyDeviceToHost));
+  std::memcpy(res, &bits, sizeof(double));
+  return NUC3D_OK;
 }
 
 int nuc3d_step(nuc3d_ctx *c, int nsteps) {
@@ -698,7 +845,7 @@ static int apply_shapes(nuc3d_ctx *c, const int shape[3]) {
       c->L.tm_dir[d].tile_start[bi + 1] =
           c->L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, c->blocks[bi].n, shape[d]);
   c->drop_graph();
-  return NUC3D_OK;
+  return build_maps(c);
 }
 
 static bool compact_scheme(int s) { return s == SCH_CRWENO5 || s == SCH_HCCS || s == SCH_HCCS77; }
@@ -1017,7 +1164,23 @@ int nuc3d_kernels_per_step(nuc3d_ctx *c, int *kernels) {
   for (int d = 0; d < 3; ++d)
     per_stage += (L.P.scheme[d] == SCH_CRWENO5 || L.P.scheme[d] == SCH_HCCS ||
                   L.P.scheme[d] == SCH_HCCS77) ? 3 : 1;
-  *kernels = 3 * per_stage;
+  *kernels = 3 * per_stage + (L.d_res_last ? 1 : 0);  // + the residual after the last stage
+  return NUC3D_OK;
+}
+
+int nuc3d_set_pipeline(nuc3d_ctx *c, int on) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->use_pipe = on != 0;
+  c->drop_graph();
+  return build_maps(c);
+}
+
+int nuc3d_get_pipeline(nuc3d_ctx *c, int *on) {
+  if (!c || !on) return fail(NUC3D_EINVAL, "null argument");
+  *on = c->L.d_maps != nullptr ? 1 : 0;
   return NUC3D_OK;
 }
 
