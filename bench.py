@@ -54,6 +54,8 @@ FLOPS = {
     "weno5z": 74,          # src/weno5z.cpp:74-109
     "weno7js": 146,        # src/weno7js.cpp:84-136
     "combine": 1,          # per face and variable: src/euler3d.cpp:45-49
+    "cd6": 8,              # per cell and field: 3 differences, 3 products, 2 sums
+                           # (src/centraldifference6th.cpp:26-43)
     "difference": 1,       # per cell and variable: src/euler3d.cpp:163-169
     "rhs_add": 1,          # per cell and variable: src/euler3d.cpp:405,419
     "rk": 14.0 / 3.0,      # per cell and variable, mean of stages 4,5,5: src/TVD-RK3.cpp:57-136
@@ -68,13 +70,17 @@ SWEEP_BYTES = {0: 72 + 40, 1: 72 + 80, 2: 72 + 80}
 SWEEP_TRAFFIC = {0: 108.1, 1: 152.1, 2: 150.8}
 
 
-def sweep_flops_per_cell(d: int, scheme: str = "weno5z", riemann: str = "AUSM") -> float:
-    """Algorithmic flops per cell of one right-hand-side sweep along d (no RK update)."""
+def sweep_flops_per_cell(d: int, scheme: str = "weno5z", riemann: str = "AUSM",
+                         ns: bool = False) -> float:
+    """Algorithmic flops per cell of one right-hand-side sweep along d (no RK update); ns:
+    plus the direction's cd6 differences of the 4 viscous fluxes and their subtraction."""
     f = FLOPS[riemann] + 10 * FLOPS[scheme] + 5 * FLOPS["combine"] + 5 * FLOPS["difference"]
     if d == 0:
         f += FLOPS["con2prim"]
     else:
         f += 5 * FLOPS["rhs_add"]
+    if ns:
+        f += 4 * FLOPS["cd6"] + 4 * FLOPS["rhs_add"]
     return f
 
 
@@ -136,6 +142,16 @@ def host_cores() -> int:
         return len(os.sched_getaffinity(0))
     except Exception:
         return os.cpu_count() or 1
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
 
 
 def decompose(shape, nranks):
@@ -225,12 +241,13 @@ def reference_arm(args):
     value, nr, sample, secs = run_reference(shape, args.steps, args.warmup)
     line = {
         "impl": "reference", "metric": "Mcell-RK3-steps/s", "value": value,
+        "cpu_model": cpu_model(),
         "unit": "Mcell-RK3-steps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "cells": cells, "parallelism": f"{nr} MPI ranks on CPU"},
         "cpu_baseline": {"value": value, "unit": "Mcell-RK3-steps/s", "cores": nr,
-                         "kind": "reference", "sample": sample},
+                         "kind": "reference", "sample": sample, "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": "Mcell-RK3-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -384,6 +401,13 @@ def ours(args):
     # ---- roofline of the dominant kernel ----
     s.set_q(b, q0)
     per = {d: s.profile_sweep(d, reps=5) for d in range(3)}
+    pipelined = s.pipeline()
+    if pipelined:  # the same launches with one tile per CTA, for comparison
+        s.set_pipeline(False)
+        per_plain = {d: s.profile_sweep(d, reps=5) for d in range(3)}
+        s.set_pipeline(True)
+    else:
+        per_plain = None
     dom = max(per, key=per.get)
     flops = sweep_flops_per_cell(dom) * cells
     achieved = flops / (per[dom] * 1e-3) / 1e12
@@ -405,12 +429,22 @@ def ours(args):
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
-            v, nr, sample, _ = run_reference(SHAPE, 1, 1)
+            # block::solve timed over 10 steps after 2 warm-up steps
+            v, nr, sample, _ = run_reference(SHAPE, 10, 2)
             cpu = {"value": v, "unit": "Mcell-RK3-steps/s", "cores": nr, "kind": "reference",
-                   "sample": sample}
+                   "sample": sample, "cpu_model": cpu_model()}
         except Exception as e:  # the baseline is a report, never a reason to fail the bench
             cpu = {"value": None, "unit": "Mcell-RK3-steps/s", "cores": 0, "kind": "reference",
-                   "sample": f"unavailable: {e}".splitlines()[0][:200]}
+                   "sample": f"unavailable: {e}".splitlines()[0][:200], "cpu_model": cpu_model()}
+    # the batched multi-block Navier-Stokes workload (24 uneven blocks), on this GPU
+    launches = s.kernels_per_step() * args.steps
+    turb = None
+    if world == 1 and not args.no_turbulence:
+        s.close()
+        try:
+            turb = turbulence24(args, with_cpu=not args.no_cpu_baseline)
+        except Exception as e:  # reported, never a reason to fail the bench
+            turb = {"unavailable": f"{type(e).__name__}: {e}".splitlines()[0][:300]}
 
     line = {
         "metric": "Mcell-RK3-steps/s", "value": value, "unit": "Mcell-RK3-steps/s",
@@ -433,13 +467,15 @@ def ours(args):
                 "h2d_bytes_per_step": 5 * cells * 8, "d2h_bytes_per_step": 5 * cells * 8,
                 "steps": e2e_steps, "api": "nuc3d_solve_host (host Q in place, every step)",
                 "serial_copies_value": e2e_serial_value},
-        "gpu_launches": s.kernels_per_step() * args.steps,
+        "gpu_launches": launches,
         "roofline": {
             "bound": "fp64", "kernel": f"sweep_kernel<{dom}> ({'xi eta zeta'.split()[dom]})",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured live: libnuc3d_probe DFMA microbenchmark",
             "flops_per_cell": sweep_flops_per_cell(dom), "ms_per_launch": per[dom],
             "ms_per_launch_all": per,
+            "pipelined": pipelined,
+            "ms_per_launch_one_tile_per_cta": per_plain,
             "traffic": (SWEEP_TRAFFIC[dom] * cells if SWEEP_TRAFFIC[dom] else None),
             "traffic_unit": "bytes per launch",
             "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
@@ -448,12 +484,14 @@ def ours(args):
         },
         "cpu_baseline": cpu,
         "hybrid": hybrid,
+        "turbulence24": turb,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
-    s.close()
+    if turb is None:
+        s.close()
     return 0
 
 
@@ -462,10 +500,52 @@ TURB_WORKLOAD = ("decaying isotropic turbulence, 2pi periodic box in 24 uneven b
                  "WENO5-Z, AUSM, cd6, Mt 0.6, Re_lambda 100, TVD-RK3 CFL 0.5")
 
 
-def turbulence24(args):
+def turbulence24_reference(seed_parts=99, sizes=(16, 24, 32, 48), steps=3, warmup=1):
+    """The reference on the host cores for the 24-block workload: the same 2 x 3 x 4
+    periodic tensor-product partition, physics and schemes, block sizes drawn from `sizes`
+    (the full 40 M cells would need its mesh written and parsed as text, minutes of I/O),
+    one reference rank (process) per block."""
+    from oracle import refrun as R
+    from nuc3d_b200 import cases as C
+    from nuc3d_b200.metrics import metrics_from_nodes
+    parts = C.uneven_blocks(sizes=sizes, seed=seed_parts)
+    n = [sum(p) for p in parts]
+    x, y, z = R.box_nodes(*n, hi=(2.0 * math.pi,) * 3)
+    prim, re = C.isotropic_turbulence(tuple(n), seed=7)
+    types, ids = C.block_topology(parts)
+    off = [np.concatenate([[0], np.cumsum(p)]) for p in parts]
+    nodes, q0 = [], []
+    for c in range(len(parts[2])):
+        for b in range(len(parts[1])):
+            for a in range(len(parts[0])):
+                lo = (off[0][a], off[1][b], off[2][c])
+                hi = (off[0][a + 1], off[1][b + 1], off[2][c + 1])
+                nsl = tuple(slice(lo[d], hi[d] + 1) for d in (2, 1, 0))
+                csl = tuple(slice(lo[d], hi[d]) for d in (2, 1, 0))
+                xyz = tuple(arr[nsl] for arr in (x, y, z))
+                m = metrics_from_nodes(*xyz)
+                nodes.append(xyz)
+                q0.append(np.ascontiguousarray(C.prim_to_q(prim[(slice(None),) + csl], m["jac"], 1.4)))
+    topo = [[f"{types[r][f]} {ids[r][f]}" for f in range(6)] for r in range(len(nodes))]
+    case = R.Case(model="NavierStokes3d", riemann="AUSM", schemes=("weno5z",) * 3,
+                  params={"Reynolds": re, "Mach": 0.6, "Pt": 0.72, "Gamma": 1.4, "T_ref": 110.4,
+                          "T_inf": 288.0, "T_wall": 1.0},
+                  nodes=nodes, bc_topo=topo, q0=q0, start_step=1)
+    out = R.run(case, "time", steps, warmup, timeout=1800)[0]
+    rec = json.loads(out.strip().splitlines()[-1])
+    cells = int(np.prod(n))
+    value = cells * steps / rec["solve_seconds"] / 1e6
+    sample = (f"{steps} timed + {warmup} warm-up steps of the 24-block partition with block sizes "
+              f"from {list(sizes)} ({cells} cells), one reference rank (process) per block on "
+              f"{host_cores()} host cores")
+    return {"value": value, "unit": "Mcell-RK3-steps/s", "cores": min(len(nodes), host_cores()),
+            "kind": "reference", "sample": sample, "cpu_model": cpu_model()}
+
+
+def turbulence24(args, with_cpu=False):
     """The batched multi-block Navier-Stokes workload on one GPU: every block of the grid in
     one context (on-device ghost copies), one launch per sweep over all blocks, the step a
-    CUDA graph, tile shapes from nuc3d_autotune."""
+    CUDA graph, tile shapes from nuc3d_autotune.  Returns its bench line (a dict)."""
     import torch
     import nuc3d_b200 as nb
     from nuc3d_b200 import cases as C
@@ -525,6 +605,17 @@ def turbulence24(args):
     ev3.synchronize()
     e2e_ms = ev2.elapsed_time(ev3)
     per = [s.profile_sweep(d, reps=3) for d in range(3)]
+    dom = int(np.argmax(per))
+    flops = sweep_flops_per_cell(dom, ns=True) * cells
+    achieved = flops / (per[dom] * 1e-3) / 1e12
+    peak = nb.fp64_peak_tflops(0)
+    cpu = None
+    if with_cpu:
+        try:
+            cpu = turbulence24_reference()
+        except Exception as e:
+            cpu = {"value": None, "unit": "Mcell-RK3-steps/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}".splitlines()[0][:200]}
     line = {
         "metric": "Mcell-RK3-steps/s", "value": whole_job_rate(1, cells, args.steps, ms),
         "unit": "Mcell-RK3-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -539,11 +630,15 @@ def turbulence24(args):
                 "steps": e2e_steps, "api": "nuc3d_solve_host (24 host arrays in place, every step)"},
         "gpu_launches": s.kernels_per_step() * args.steps,
         "sweep_ms_per_launch": per,
-        "roofline": None, "cpu_baseline": None,
+        "roofline": {"bound": "fp64", "kernel": f"sweep_kernel<{dom}> ({'xi eta zeta'.split()[dom]}, NS)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": "measured live: libnuc3d_probe DFMA microbenchmark",
+                     "flops_per_cell": sweep_flops_per_cell(dom, ns=True),
+                     "ms_per_launch": per[dom], "traffic": None},
+        "cpu_baseline": cpu,
     }
-    print(json.dumps(line), flush=True)
     s.close()
-    return 0
+    return line
 
 
 def profile_case(args):
@@ -593,6 +688,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--exact", action="store_true", help="reference-order arithmetic")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-turbulence", action="store_true",
+                    help="leave out the 24-block Navier-Stokes line of the default run")
     ap.add_argument("--tiles", type=lambda x: tuple(int(v) for v in x.split(",")), default=None,
                     help="sweep tile shapes per direction, e.g. 2,0,0 (default: nuc3d_autotune)")
     ap.add_argument("--workload", default="sphere256", choices=["sphere256", "turbulence24"],
@@ -612,7 +709,8 @@ def main():
         if args.impl == "reference" or args.gpus > 1:
             print(json.dumps({"impl": args.impl, "unavailable": "turbulence24 runs our arm on one GPU only"}))
             return 0
-        return turbulence24(args)
+        print(json.dumps(turbulence24(args, with_cpu=not args.no_cpu_baseline)), flush=True)
+        return 0
     if args.impl == "reference":
         return reference_arm(args)
     return ours(args)
