@@ -37,19 +37,31 @@ def test_pipelined_sweeps_bitwise_reference(name):
     assert res == g.res[-1]
 
 
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["sphere_euler_weno5z_ausm_outlet", "mixed_euler_lf_outlet_symm",
                                   "sphere_reset_euler_weno5z_ausm", "mixed_low_order_ausmp"])
 @pytest.mark.parametrize("shape", [(0, 0, 0), (1, 1, 1), (2, 2, 2), (2, 0, 1)])
 @pytest.mark.parametrize("exact", [True, False])
 def test_pipelined_equals_plain(name, shape, exact):
+    """Reference-order build: identical bits.  Throughput build: the compiler contracts
+    multiply-adds into FMAs per kernel, so the two kernels agree to round-off (the parity
+    tests' relative max-norm 1e-11)."""
     g = G.load(name)
     a = _run(g, exact, True, shape)
     b = _run(g, exact, False, shape)
-    assert a[0] == b[0]
-    assert np.array_equal(a[1], b[1])
-    assert np.array_equal(a[2], b[2])
-    assert a[3] == b[3] and a[4] == b[4] and a[5] == b[5] and a[6] == b[6]
+    if exact:
+        assert a[0] == b[0]
+        assert np.array_equal(a[1], b[1])
+        assert np.array_equal(a[2], b[2])
+        assert a[3] == b[3] and a[4] == b[4] and a[5] == b[5] and a[6] == b[6]
+    else:
+        assert abs(a[0] - b[0]) <= 1e-11 * b[0]
+        assert _rel(a[1], b[1]) < 1e-11 and _rel(a[2], b[2]) < 1e-11
+        assert a[5] == b[5] and abs(a[6] - b[6]) <= 1e-9 * b[6]
 
 
 @pytest.mark.gpu

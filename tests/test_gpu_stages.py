@@ -44,7 +44,9 @@ def test_residual_two_ranks_is_the_maximum():
 def test_stage_by_stage_equals_step(name, exact):
     """rhs_stage(s) + rk_stage(s, dt) for s = 0, 1, 2 with dt = cfl * dt_local of stage 0,
     as PDEData3d::solve fixes it (src/PDEData3d.cpp:74-80), is nuc3d_step: the state, time,
-    dt and residual; the reference-order build also equals the reference's step."""
+    dt and residual; the reference-order build also equals the reference's step.  The
+    throughput build's residual sums per cell tile here and per sweep tile in the step, so
+    it agrees to round-off."""
     g = G.load(name)
     a = G.solver(g, exact=exact)
     b = G.solver(g, exact=exact)
@@ -59,7 +61,10 @@ def test_stage_by_stage_equals_step(name, exact):
         b.step(1)
         assert np.array_equal(a.get_q(0), b.get_q(0)), k
         assert a.time_dt() == b.time_dt()
-        assert a.residual() == b.residual()
+        if exact:
+            assert a.residual() == b.residual()
+        else:
+            assert abs(a.residual() - b.residual()) <= 1e-12 * b.residual()
         if exact and k == 0:
             assert np.array_equal(a.get_q(0), g.q1)
             assert a.residual() == g.res[0]

@@ -63,8 +63,15 @@ def test_noalloc_matches_allocating_rhs(name, exact):
         rc = _call(lib, cfg_c, g.cfg["shape"], G.bc_arrays(g), dev, rhs, dt, stream)
         assert rc == 0, lib.nuc3d_last_error().decode()
         got = rhs.cpu().numpy()
-        assert dt.value == dt_ref
-        assert np.array_equal(got, rhs_ref), float(np.nanmax(np.abs(got - rhs_ref)))
+        if exact:
+            assert dt.value == dt_ref
+            assert np.array_equal(got, rhs_ref), float(np.nanmax(np.abs(got - rhs_ref)))
+        else:
+            # the allocating path runs the pipelined sweeps, this one the one-tile-per-CTA
+            # sweeps; the throughput build contracts FMAs per kernel: round-off apart
+            assert abs(dt.value - dt_ref) <= 1e-11 * dt_ref
+            err = float(np.max(np.abs(got - rhs_ref)) / np.max(np.abs(rhs_ref)))
+            assert err < 1e-11, err
 
 
 def test_noalloc_rejects_what_it_cannot_do():
