@@ -236,8 +236,9 @@ int nuc3d_set_sensor(nuc3d_ctx *ctx, const float *params, float logit_threshold)
 int nuc3d_set_tiles(nuc3d_ctx *ctx, const int shape[3]);
 int nuc3d_get_tiles(nuc3d_ctx *ctx, int shape[3]);
 /* Time every shape of every explicit-scheme direction's right-hand-side sweep on the
-   current state (reps launches each; the state and the status word are left as they
-   were, the RHS array is overwritten) and keep the fastest per direction.  The choice is cached in the process per grid (block
+   current state, pipelined and not where the pipelined sweeps apply (reps launches each;
+   the state and the status word are left as they were, the RHS array is overwritten) and
+   keep the fastest per direction.  The choice is cached in the process per grid (block
    extents, schemes, model, build, hybrid or plain): a later context of the same grid takes
    it without timing.  shape_out (may be NULL): the shapes chosen; ms_out (may be NULL):
    9 doubles, ms per launch of direction d with shape s at [3d + s], -1 where not timed
@@ -249,7 +250,9 @@ int nuc3d_autotune(nuc3d_ctx *ctx, int reps, int shape_out[3], double ms_out[9])
    producer warp loads the next tiles' state, Jacobian and metric with tensor-map (TMA)
    copies while the other warps compute; results are identical either way.  It applies to
    Euler3d contexts whose blocks all have an even nx (16-byte rows); elsewhere, or with
-   on = 0, every sweep CTA loads its own tile.  nuc3d_get_pipeline: 1 if it is in use. */
+   on = 0, every sweep CTA loads its own tile.  nuc3d_autotune also chooses, per direction,
+   between the two.  nuc3d_get_pipeline: the directions that run pipelined (bit d), 0 for
+   none. */
 int nuc3d_set_pipeline(nuc3d_ctx *ctx, int on);
 int nuc3d_get_pipeline(nuc3d_ctx *ctx, int *on);
 

@@ -188,6 +188,7 @@ struct Launch {
   // memory and the persistent grid (CTAs); null / 0: the one-tile-per-CTA sweeps
   const CUtensorMap *d_maps;
   int pipe_grid;
+  int pipe_dirs;           // bit d: direction d runs pipelined (nuc3d_autotune picks per direction)
   // each block's residual root of the previous step (the reference's static res_last);
   // null: no residual (nuc3d_rhs_noalloc)
   double *d_res_last;

@@ -1715,7 +1715,7 @@ inline cudaError_t launch_sweep_s(const Launch &L, int stage, int flags) {
     }
   }
 #endif
-  if (L.d_maps && L.pipe_grid > 0 && !ns) {
+  if (L.d_maps && L.pipe_grid > 0 && !ns && ((L.pipe_dirs >> DIR) & 1)) {
     // persistent sweep fed by tensor-map loads (sweep_pipe.cuh)
     const int grid = ntiles < L.pipe_grid ? ntiles : L.pipe_grid;
     pipe_sweep_kernel<DIR, SCH, SHP><<<grid, kPipeThreads, PipeSmem<DIR, SCH, SHP>::TOTAL, L.stream>>>(

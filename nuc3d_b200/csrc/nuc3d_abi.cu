@@ -117,6 +117,7 @@ struct nuc3d_ctx {
   std::vector<BlockDev> hdesc;  // host copy of the block descriptors (tile divisors change)
   // pipelined sweeps: tensor maps of every block and direction (built by build_maps)
   bool use_pipe = true;
+  int pipe_mask = 7;  // directions to run pipelined where the grid allows (bit d)
   CUtensorMap *d_maps = nullptr;
   // the residual of each step: per-tile partial sums, each block's previous residual root
   double *d_res_part = nullptr, *d_res_last = nullptr;
@@ -499,6 +500,7 @@ int build_maps(nuc3d_ctx *c) {
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   L.d_maps = c->d_maps;
   L.pipe_grid = 2 * sms;  // two persistent CTAs per SM
+  L.pipe_dirs = c->pipe_mask;
   return NUC3D_OK;
 }
 
@@ -871,12 +873,13 @@ int nuc3d_get_tiles(nuc3d_ctx *c, int shape[3]) {
 namespace {
 // Tile shapes chosen by nuc3d_autotune, per grid: block extents, schemes, model, build.
 std::mutex g_tune_mutex;
-std::map<std::string, std::array<int, 3>> g_tune_cache;
+std::map<std::string, std::array<int, 4>> g_tune_cache;  // shapes, pipelined directions
 
 std::string tune_key(const nuc3d_ctx *c) {
   std::string k = c->exact ? "x" : "f";
   k += c->P.model == MODEL_NS ? "ns" : "eu";
   k += c->P.sensor ? "h" : "p";
+  k += c->use_pipe ? "t" : "n";
   for (int d = 0; d < 3; ++d) k += ":" + std::to_string(c->P.scheme[d]) + "." + std::to_string(c->P.vis[d]);
   for (const HostBlock &b : c->blocks)
     k += "|" + std::to_string(b.n[0]) + "x" + std::to_string(b.n[1]) + "x" + std::to_string(b.n[2]);
@@ -889,7 +892,7 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
   if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
   if (reps < 1) reps = 3;
   const std::string key = tune_key(c);
-  std::array<int, 3> best = {0, 0, 0};
+  std::array<int, 4> best = {0, 0, 0, 0};  // shapes, then the pipelined directions (bits)
   bool cached = false;
   {
     std::lock_guard<std::mutex> g(g_tune_mutex);
@@ -910,34 +913,47 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
     CUDA_TRY(cudaEventCreate(&ev.b));
     cudaEvent_t e0 = ev.a, e1 = ev.b;
     int cur[3] = {c->L.shape[0], c->L.shape[1], c->L.shape[2]};
+    // every tile shape of every explicit direction, each pipelined and one tile per CTA
+    // where the pipelined sweeps apply (the pipeline's bit for a direction is its choice)
+    const int mask0 = c->pipe_mask;
+    const bool can_pipe = c->L.d_maps != nullptr;
+    int mask = mask0;
     for (int d = 0; d < 3; ++d) {
       if (compact_scheme(c->P.scheme[d])) { best[d] = 0; continue; }
       double tbest = 1e300;
+      int best_mode = (mask0 >> d) & 1;
       for (int sh = 0; sh < kTileShapes; ++sh) {
-        cur[d] = sh;
-        if (int r = apply_shapes(c, cur)) return r;
-        auto sweep = [&]() {
-          return c->exact ? nuc3d::exact::run_sweep(c->L, d, 0, 0) : nuc3d::fast::run_sweep(c->L, d, 0, 0);
-        };
-        CUDA_TRY(sweep());  // warm-up
-        CUDA_TRY(cudaEventRecord(e0, c->stream));
-        for (int r = 0; r < reps; ++r) CUDA_TRY(sweep());
-        CUDA_TRY(cudaEventRecord(e1, c->stream));
-        CUDA_TRY(cudaEventSynchronize(e1));
-        float t = 0.0f;
-        CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
-        const double ms = (double)t / reps;
-        if (ms_out) ms_out[3 * d + sh] = ms;
-        if (ms < tbest) { tbest = ms; best[d] = sh; }
+        for (int mode = can_pipe ? 1 : 0; mode >= 0; --mode) {
+          cur[d] = sh;
+          mask = (mask & ~(1 << d)) | (mode << d);
+          c->pipe_mask = mask;
+          if (int r = apply_shapes(c, cur)) return r;
+          auto sweep = [&]() {
+            return c->exact ? nuc3d::exact::run_sweep(c->L, d, 0, 0) : nuc3d::fast::run_sweep(c->L, d, 0, 0);
+          };
+          CUDA_TRY(sweep());  // warm-up
+          CUDA_TRY(cudaEventRecord(e0, c->stream));
+          for (int r = 0; r < reps; ++r) CUDA_TRY(sweep());
+          CUDA_TRY(cudaEventRecord(e1, c->stream));
+          CUDA_TRY(cudaEventSynchronize(e1));
+          float t = 0.0f;
+          CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+          const double ms = (double)t / reps;
+          if (ms_out && (ms_out[3 * d + sh] < 0.0 || ms < ms_out[3 * d + sh])) ms_out[3 * d + sh] = ms;
+          if (ms < tbest) { tbest = ms; best[d] = sh; best_mode = mode; }
+        }
       }
       cur[d] = best[d];
+      mask = (mask & ~(1 << d)) | (best_mode << d);
     }
+    best[3] = mask;
     CUDA_TRY(cudaMemcpy(&c->d_state->status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(&c->d_state->reset_cells, &resets0, sizeof(resets0), cudaMemcpyHostToDevice));
     std::lock_guard<std::mutex> g(g_tune_mutex);
     g_tune_cache[key] = best;
   }
   const int shp[3] = {best[0], best[1], best[2]};
+  if (c->use_pipe) c->pipe_mask = best[3];
   if (int r = apply_shapes(c, shp)) return r;
   if (shape_out)
     for (int d = 0; d < 3; ++d) shape_out[d] = best[d];
@@ -1174,13 +1190,14 @@ int nuc3d_set_pipeline(nuc3d_ctx *c, int on) {
   cudaSetDevice(c->device);
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->use_pipe = on != 0;
+  c->pipe_mask = on ? 7 : 0;
   c->drop_graph();
   return build_maps(c);
 }
 
 int nuc3d_get_pipeline(nuc3d_ctx *c, int *on) {
   if (!c || !on) return fail(NUC3D_EINVAL, "null argument");
-  *on = c->L.d_maps != nullptr ? 1 : 0;
+  *on = c->L.d_maps != nullptr ? c->L.pipe_dirs : 0;
   return NUC3D_OK;
 }
 

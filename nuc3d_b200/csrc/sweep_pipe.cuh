@@ -21,6 +21,10 @@
 // barrier), the producer stops issuing, and it waits (bounded the same way) for the copies
 // it issued before it returns.
 
+#ifndef NUC3D_PIPE_FACE_UNROLL
+#define NUC3D_PIPE_FACE_UNROLL 2  // variables per iteration of the face loop
+#endif
+constexpr int kPipeFaceUnroll = NUC3D_PIPE_FACE_UNROLL;
 constexpr int kProdWarp = kThreads / 32;         // warp index of the producer
 constexpr int kPipeThreads = kThreads + 32;      // 288 consumers + one producer warp
 constexpr unsigned long long kPipeWaitNs = 2000000000ull;  // 2 s
@@ -427,7 +431,7 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
         const int f = T.c0 + fl;
         if (!edge) {
           const bool cz = compat && f >= T.ts && f <= T.G.L - T.ts;
-#pragma unroll 2
+#pragma unroll kPipeFaceUnroll
           for (int v = 0; v < 5; ++v) {
             const double *rowP = sF + (v * TW + w) * SP + (R + fl);
             const double *rowN = sF + ((5 + v) * TW + w) * SP + (R + fl);
