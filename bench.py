@@ -436,15 +436,20 @@ def ours(args):
         except Exception as e:  # the baseline is a report, never a reason to fail the bench
             cpu = {"value": None, "unit": "Mcell-RK3-steps/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}".splitlines()[0][:200], "cpu_model": cpu_model()}
-    # the batched multi-block Navier-Stokes workload (24 uneven blocks), on this GPU
+    # the batched multi-block Navier-Stokes workload (24 uneven blocks) and the
+    # shock-turbulence workload (plain against the learned hybrid), on this GPU
     launches = s.kernels_per_step() * args.steps
-    turb = None
+    turb = shock = None
     if world == 1 and not args.no_turbulence:
         s.close()
         try:
             turb = turbulence24(args, with_cpu=not args.no_cpu_baseline)
         except Exception as e:  # reported, never a reason to fail the bench
             turb = {"unavailable": f"{type(e).__name__}: {e}".splitlines()[0][:300]}
+        try:
+            shock = shock_turbulence(args)
+        except Exception as e:
+            shock = {"unavailable": f"{type(e).__name__}: {e}".splitlines()[0][:300]}
 
     line = {
         "metric": "Mcell-RK3-steps/s", "value": value, "unit": "Mcell-RK3-steps/s",
@@ -485,6 +490,7 @@ def ours(args):
         "cpu_baseline": cpu,
         "hybrid": hybrid,
         "turbulence24": turb,
+        "shock_turbulence": shock,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -493,6 +499,74 @@ def ours(args):
     if turb is None:
         s.close()
     return 0
+
+
+SHOCK_WORKLOAD = ("Mach 1.5 normal shock at x = pi/2 in decaying isotropic turbulence (the 24-block "
+                  "case's spectrum, Mt 0.6, Re_lambda 100), 512x256x256 FP64 Navier-Stokes, inflow "
+                  "x-, outflow x+, periodic y/z, WENO5-Z, AUSM, cd6, TVD-RK3 CFL 0.5")
+
+
+def shock_turbulence(args, steps=10, warm=2):
+    """Plain WENO-Z against the hybrid with the learned face sensor (trained on the
+    Taylor-Green and spherical-blast runs only, so this flow is held out) on the
+    shock-turbulence workload: Mcell-RK3-steps/s of both from the same state over the same
+    steps, the L1 density error of the hybrid against plain, and the shock position."""
+    import torch
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+    from nuc3d_b200 import sensor as SENS
+    shape = (512, 256, 256)
+    prim, re, inlet, nodes = C.shock_turbulence(shape)
+    h = 2.0 * math.pi / shape[1]
+    q0 = C.prim_to_q(prim, np.full(prim.shape[1:], 1.0 / (h * h * h)), 1.4)
+    del prim
+    cells = int(np.prod(shape))
+    s = nb.Solver(nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="NavierStokes3d",
+                            reynolds=re, mach=0.6, cfl=0.5, exact=False))
+    t, i = C.shock_faces()
+    vals = np.zeros((6, 5))
+    vals[0] = inlet
+    b = s.add_block(*shape, t, i, vals)
+    s.set_nodes(b, *nodes)
+    del nodes
+    s.finalize()
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+
+    def run(label):
+        s.set_q(b, q0)
+        s.set_time(0.0)
+        tiles = s.autotune(reps=2)["shape"]
+        s.set_q(b, q0)
+        s.step(warm)
+        s.sync()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        s.step(steps, sync=False)
+        ev1.record(stream)
+        ev1.synchronize()
+        s.sync()
+        ms = ev0.elapsed_time(ev1) / steps
+        rho = s.get_q(b)[0] * (1.0 / (h * h * h))  # U/J -> rho on the uniform mesh
+        return ms, rho, tiles
+
+    ms_p, rho_p, tiles_p = run("plain")
+    s.set_sensor(SENS.load_weights(), SENS.DEFAULT_THRESHOLD)
+    ms_h, rho_h, tiles_h = run("hybrid")
+    s.set_sensor(None)
+    s.close()
+    vp = cells / (ms_p * 1e-3) / 1e6
+    vh = cells / (ms_h * 1e-3) / 1e6
+    return {"workload": SHOCK_WORKLOAD, "cells": cells, "steps_compared": warm + steps,
+            "plain": {"value": vp, "unit": "Mcell-RK3-steps/s", "ms_per_step": ms_p,
+                      "tile_shapes": list(tiles_p)},
+            "hybrid": {"value": vh, "unit": "Mcell-RK3-steps/s", "ms_per_step": ms_h,
+                       "tile_shapes": list(tiles_h), "logit_threshold": SENS.DEFAULT_THRESHOLD},
+            "vs_plain": vh / vp,
+            "l1_density_error_vs_plain": float(np.abs(rho_h - rho_p).sum() / np.abs(rho_p).sum()),
+            "shock_x": {"initial": 0.5 * math.pi, "plain": C.shock_position(rho_p, h),
+                        "hybrid": C.shock_position(rho_h, h)},
+            "sensor_training": "Taylor-Green vortex and spherical blast runs only (held out here)"}
 
 
 TURB_WORKLOAD = ("decaying isotropic turbulence, 2pi periodic box in 24 uneven blocks (per-axis "
@@ -692,8 +766,11 @@ def main():
                     help="leave out the 24-block Navier-Stokes line of the default run")
     ap.add_argument("--tiles", type=lambda x: tuple(int(v) for v in x.split(",")), default=None,
                     help="sweep tile shapes per direction, e.g. 2,0,0 (default: nuc3d_autotune)")
-    ap.add_argument("--workload", default="sphere256", choices=["sphere256", "turbulence24"],
-                    help="turbulence24: the 24-block Navier-Stokes grid on one GPU (our arm only)")
+    ap.add_argument("--workload", default="sphere256",
+                    choices=["sphere256", "turbulence24", "shock_turbulence"],
+                    help="turbulence24: the 24-block Navier-Stokes grid on one GPU; "
+                         "shock_turbulence: plain against hybrid on the shock-turbulence grid "
+                         "(our arm only)")
     ap.add_argument("--profile-case", action="store_true",
                     help="untimed run of the workload at --shape (the target of ncu captures)")
     ap.add_argument("--shape", type=int, default=128, help="--profile-case: cells per axis")
@@ -705,6 +782,12 @@ def main():
         return profile_case(args)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.workload == "shock_turbulence":
+        if args.impl == "reference" or args.gpus > 1:
+            print(json.dumps({"impl": args.impl, "unavailable": "shock_turbulence runs our arm on one GPU only"}))
+            return 0
+        print(json.dumps(shock_turbulence(args)), flush=True)
+        return 0
     if args.workload == "turbulence24":
         if args.impl == "reference" or args.gpus > 1:
             print(json.dumps({"impl": args.impl, "unavailable": "turbulence24 runs our arm on one GPU only"}))

@@ -8,6 +8,8 @@ No dataset is involved: every state is generated from a formula.
                         (src/block.cpp:785-816)
   * isotropic_turbulence + uneven_blocks -- decaying isotropic turbulence in a periodic
                         2 pi box cut into blocks of uneven sizes (seeded), injected the same way
+  * shock_turbulence -- a Rankine-Hugoniot normal shock in that turbulence, inflow/outflow
+                        in x, periodic y and z
 Uniform boxes get analytic metrics (xi_x = 1/hx, jac = 1/(hx hy hz)); curvilinear
 meshes go through nuc3d_b200.metrics (block::getJacobians).
 """
@@ -127,6 +129,64 @@ def isotropic_turbulence(shape, seed=0, k0=4.0, mt=0.6, gamma=1.4, re_lambda=100
     rho = np.ones_like(u)
     p = rho / (gamma * mt * mt)
     return np.stack([rho, u, v, w, p]), re_lambda / (urms * lam)
+
+
+def normal_shock(m1, gamma=1.4):
+    """Rankine-Hugoniot jumps of a normal shock of upstream Mach number m1: (rho2/rho1,
+    u2/u1, p2/p1)."""
+    r = (gamma + 1.0) * m1 * m1 / ((gamma - 1.0) * m1 * m1 + 2.0)
+    return r, 1.0 / r, 1.0 + 2.0 * gamma / (gamma + 1.0) * (m1 * m1 - 1.0)
+
+
+def shock_turbulence(shape=(512, 256, 256), m1=1.5, x_shock=0.5 * math.pi, seed=7, mt=0.6,
+                     gamma=1.4, re_lambda=100.0):
+    """A Mach m1 normal shock at x = x_shock in the decaying-turbulence field of the
+    24-block workload: the box [0, 2 pi nx/ny] x [0, 2 pi]^2 with uniform spacing 2 pi/ny,
+    periodic in y and z, inflow through x = 0 and outflow through the far x face.
+
+    Nondimensionalised as the reference (T = gamma Ma^2 p / rho) with Ma = mt: upstream
+    rho = T = 1, so the sound speed is 1/mt and the mean velocity m1/mt along x; downstream
+    the Rankine-Hugoniot state.  The solenoidal fluctuation of isotropic_turbulence (rms
+    |u| = 1, turbulent Mach number mt, its 2 pi period repeated along x) is added on both
+    sides.  Returns (prim (5, nz, ny, nx), reynolds, inlet (rho, u, v, w, p) of the x- face,
+    node coordinates (x, y, z))."""
+    nx, ny, nz = shape
+    h = 2.0 * math.pi / ny
+    turb, re = isotropic_turbulence((ny, ny, nz), seed=seed, mt=mt, gamma=gamma, re_lambda=re_lambda)
+    reps = -(-nx // ny)
+    fl = np.concatenate([turb[:, :, :, :]] * reps, axis=3)[:, :, :, :nx]
+    xc = (np.arange(nx) + 0.5) * h
+    up = xc < x_shock
+    rr, ur, pr = normal_shock(m1, gamma)
+    rho1, p1 = 1.0, 1.0 / (gamma * mt * mt)
+    u1 = m1 / mt
+    rho = np.where(up, rho1, rho1 * rr)[None, None, :] * np.ones((nz, ny, 1))
+    umean = np.where(up, u1, u1 * ur)[None, None, :]
+    p = np.where(up, p1, p1 * pr)[None, None, :] * np.ones((nz, ny, 1))
+    prim = np.stack([rho, umean + fl[1], fl[2], fl[3], p])
+    xs = np.arange(nx + 1) * h
+    ys = np.arange(ny + 1) * h
+    zs = np.arange(nz + 1) * h
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    return prim, re, (rho1, u1, 0.0, 0.0, p1), (X, Y, Z)
+
+
+def shock_faces(block=0):
+    """BC_Topo of the shock-turbulence block: inlet on x-, outlet on x+, periodic y and z."""
+    return [-1, -1, block, block, block, block], [0, 1, 3, 2, 5, 4]
+
+
+def shock_position(rho, h):
+    """x of the shock: where the density averaged over y and z first reaches the mean of
+    its upstream (first column) and downstream (last column) values, linearly interpolated
+    between cell centres."""
+    prof = rho.mean(axis=(0, 1))
+    mid = 0.5 * (prof[0] + prof[-1])
+    i = int(np.argmax(prof >= mid))
+    if i == 0:
+        return 0.5 * h
+    t = (mid - prof[i - 1]) / (prof[i] - prof[i - 1])
+    return (i - 0.5 + t) * h
 
 
 def uneven_blocks(nblocks=(2, 3, 4), sizes=(48, 64, 96, 128, 160), seed=0):

@@ -22,7 +22,7 @@
 // it issued before it returns.
 
 #ifndef NUC3D_PIPE_FACE_UNROLL
-#define NUC3D_PIPE_FACE_UNROLL 2  // variables per iteration of the face loop
+#define NUC3D_PIPE_FACE_UNROLL 5  // variables per iteration of the face loop (5: 2-3% faster than 1 or 2)
 #endif
 constexpr int kPipeFaceUnroll = NUC3D_PIPE_FACE_UNROLL;
 constexpr int kProdWarp = kThreads / 32;         // warp index of the producer
