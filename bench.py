@@ -3,6 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --workload turbulence24      (the 24-block Navier-Stokes grid)
+    python bench.py --workload shock_turbulence|boundary_layer   (plain against hybrid)
     python bench.py --profile-case --shape 192 --sweeps 2 [--steps N] [--ns] [--hybrid]
                                                  (untimed: the command ncu captures)
 
@@ -439,7 +440,7 @@ def ours(args):
     # the batched multi-block Navier-Stokes workload (24 uneven blocks) and the
     # shock-turbulence workload (plain against the learned hybrid), on this GPU
     launches = s.kernels_per_step() * args.steps
-    turb = shock = None
+    turb = shock = bl = None
     if world == 1 and not args.no_turbulence:
         s.close()
         try:
@@ -450,6 +451,10 @@ def ours(args):
             shock = shock_turbulence(args)
         except Exception as e:
             shock = {"unavailable": f"{type(e).__name__}: {e}".splitlines()[0][:300]}
+        try:
+            bl = boundary_layer(args)
+        except Exception as e:
+            bl = {"unavailable": f"{type(e).__name__}: {e}".splitlines()[0][:300]}
 
     line = {
         "metric": "Mcell-RK3-steps/s", "value": value, "unit": "Mcell-RK3-steps/s",
@@ -491,6 +496,7 @@ def ours(args):
         "hybrid": hybrid,
         "turbulence24": turb,
         "shock_turbulence": shock,
+        "boundary_layer": bl,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -567,6 +573,103 @@ def shock_turbulence(args, steps=10, warm=2):
             "shock_x": {"initial": 0.5 * math.pi, "plain": C.shock_position(rho_p, h),
                         "hybrid": C.shock_position(rho_h, h)},
             "sensor_training": "Taylor-Green vortex and spherical blast runs only (held out here)"}
+
+
+BL_WORKLOAD = ("supersonic flat-plate boundary layer, Ma 2.25, Re_x 1e5 at the inflow (Re_delta "
+               "1581), isothermal wall T_w/T_inf 1.9, Gaussian bump h 0.5 delta w 2 delta, "
+               "1024x256x128 cells on a tanh wall-normal stretched mesh in 4x2x2 = 16 uneven "
+               "blocks; inlet x-, outlet x+, wall y-, outlet y+, periodic z; FP64 Navier-Stokes, "
+               "WENO5-Z, AUSM, cd6, TVD-RK3 CFL 0.5")
+
+
+def boundary_layer(args, steps=10, warm=2, thresholds=(-4.0, -2.0, 0.0)):
+    """The boundary-layer workload on one GPU: the 16 blocks in one context (on-device ghost
+    copies, one launch per sweep over all blocks), metrics from the nodes on the device.
+    Plain WENO-Z, then the learned hybrid (batched over the same blocks) at each logit
+    threshold, all from the same state over the same steps; the volume-weighted L1 density
+    error of each against plain.  The error they are matched against is the L1 distance
+    between two plain fifth-order schemes (WENO5-JS against WENO5-Z) over the same steps:
+    a hybrid within it changes the solution less than the choice of WENO weights does."""
+    import torch
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+    from nuc3d_b200 import sensor as SENS
+
+    torch.cuda.set_device(0)
+    shape = (1024, 256, 128)
+    blocks, types, ids, values, prm = C.boundary_layer(shape)
+    cells = int(np.prod(shape))
+    stream = torch.cuda.Stream()
+
+    def solver(scheme):
+        s = nb.Solver(nb.Config(scheme_ivs=(scheme,) * 3, riemann="AUSM", model="NavierStokes3d",
+                                reynolds=prm["Reynolds"], mach=prm["Mach"], t_wall=prm["T_wall"],
+                                cfl=0.5, exact=False))
+        for r, b in enumerate(blocks):
+            s.add_block(*b["shape"], types[r], ids[r], values[r])
+        for r, b in enumerate(blocks):
+            s.set_nodes(r, *b["nodes"])
+        s.finalize()
+        s.set_stream(stream.cuda_stream)
+        if "q" not in blocks[0]:
+            for r, b in enumerate(blocks):
+                b["q"] = np.ascontiguousarray(C.prim_to_q(b["prim"], s.get_metrics(r)["jac"],
+                                                          prm["Gamma"]))
+                del b["prim"]
+        return s
+
+    def run(s):
+        for r, b in enumerate(blocks):
+            s.set_q(r, b["q"])
+        s.set_time(0.0)
+        tiles = s.autotune(reps=2)["shape"]
+        for r, b in enumerate(blocks):
+            s.set_q(r, b["q"])
+        s.step(warm)
+        s.sync()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        s.step(steps, sync=False)
+        ev1.record(stream)
+        ev1.synchronize()
+        s.sync()
+        ms = ev0.elapsed_time(ev1) / steps
+        # U/J = rho x cell volume: its L1 norm is the volume-weighted L1 norm of rho
+        mass = np.concatenate([s.get_q(r)[0].ravel() for r in range(len(blocks))])
+        return ms, mass, list(tiles), s.status()
+
+    s = solver("weno5z")
+    ms_p, m_p, tiles_p, st_p = run(s)
+    l1 = lambda m: float(np.abs(m - m_p).sum() / np.abs(m_p).sum())  # noqa: E731
+    hyb = []
+    for th in thresholds:
+        s.set_sensor(SENS.load_weights(), th)
+        ms_h, m_h, tiles_h, _ = run(s)
+        hyb.append({"logit_threshold": th, "value": cells / (ms_h * 1e-3) / 1e6,
+                    "ms_per_step": ms_h, "vs_plain": ms_p / ms_h, "l1_density_error_vs_plain": l1(m_h),
+                    "tile_shapes": tiles_h})
+        del m_h
+    s.set_sensor(None)
+    s.close()
+    s = solver("weno5js")
+    ms_js, m_js, _, _ = run(s)
+    s.close()
+    target = l1(m_js)
+    ok = [h for h in hyb if h["l1_density_error_vs_plain"] <= target]
+    best = max(ok, key=lambda h: h["value"]) if ok else None
+    return {"workload": BL_WORKLOAD, "cells": cells, "blocks": len(blocks),
+            "block_shapes": [list(b["shape"]) for b in blocks], "steps_compared": warm + steps,
+            "plain": {"value": cells / (ms_p * 1e-3) / 1e6, "unit": "Mcell-RK3-steps/s",
+                      "ms_per_step": ms_p, "tile_shapes": tiles_p, "status_bits": st_p},
+            "hybrid": hyb,
+            "matched_error": {"target_l1": target,
+                              "target": "L1 density distance of plain WENO5-JS from plain WENO5-Z "
+                                        "over the same steps",
+                              "weno5js_ms_per_step": ms_js,
+                              "hybrid_at_target": best,
+                              "vs_plain": best["vs_plain"] if best else None},
+            "sensor_training": "Taylor-Green vortex and spherical blast runs only (held out here)",
+            "metrics": "nuc3d_block_set_nodes (block::getJacobians on the device)"}
 
 
 TURB_WORKLOAD = ("decaying isotropic turbulence, 2pi periodic box in 24 uneven blocks (per-axis "
@@ -767,10 +870,10 @@ def main():
     ap.add_argument("--tiles", type=lambda x: tuple(int(v) for v in x.split(",")), default=None,
                     help="sweep tile shapes per direction, e.g. 2,0,0 (default: nuc3d_autotune)")
     ap.add_argument("--workload", default="sphere256",
-                    choices=["sphere256", "turbulence24", "shock_turbulence"],
+                    choices=["sphere256", "turbulence24", "shock_turbulence", "boundary_layer"],
                     help="turbulence24: the 24-block Navier-Stokes grid on one GPU; "
-                         "shock_turbulence: plain against hybrid on the shock-turbulence grid "
-                         "(our arm only)")
+                         "shock_turbulence / boundary_layer: plain against hybrid on those "
+                         "grids (our arm only)")
     ap.add_argument("--profile-case", action="store_true",
                     help="untimed run of the workload at --shape (the target of ncu captures)")
     ap.add_argument("--shape", type=int, default=128, help="--profile-case: cells per axis")
@@ -782,11 +885,13 @@ def main():
         return profile_case(args)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    if args.workload == "shock_turbulence":
+    if args.workload in ("shock_turbulence", "boundary_layer"):
         if args.impl == "reference" or args.gpus > 1:
-            print(json.dumps({"impl": args.impl, "unavailable": "shock_turbulence runs our arm on one GPU only"}))
+            print(json.dumps({"impl": args.impl,
+                              "unavailable": f"{args.workload} runs our arm on one GPU only"}))
             return 0
-        print(json.dumps(shock_turbulence(args)), flush=True)
+        fn = shock_turbulence if args.workload == "shock_turbulence" else boundary_layer
+        print(json.dumps(fn(args)), flush=True)
         return 0
     if args.workload == "turbulence24":
         if args.impl == "reference" or args.gpus > 1:

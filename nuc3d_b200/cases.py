@@ -10,6 +10,8 @@ No dataset is involved: every state is generated from a formula.
                         2 pi box cut into blocks of uneven sizes (seeded), injected the same way
   * shock_turbulence -- a Rankine-Hugoniot normal shock in that turbulence, inflow/outflow
                         in x, periodic y and z
+  * boundary_layer   -- a supersonic boundary layer over a Gaussian bump on a tanh-stretched
+                        mesh in uneven blocks, isothermal wall
 Uniform boxes get analytic metrics (xi_x = 1/hx, jac = 1/(hx hy hz)); curvilinear
 meshes go through nuc3d_b200.metrics (block::getJacobians).
 """
@@ -187,6 +189,102 @@ def shock_position(rho, h):
         return 0.5 * h
     t = (mid - prof[i - 1]) / (prof[i] - prof[i - 1])
     return (i - 0.5 + t) * h
+
+
+def split_sizes(total, parts, seed, quantum=4, spread=0.25):
+    """`parts` uneven extents (multiples of `quantum`) summing to `total`, drawn with a
+    fixed seed within +-spread of the even split."""
+    rng = np.random.default_rng(seed)
+    base = total / parts
+    while True:
+        w = base * (1.0 + spread * rng.uniform(-1.0, 1.0, parts))
+        n = [max(quantum, int(round(x / quantum)) * quantum) for x in w[:-1]]
+        last = total - sum(n)
+        if last >= quantum and last % quantum == 0:
+            return n + [last]
+
+
+def boundary_layer(shape=(1024, 256, 128), nblocks=(4, 2, 2), seed=5, mach=2.25, t_wall=1.9,
+                   re_delta=1581.0, lengths=(32.0, 8.0, 4.0), bump=(12.0, 0.5, 2.0),
+                   stretch=2.5, gamma=1.4):
+    """Supersonic flat-plate boundary layer over a Gaussian roughness bump, cut into
+    nblocks (x, y, z) uneven blocks.
+
+    Lengths in units of the inflow boundary-layer thickness delta; the bump y_w(x) =
+    h exp(-((x - x_b)/w)^2) with (x_b, h, w) = bump, h = 0.5 delta, w = 2 delta.  Nodes:
+    x and z uniform; y from the local wall to the top, clustered at the wall by tanh
+    stretching, y = y_w + (Ly - y_w) (1 - tanh(b (1 - s)) / tanh(b)), s uniform in [0, 1].
+    Nondimensionalised as the reference (T = gamma Ma^2 p / rho) with the free stream
+    rho = T = u = 1, Ma = mach; Reynolds number per delta re_delta (Re_x = 1e5 at the
+    inflow with the Blasius thickness delta = 5 x / sqrt(Re_x)).  Initial state: a tanh
+    velocity profile u = tanh(3 d / delta) in the wall distance d, the Crocco-Busemann
+    temperature between the isothermal wall T_w = t_wall and the free stream (recovery
+    factor 0.89), uniform pressure.  Faces: inlet (free stream) on x-, outlet on x+,
+    isothermal wall on y-, outlet on y+, periodic z.
+    Returns (blocks, types, ids, values, params): blocks a list of dicts with 'shape',
+    'lo' (cell offsets), 'nodes' (x, y, z), 'prim' (5, nz, ny, nx); types/ids/values per
+    block as nuc3d_block_add takes them; params the PhysModel values."""
+    nx, ny, nz = shape
+    parts = [split_sizes(shape[d], nblocks[d], seed + d) for d in range(3)]
+    Lx, Ly, Lz = lengths
+    xb, hb, wb = bump
+    xs = np.arange(nx + 1) * (Lx / nx)
+    zs = np.arange(nz + 1) * (Lz / nz)
+    sgrid = np.arange(ny + 1) / ny
+    yw = hb * np.exp(-((xs - xb) / wb) ** 2)
+    fr = 1.0 - np.tanh(stretch * (1.0 - sgrid)) / np.tanh(stretch)
+    Yn = yw[None, :] + (Ly - yw[None, :]) * fr[:, None]          # (ny+1, nx+1)
+    p_inf = 1.0 / (gamma * mach * mach)
+    t_rec = 1.0 + 0.89 * 0.5 * (gamma - 1.0) * mach * mach
+    types, ids, values = [], [], []
+    na, nb_, nc = nblocks
+    idx = lambda a, b, c: a + na * (b + nb_ * c)  # noqa: E731
+    off = [np.concatenate([[0], np.cumsum(p)]) for p in parts]
+    inlet = [1.0, 1.0, 0.0, 0.0, p_inf]
+    blocks = []
+    for c in range(nc):
+        for b in range(nb_):
+            for a in range(na):
+                lo = (int(off[0][a]), int(off[1][b]), int(off[2][c]))
+                n = (parts[0][a], parts[1][b], parts[2][c])
+                xi = xs[lo[0]:lo[0] + n[0] + 1]
+                zi = zs[lo[2]:lo[2] + n[2] + 1]
+                yi = Yn[lo[1]:lo[1] + n[1] + 1, lo[0]:lo[0] + n[0] + 1]
+                X = np.broadcast_to(xi[None, None, :], (n[2] + 1, n[1] + 1, n[0] + 1)).copy()
+                Y = np.broadcast_to(yi[None, :, :], (n[2] + 1, n[1] + 1, n[0] + 1)).copy()
+                Z = np.broadcast_to(zi[:, None, None], (n[2] + 1, n[1] + 1, n[0] + 1)).copy()
+                # cell centres (averages of the 8 nodes) and their wall distance
+                cen = lambda A: 0.125 * (A[:-1, :-1, :-1] + A[1:, :-1, :-1] + A[:-1, 1:, :-1] + A[:-1, :-1, 1:]
+                                         + A[1:, 1:, :-1] + A[1:, :-1, 1:] + A[:-1, 1:, 1:] + A[1:, 1:, 1:])  # noqa: E731
+                xc, yc = cen(X), cen(Y)
+                dist = yc - hb * np.exp(-((xc - xb) / wb) ** 2)
+                u = np.tanh(3.0 * np.maximum(dist, 0.0))
+                T = t_wall + (t_rec - t_wall) * u + (1.0 - t_rec) * u * u
+                p = np.full_like(u, p_inf)
+                rho = p * gamma * mach * mach / T
+                zero = np.zeros_like(u)
+                blocks.append(dict(shape=n, lo=lo, nodes=(X, Y, Z), prim=np.stack([rho, u, zero, zero, p])))
+                t, i, v = [], [], np.zeros((6, 5))
+                pos = (a, b, c)
+                for f in range(6):
+                    d, side = f // 2, f % 2
+                    q = list(pos)
+                    q[d] += 1 if side else -1
+                    if d == 2:  # periodic spanwise
+                        q[2] %= nc
+                        t.append(idx(*q)); i.append(f ^ 1)
+                    elif 0 <= q[d] < nblocks[d]:
+                        t.append(idx(*q)); i.append(f ^ 1)
+                    elif f == 0:
+                        t.append(-1); i.append(0); v[0] = inlet
+                    elif f == 2:
+                        t.append(-1); i.append(2)
+                    else:
+                        t.append(-1); i.append(1)
+                types.append(t); ids.append(i); values.append(v)
+    params = {"Reynolds": re_delta, "Mach": mach, "Pt": 0.72, "Gamma": gamma, "T_ref": 110.4,
+              "T_inf": 288.0, "T_wall": t_wall}
+    return blocks, types, ids, values, params
 
 
 def uneven_blocks(nblocks=(2, 3, 4), sizes=(48, 64, 96, 128, 160), seed=0):
