@@ -4,6 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --workload turbulence24      (the 24-block Navier-Stokes grid)
     python bench.py --workload shock_turbulence|boundary_layer   (plain against hybrid)
+    python bench.py --workload compact           (crweno5 / hccs: fused against three kernels)
     python bench.py --profile-case --shape 192 --sweeps 2 [--steps N] [--ns] [--hybrid]
                                                  (untimed: the command ncu captures)
 
@@ -54,6 +55,11 @@ FLOPS = {
     "weno5js": 67,         # per face, variable and split: src/weno5js.cpp:75-108
     "weno5z": 74,          # src/weno5z.cpp:74-109
     "weno7js": 146,        # src/weno7js.cpp:84-136
+    # compact schemes, per face, variable and split: the interior row (crweno5
+    # src/crweno5.cpp:135-163: 68; hccs src/hccs.cpp:154-187: 104) + the Thomas solve
+    # (src/crweno5.cpp:207-218: 10 per row)
+    "crweno5": 78,
+    "hccs": 114,
     "combine": 1,          # per face and variable: src/euler3d.cpp:45-49
     "cd6": 8,              # per cell and field: 3 differences, 3 products, 2 sums
                            # (src/centraldifference6th.cpp:26-43)
@@ -69,6 +75,9 @@ SWEEP_BYTES = {0: 72 + 40, 1: 72 + 80, 2: 72 + 80}
 # dram__bytes_write.sum of a 192^3 block, whose every array is larger than L2, divided by
 # its cells; a launch's traffic grows with its cells).
 SWEEP_TRAFFIC = {0: 108.1, 1: 152.1, 2: 150.8}
+# The same for the pipelined sweeps (pipe_sweep_kernel, tile 2 x 128, 192^3): their TMA
+# boxes carry each tile's halo, so they read 10-14% more.
+SWEEP_TRAFFIC_PIPE = {0: 118.7, 1: 164.0, 2: 158.9}
 
 
 def sweep_flops_per_cell(d: int, scheme: str = "weno5z", riemann: str = "AUSM",
@@ -440,7 +449,7 @@ def ours(args):
     # the batched multi-block Navier-Stokes workload (24 uneven blocks) and the
     # shock-turbulence workload (plain against the learned hybrid), on this GPU
     launches = s.kernels_per_step() * args.steps
-    turb = shock = bl = None
+    turb = shock = bl = compact = None
     if world == 1 and not args.no_turbulence:
         s.close()
         try:
@@ -455,6 +464,10 @@ def ours(args):
             bl = boundary_layer(args)
         except Exception as e:
             bl = {"unavailable": f"{type(e).__name__}: {e}".splitlines()[0][:300]}
+        try:
+            compact = compact256(args)
+        except Exception as e:
+            compact = {"unavailable": f"{type(e).__name__}: {e}".splitlines()[0][:300]}
 
     line = {
         "metric": "Mcell-RK3-steps/s", "value": value, "unit": "Mcell-RK3-steps/s",
@@ -484,9 +497,10 @@ def ours(args):
             "peak_source": "measured live: libnuc3d_probe DFMA microbenchmark",
             "flops_per_cell": sweep_flops_per_cell(dom), "ms_per_launch": per[dom],
             "ms_per_launch_all": per,
-            "pipelined": pipelined,
+            "pipelined": bool((pipelined >> dom) & 1),
+            "pipelined_dirs": pipelined,
             "ms_per_launch_one_tile_per_cta": per_plain,
-            "traffic": (SWEEP_TRAFFIC[dom] * cells if SWEEP_TRAFFIC[dom] else None),
+            "traffic": ((SWEEP_TRAFFIC_PIPE if (pipelined >> dom) & 1 else SWEEP_TRAFFIC)[dom] * cells),
             "traffic_unit": "bytes per launch",
             "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
                     "frac": hbm_achieved / hbm_peak, "peak_source": hbm_src,
@@ -497,6 +511,7 @@ def ours(args):
         "turbulence24": turb,
         "shock_turbulence": shock,
         "boundary_layer": bl,
+        "compact": compact,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -575,6 +590,68 @@ def shock_turbulence(args, steps=10, warm=2):
             "sensor_training": "Taylor-Green vortex and spherical blast runs only (held out here)"}
 
 
+COMPACT_WORKLOAD = ("spherical Riemann 256^3, FP64 Euler, {scheme} in every direction, AUSM, "
+                    "outlet faces, TVD-RK3 CFL 0.5")
+
+
+def compact256(args, steps=10, warm=3):
+    """The bench workload with the compact schemes (crweno5, hccs) in every direction: the
+    throughput build's fused line sweep (compact_line_kernel, one kernel per direction)
+    against its three-kernel path (rows to HBM, Thomas per system, faces), step times and
+    the fused sweep's per-launch roofline."""
+    import torch
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+
+    torch.cuda.set_device(0)
+    q0, _ = C.spherical_riemann(SHAPE)
+    cells = int(np.prod(SHAPE))
+    stream = torch.cuda.Stream()
+    peak = nb.fp64_peak_tflops(0)
+    out = {}
+    for scheme in ("crweno5", "hccs"):
+        s = nb.Solver(nb.Config(scheme_ivs=(scheme,) * 3, riemann="AUSM", model="Euler3d", mach=1.0,
+                                cfl=0.5, exact=False))
+        b = s.add_block(*SHAPE, *C.outlet_faces())
+        s.set_nodes(b, *C.unit_box_nodes(SHAPE))
+        s.finalize()
+        s.set_stream(stream.cuda_stream)
+        res = {}
+        for fused in (True, False):
+            s.set_compact_solver(fused)
+            s.set_q(b, q0)
+            s.set_time(0.0)
+            s.step(warm)
+            s.sync()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with ClockSampler(0) as clk:
+                ev0.record(stream)
+                s.step(steps, sync=False)
+                ev1.record(stream)
+                ev1.synchronize()
+            s.sync()
+            ms = ev0.elapsed_time(ev1) / steps
+            per = [s.profile_sweep(d, reps=3) for d in range(3)]
+            res[fused] = {"value": cells / (ms * 1e-3) / 1e6, "ms_per_step": ms,
+                          "sweep_ms_per_launch": per, "kernels_per_step": s.kernels_per_step(),
+                          "clocks": clk.summary()}
+        s.close()
+        per = res[True]["sweep_ms_per_launch"]
+        dom = int(np.argmax(per))
+        f = sweep_flops_per_cell(dom, scheme=scheme)
+        achieved = f * cells / (per[dom] * 1e-3) / 1e12
+        out[scheme] = {
+            "workload": COMPACT_WORKLOAD.format(scheme=scheme), "unit": "Mcell-RK3-steps/s",
+            "fused": res[True], "three_kernels": res[False],
+            "vs_three_kernels": res[True]["value"] / res[False]["value"],
+            "roofline": {"bound": "fp64", "kernel": f"compact_line_kernel<{dom}> "
+                         f"({'xi eta zeta'.split()[dom]})", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "flops_per_cell": f,
+                         "peak_source": "measured live: libnuc3d_probe DFMA microbenchmark",
+                         "ms_per_launch": per[dom]}}
+    return out
+
+
 BL_WORKLOAD = ("supersonic flat-plate boundary layer, Ma 2.25, Re_x 1e5 at the inflow (Re_delta "
                "1581), isothermal wall T_w/T_inf 1.9, Gaussian bump h 0.5 delta w 2 delta, "
                "1024x256x128 cells on a tanh wall-normal stretched mesh in 4x2x2 = 16 uneven "
@@ -582,23 +659,18 @@ BL_WORKLOAD = ("supersonic flat-plate boundary layer, Ma 2.25, Re_x 1e5 at the i
                "WENO5-Z, AUSM, cd6, TVD-RK3 CFL 0.5")
 
 
-def boundary_layer(args, steps=10, warm=2, thresholds=(-4.0, -2.0, 0.0)):
-    """The boundary-layer workload on one GPU: the 16 blocks in one context (on-device ghost
-    copies, one launch per sweep over all blocks), metrics from the nodes on the device.
-    Plain WENO-Z, then the learned hybrid (batched over the same blocks) at each logit
-    threshold, all from the same state over the same steps; the volume-weighted L1 density
-    error of each against plain.  The error they are matched against is the L1 distance
-    between two plain fifth-order schemes (WENO5-JS against WENO5-Z) over the same steps:
-    a hybrid within it changes the solution less than the choice of WENO weights does."""
+def _bl_compare(shape, steps, warm, thresholds, autotune=True):
+    """Plain WENO-Z, the hybrid at each logit threshold and plain WENO5-JS on the
+    boundary-layer grid of `shape`, all from the same state over warm + steps steps: device
+    ms per step and, per variant, the volume-weighted L1 density distance from plain
+    WENO-Z (U/J = rho x cell volume, so the L1 norm of U/J is that of rho weighted by
+    volume)."""
     import torch
     import nuc3d_b200 as nb
     from nuc3d_b200 import cases as C
     from nuc3d_b200 import sensor as SENS
 
-    torch.cuda.set_device(0)
-    shape = (1024, 256, 128)
     blocks, types, ids, values, prm = C.boundary_layer(shape)
-    cells = int(np.prod(shape))
     stream = torch.cuda.Stream()
 
     def solver(scheme):
@@ -619,12 +691,15 @@ def boundary_layer(args, steps=10, warm=2, thresholds=(-4.0, -2.0, 0.0)):
         return s
 
     def run(s):
+        tiles = None
+        if autotune:
+            for r, b in enumerate(blocks):
+                s.set_q(r, b["q"])
+            s.set_time(0.0)
+            tiles = list(s.autotune(reps=2)["shape"])
         for r, b in enumerate(blocks):
             s.set_q(r, b["q"])
         s.set_time(0.0)
-        tiles = s.autotune(reps=2)["shape"]
-        for r, b in enumerate(blocks):
-            s.set_q(r, b["q"])
         s.step(warm)
         s.sync()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -633,41 +708,64 @@ def boundary_layer(args, steps=10, warm=2, thresholds=(-4.0, -2.0, 0.0)):
         ev1.record(stream)
         ev1.synchronize()
         s.sync()
-        ms = ev0.elapsed_time(ev1) / steps
-        # U/J = rho x cell volume: its L1 norm is the volume-weighted L1 norm of rho
         mass = np.concatenate([s.get_q(r)[0].ravel() for r in range(len(blocks))])
-        return ms, mass, list(tiles), s.status()
+        return {"ms_per_step": ev0.elapsed_time(ev1) / steps, "tile_shapes": tiles,
+                "status_bits": s.status(), "time": s.time_dt()[0]}, mass
 
     s = solver("weno5z")
-    ms_p, m_p, tiles_p, st_p = run(s)
+    plain, m_p = run(s)
     l1 = lambda m: float(np.abs(m - m_p).sum() / np.abs(m_p).sum())  # noqa: E731
     hyb = []
     for th in thresholds:
         s.set_sensor(SENS.load_weights(), th)
-        ms_h, m_h, tiles_h, _ = run(s)
-        hyb.append({"logit_threshold": th, "value": cells / (ms_h * 1e-3) / 1e6,
-                    "ms_per_step": ms_h, "vs_plain": ms_p / ms_h, "l1_density_error_vs_plain": l1(m_h),
-                    "tile_shapes": tiles_h})
+        h, m_h = run(s)
+        h.update(logit_threshold=th, vs_plain=plain["ms_per_step"] / h["ms_per_step"],
+                 l1_density_error_vs_plain=l1(m_h))
+        hyb.append(h)
         del m_h
     s.set_sensor(None)
     s.close()
     s = solver("weno5js")
-    ms_js, m_js, _, _ = run(s)
+    js, m_js = run(s)
     s.close()
-    target = l1(m_js)
-    ok = [h for h in hyb if h["l1_density_error_vs_plain"] <= target]
-    best = max(ok, key=lambda h: h["value"]) if ok else None
-    return {"workload": BL_WORKLOAD, "cells": cells, "blocks": len(blocks),
-            "block_shapes": [list(b["shape"]) for b in blocks], "steps_compared": warm + steps,
-            "plain": {"value": cells / (ms_p * 1e-3) / 1e6, "unit": "Mcell-RK3-steps/s",
-                      "ms_per_step": ms_p, "tile_shapes": tiles_p, "status_bits": st_p},
-            "hybrid": hyb,
-            "matched_error": {"target_l1": target,
-                              "target": "L1 density distance of plain WENO5-JS from plain WENO5-Z "
-                                        "over the same steps",
-                              "weno5js_ms_per_step": ms_js,
-                              "hybrid_at_target": best,
-                              "vs_plain": best["vs_plain"] if best else None},
+    js["l1_density_distance_vs_plain"] = l1(m_js)
+    return {"cells": int(np.prod(shape)), "blocks": len(blocks),
+            "block_shapes": [list(b["shape"]) for b in blocks], "steps": warm + steps,
+            "plain": plain, "hybrid": hyb, "weno5js": js}
+
+
+def boundary_layer(args, thresholds=(-4.0, -2.0, 0.0)):
+    """The boundary-layer workload on one GPU: the 16 blocks in one context (on-device ghost
+    copies, one launch per sweep over all blocks), metrics from the nodes on the device.
+    Throughput of plain WENO-Z and of the learned hybrid (batched over the same blocks) at
+    each logit threshold on the full 1024 x 256 x 128 grid over 12 steps.  Their accuracy
+    over a horizon in which the flow over the bump develops (800 steps; the line gives the
+    time reached, in delta / U_inf) on the same case at 256 x 64 x 32: the volume-weighted L1 density
+    distance of each hybrid from plain WENO-Z, matched against the distance between two
+    plain fifth-order schemes (WENO5-JS and WENO5-Z); a hybrid within it changes the
+    solution less than the choice of WENO weights does."""
+    full = _bl_compare((1024, 256, 128), 10, 2, thresholds)
+    small = _bl_compare((256, 64, 32), 790, 10, thresholds, autotune=False)
+    target = small["weno5js"]["l1_density_distance_vs_plain"]
+    ok = [k for k, h in enumerate(small["hybrid"]) if h["l1_density_error_vs_plain"] <= target]
+    best = max(ok, key=lambda k: full["hybrid"][k]["vs_plain"]) if ok else None
+    cells = full["cells"]
+    pv = cells / (full["plain"]["ms_per_step"] * 1e-3) / 1e6
+    return {"workload": BL_WORKLOAD, "cells": cells, "blocks": full["blocks"],
+            "block_shapes": full["block_shapes"], "steps_timed": 10,
+            "plain": dict(full["plain"], value=pv, unit="Mcell-RK3-steps/s"),
+            "hybrid": [dict(h, value=cells / (h["ms_per_step"] * 1e-3) / 1e6,
+                            l1_density_error_vs_plain_800_steps=small["hybrid"][k]["l1_density_error_vs_plain"])
+                       for k, h in enumerate(full["hybrid"])],
+            "weno5js": full["weno5js"],
+            "matched_error": {
+                "grid": "the same case at 256x64x32 cells (16 blocks), 800 steps, t = %.3g" % small["plain"]["time"],
+                "target_l1": target,
+                "target": "L1 density distance of plain WENO5-JS from plain WENO5-Z",
+                "hybrid_l1": [h["l1_density_error_vs_plain"] for h in small["hybrid"]],
+                "hybrid_at_target": ({"logit_threshold": thresholds[best],
+                                      "vs_plain": full["hybrid"][best]["vs_plain"]}
+                                     if best is not None else None)},
             "sensor_training": "Taylor-Green vortex and spherical blast runs only (held out here)",
             "metrics": "nuc3d_block_set_nodes (block::getJacobians on the device)"}
 
@@ -870,7 +968,8 @@ def main():
     ap.add_argument("--tiles", type=lambda x: tuple(int(v) for v in x.split(",")), default=None,
                     help="sweep tile shapes per direction, e.g. 2,0,0 (default: nuc3d_autotune)")
     ap.add_argument("--workload", default="sphere256",
-                    choices=["sphere256", "turbulence24", "shock_turbulence", "boundary_layer"],
+                    choices=["sphere256", "turbulence24", "shock_turbulence", "boundary_layer",
+                             "compact"],
                     help="turbulence24: the 24-block Navier-Stokes grid on one GPU; "
                          "shock_turbulence / boundary_layer: plain against hybrid on those "
                          "grids (our arm only)")
@@ -885,12 +984,13 @@ def main():
         return profile_case(args)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    if args.workload in ("shock_turbulence", "boundary_layer"):
+    if args.workload in ("shock_turbulence", "boundary_layer", "compact"):
         if args.impl == "reference" or args.gpus > 1:
             print(json.dumps({"impl": args.impl,
                               "unavailable": f"{args.workload} runs our arm on one GPU only"}))
             return 0
-        fn = shock_turbulence if args.workload == "shock_turbulence" else boundary_layer
+        fn = {"shock_turbulence": shock_turbulence, "boundary_layer": boundary_layer,
+              "compact": compact256}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return 0
     if args.workload == "turbulence24":

@@ -256,6 +256,19 @@ int nuc3d_autotune(nuc3d_ctx *ctx, int reps, int shape_out[3], double ms_out[9])
 int nuc3d_set_pipeline(nuc3d_ctx *ctx, int on);
 int nuc3d_get_pipeline(nuc3d_ctx *ctx, int *on);
 
+/* Line solver of the compact schemes (after nuc3d_finalize).  The reference solves each
+   line's tridiagonal system with the Thomas algorithm (src/crweno5.cpp:207-218,
+   src/hccs.cpp:252-264).  The reference-order build always does the same, in three
+   kernels per direction: rows to device memory, one thread per system, faces back.
+   The throughput build by default (fused = 1) runs crweno5 and hccs directions whose
+   lines have at most 256 cells in one kernel per direction: a CTA per line generates the
+   rows in shared memory and solves each system with one warp (partition method and
+   cyclic reduction), agreeing with Thomas to round-off.  fused = 0 selects the
+   three-kernel path there too.  nuc3d_get_compact_solver: the directions that run
+   fused (bit d). */
+int nuc3d_set_compact_solver(nuc3d_ctx *ctx, int fused);
+int nuc3d_get_compact_solver(nuc3d_ctx *ctx, int *dirs);
+
 /* Kernels one nuc3d_step(ctx, 1) launches (after nuc3d_finalize): per RK stage the BC
    ghost pass (when a block has a physical face), the NS primitive and gradient passes,
    and one sweep per direction (three kernels for a compact-scheme direction); then the

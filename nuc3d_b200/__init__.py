@@ -42,6 +42,7 @@ EXPORTED = (
     "nuc3d_sensor_loss_grad", "nuc3d_sensor_adam", "nuc3d_set_sensor", "nuc3d_set_tiles",
     "nuc3d_get_tiles", "nuc3d_autotune", "nuc3d_get_energy_resets", "nuc3d_set_pipeline",
     "nuc3d_get_pipeline", "nuc3d_rhs_stage", "nuc3d_rk_stage", "nuc3d_get_residual",
+    "nuc3d_set_compact_solver", "nuc3d_get_compact_solver",
 )
 
 
@@ -115,6 +116,8 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_get_energy_resets.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong)]
     lib.nuc3d_set_pipeline.argtypes = [P, I]
     lib.nuc3d_get_pipeline.argtypes = [P, ctypes.POINTER(I)]
+    lib.nuc3d_set_compact_solver.argtypes = [P, I]
+    lib.nuc3d_get_compact_solver.argtypes = [P, ctypes.POINTER(I)]
     lib.nuc3d_rhs_stage.argtypes = [P, I, PD]
     lib.nuc3d_rk_stage.argtypes = [P, I, D]
     lib.nuc3d_get_residual.argtypes = [P, PD]
@@ -359,11 +362,23 @@ class Solver:
         """Persistent TMA-fed sweeps on (default) or off; results are identical."""
         _check(self.lib.nuc3d_set_pipeline(self._ctx, 1 if on else 0))
 
-    def pipeline(self) -> bool:
-        """Whether the sweeps run pipelined (Euler, even nx, switched on)."""
+    def pipeline(self) -> int:
+        """Directions (bit d) whose sweeps run pipelined (Euler, even nx, switched on);
+        0 for none."""
         v = ctypes.c_int()
         _check(self.lib.nuc3d_get_pipeline(self._ctx, ctypes.byref(v)))
-        return bool(v.value)
+        return v.value
+
+    def set_compact_solver(self, fused: bool) -> None:
+        """Compact-scheme line solves fused into one kernel per direction (throughput build,
+        lines of at most 256 cells; the default) or rows, Thomas and faces in three."""
+        _check(self.lib.nuc3d_set_compact_solver(self._ctx, 1 if fused else 0))
+
+    def compact_solver(self) -> int:
+        """Directions (bit d) whose compact scheme runs the fused line kernel."""
+        v = ctypes.c_int()
+        _check(self.lib.nuc3d_get_compact_solver(self._ctx, ctypes.byref(v)))
+        return v.value
 
     def energy_resets(self) -> int:
         """Cells whose energy con2prim reset, once per cell and right-hand side, since the

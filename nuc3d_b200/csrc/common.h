@@ -75,8 +75,12 @@ struct BlockDev {
 // tile_l(s) cells along them; 0: 4 x 64, 1: 8 x 32, 2: 2 x 128.  All hold 256 cells, so
 // every sweep CTA has the same 288 threads.  Compact schemes use shape 0.
 constexpr int kTileShapes = 3;
-__host__ __device__ constexpr int tile_w(int s) { return s == 1 ? 8 : (s == 2 ? 2 : 4); }
-__host__ __device__ constexpr int tile_l(int s) { return s == 1 ? 32 : (s == 2 ? 128 : 64); }
+// Shape kLineShape (1 x 256, one whole line of at most 256 cells) is not an autotuner
+// choice: it is the tile of the fused compact sweep (compact_line_kernel).
+constexpr int kLineShape = 3;
+constexpr int kLineMax = 256;
+__host__ __device__ constexpr int tile_w(int s) { return s == 1 ? 8 : (s == 2 ? 2 : (s == 3 ? 1 : 4)); }
+__host__ __device__ constexpr int tile_l(int s) { return s == 1 ? 32 : (s == 2 ? 128 : (s == 3 ? 256 : 64)); }
 
 // Boxes of the pipelined sweep's tensor-map loads (pipe_sweep_kernel), for direction d, a
 // tile of tw lines x tl cells and a scheme reaching r cells: the halo box covers line
@@ -180,6 +184,8 @@ struct Launch {
   TileMap tm_dir[3];
   TileMap tm_sys[3];       // compact schemes: 256-system tiles per direction
   TileMap tm_cells;
+  TileMap tm_line[3];      // fused compact sweeps: one tile per line
+  int line_dirs;           // bit d: direction d's compact scheme runs compact_line_kernel
   const FaceJobs *d_jobs;  // device copy
   int bc_tiles;            // CTAs of the BC ghost pass (0: no physical faces)
   cudaStream_t stream;

@@ -1113,6 +1113,266 @@ compact_finish_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverPar
   if (st) atomicOr(&S->status, st);
 }
 
+#if NUC3D_FAST
+// ---------------------------------------------------------------------------------
+// Fused compact sweep (throughput build; crweno5 and hccs on lines of at most 256 cells).
+// One CTA per line, 10 warps: phase 1 splits the line into shared memory; warp s solves
+// the tridiagonal system of (variable s/2, split s%2) from those fluxes -- its rows are
+// generated where they are needed, never stored to HBM -- and the explicit faces; the
+// two splits are added; phase 3 as in the sweep.  The solve is the partition method
+// (Wang 1981) on 32 lanes: lane l owns a chunk of 2..8 consecutive rows, eliminates it
+// (forward to the chunk's first unknown, backward to its last) in registers, which leaves
+// two rows per lane coupling only chunk ends; the 64-row reduced system is solved by
+// parallel cyclic reduction (Hockney 1965) over warp shuffles (6 steps), and each lane
+// recovers its interior unknowns.  The operation order differs from the reference's
+// Thomas sweep (src/crweno5.cpp:207-218), so the results agree to round-off, not bits;
+// the reference-order build keeps compact_thomas_kernel.
+// ---------------------------------------------------------------------------------
+constexpr int kLineThreads = 320;  // 10 warps: one per (variable, split) system
+constexpr int kLineChunk = 8;      // rows per lane at most: systems of at most 256 rows
+
+// Normalised row (a, c, d with unit diagonal) of the reduced system, for the shuffles.
+struct PcrRow {
+  double a, c, d;
+};
+__device__ __forceinline__ PcrRow pcr_shfl_up(PcrRow r, int o, int lane) {
+  PcrRow x;
+  x.a = __shfl_up_sync(0xffffffffu, r.a, o);
+  x.c = __shfl_up_sync(0xffffffffu, r.c, o);
+  x.d = __shfl_up_sync(0xffffffffu, r.d, o);
+  if (lane < o) x.a = x.c = x.d = 0.0;  // beyond the system's first row: an identity row
+  return x;
+}
+__device__ __forceinline__ PcrRow pcr_shfl_down(PcrRow r, int o, int lane) {
+  PcrRow x;
+  x.a = __shfl_down_sync(0xffffffffu, r.a, o);
+  x.c = __shfl_down_sync(0xffffffffu, r.c, o);
+  x.d = __shfl_down_sync(0xffffffffu, r.d, o);
+  if (lane + o > 31) x.a = x.c = x.d = 0.0;
+  return x;
+}
+// One cyclic-reduction update of row (a, b, c, d) from its normalised neighbours lo
+// (the row s above) and hi (the row s below): the result couples rows 2s away.
+__device__ __forceinline__ void pcr_update(double &a, double &b, double &c, double &d, PcrRow lo,
+                                           PcrRow hi) {
+  const double na = -a * lo.a, nc = -c * hi.c;
+  b = b - a * lo.c - c * hi.a;
+  d = d - a * lo.d - c * hi.d;
+  a = na;
+  c = nc;
+}
+__device__ __forceinline__ PcrRow pcr_norm(double a, double b, double c, double d) {
+  const double r = qdiv(1.0, b);
+  return PcrRow{a * r, c * r, d * r};
+}
+
+// Solve the m-row tridiagonal system row(r, a, b, c, d) (a of row 0 and c of row m-1
+// zero), 2 <= m <= 32 * kLineChunk, with the 32 lanes of this warp; out(r, x) receives
+// every unknown once.
+template <class RowF, class OutF>
+__device__ __forceinline__ void warp_tridiag(int m, RowF row, OutF out) {
+  const int lane = threadIdx.x & 31;
+  const int np = min(32, m >> 1);  // active lanes, each with >= 2 rows
+  const int q = m / np, rem = m - q * np;
+  const bool act = lane < np;
+  const int r0 = lane * q + min(lane, rem);
+  const int kk = act ? q + (lane < rem ? 1 : 0) : 0;
+  double A[kLineChunk], C[kLineChunk], D[kLineChunk];
+  // the lane's two rows of the reduced system: F (its first unknown: couples the previous
+  // lane's last and its own last) and L (its last: couples its own first and the next
+  // lane's first); inactive lanes hold identity rows
+  double fa = 0.0, fb = 1.0, fc = 0.0, fd = 0.0, la = 0.0, lb = 1.0, lc = 0.0, ld = 0.0;
+  // forward: row j becomes x_j + A_j x_first + C_j x_{j+1} = D_j (row 0 keeps its a,
+  // the coupling to the previous chunk's last unknown).  The last row's values are final
+  // here: L takes each valid row's in turn (no select by kk, which the compiler would
+  // turn into an indexed, local-memory load).
+#pragma unroll
+  for (int j = 0; j < kLineChunk; ++j) {
+    A[j] = C[j] = D[j] = 0.0;
+    if (j < kk) {
+      double a, b, c, d;
+      row(r0 + j, a, b, c, d);
+      if (j < 2) {
+        const double r = qdiv(1.0, b);
+        A[j] = a * r;
+        C[j] = c * r;
+        D[j] = d * r;
+      } else {
+        const double r = qdiv(1.0, b - a * C[j - 1]);
+        A[j] = -r * a * A[j - 1];
+        C[j] = r * c;
+        D[j] = r * (d - a * D[j - 1]);
+      }
+      la = A[j];
+      lc = C[j];
+      ld = D[j];
+    }
+  }
+  // backward: rows 1 .. kk-2 become x_j + A_j x_first + C_j x_last = D_j
+#pragma unroll
+  for (int j = kLineChunk - 3; j >= 1; --j) {
+    if (j <= kk - 3) {
+      A[j] = A[j] - C[j] * A[j + 1];
+      D[j] = D[j] - C[j] * D[j + 1];
+      C[j] = -C[j] * C[j + 1];
+    }
+  }
+  if (act) {
+    if (kk >= 3) {
+      const double r = qdiv(1.0, 1.0 - C[0] * A[1]);
+      fa = r * A[0];
+      fc = -r * C[0] * C[1];
+      fd = r * (D[0] - C[0] * D[1]);
+    } else {
+      fa = A[0];
+      fc = C[0];
+      fd = D[0];
+    }
+  }
+  // cyclic reduction over the 64 reduced rows (row 2l = F of lane l, 2l+1 = L of lane l)
+  {
+    const PcrRow nf = pcr_norm(fa, fb, fc, fd), nl = pcr_norm(la, lb, lc, ld);
+    const PcrRow lo = pcr_shfl_up(nl, 1, lane), hi = pcr_shfl_down(nf, 1, lane);
+    pcr_update(fa, fb, fc, fd, lo, nl);
+    pcr_update(la, lb, lc, ld, nf, hi);
+  }
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const PcrRow nf = pcr_norm(fa, fb, fc, fd), nl = pcr_norm(la, lb, lc, ld);
+    const PcrRow flo = pcr_shfl_up(nf, o, lane), fhi = pcr_shfl_down(nf, o, lane);
+    const PcrRow llo = pcr_shfl_up(nl, o, lane), lhi = pcr_shfl_down(nl, o, lane);
+    pcr_update(fa, fb, fc, fd, flo, fhi);
+    pcr_update(la, lb, lc, ld, llo, lhi);
+  }
+  if (!act) return;
+  const double xf = qdiv(fd, fb), xl = qdiv(ld, lb);
+  out(r0, xf);
+#pragma unroll
+  for (int j = 1; j < kLineChunk - 1; ++j)
+    if (j < kk - 1) out(r0 + j, D[j] - A[j] * xf - C[j] * xl);
+  out(r0 + kk - 1, xl);
+}
+
+// Row (a, b, c, d) of face f of one line's system from the split fluxes A(c) = rowF[c]:
+// the compact row (src/crweno5.cpp:124-199, src/hccs.cpp:145-188 and their F- mirrors), or
+// at the system's end rows the explicit interior reconstruction.
+struct LineRow {
+  double a, b, c, d;
+};
+template <int SCH>
+__device__ __forceinline__ LineRow line_row(const double *rowF, int f, int side, bool end) {
+  auto A = [rowF](int c) { return rowF[c]; };
+  LineRow q;
+  if (end) {
+    q.a = 0.0;
+    q.b = 1.0;
+    q.c = 0.0;
+    q.d = side ? recon_neg_in<SCH>(f, A) : recon_pos_in<SCH>(f, false, A);
+    return q;
+  }
+  double s5[5];
+  if (side) { s5[0] = A(f + 2); s5[1] = A(f + 1); s5[2] = A(f); s5[3] = A(f - 1); s5[4] = A(f - 2); }
+  else { s5[0] = A(f - 3); s5[1] = A(f - 2); s5[2] = A(f - 1); s5[3] = A(f); s5[4] = A(f + 1); }
+  double lo, di, up;
+  compact_row<SCH>(s5, lo, di, up, q.d);
+  q.b = di;
+  if (side) { q.a = up; q.c = lo; } else { q.a = lo; q.c = up; }
+  return q;
+}
+
+// The line of tile t (lines numbered lane-fastest, then outer index).
+template <int DIR>
+__device__ __forceinline__ TileCtx decode_line(const BlockDev *__restrict__ blocks, const TileMap &tm,
+                                               const SolverParams &P) {
+  TileCtx T;
+  T.t = (int)blockIdx.x;
+  T.b = find_block(tm, T.t);
+  T.B = &blocks[T.b];
+  for (int d = 0; d < 3; ++d) T.n[d] = T.B->n[d];
+  T.G = make_geo(DIR, T.n);
+  const int lt = T.t - tm.tile_start[T.b];
+  T.o = lt / T.G.nW;
+  T.w0 = lt - T.o * T.G.nW;
+  T.nw = 1;
+  T.c0 = 0;
+  T.cl = T.G.L;
+  T.N = T.B->N;
+  T.ts = P.ts[DIR];
+  T.physL = T.B->face[2 * DIR].type < 0;
+  T.physR = T.B->face[2 * DIR + 1].type < 0;
+  return T;
+}
+
+template <int DIR, int SCH>
+__host__ __device__ inline size_t compact_line_smem_bytes(bool ns) {
+  using M = TileSmem<DIR, SCH, kLineShape>;
+  size_t n = (size_t)10 * M::SP + (size_t)10 * M::SH;
+  if (ns) n += (size_t)4 * M::SV;
+  if (DIR == 2) n += (size_t)5 * M::SQ;
+  return n * sizeof(double);
+}
+
+template <int DIR, int SCH>
+__global__ void __launch_bounds__(kLineThreads, 2)
+compact_line_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
+                    int stage, int flags) {
+  using M = TileSmem<DIR, SCH, kLineShape>;
+  constexpr int R = M::R, SP = M::SP, SH = M::SH, SV = M::SV;
+  static_assert(M::TL >= kLineMax && M::TW == 1, "one whole line per CTA");
+  extern __shared__ double smem[];
+  double *sF = smem;           // [10][SP] split fluxes; later [5][SH] the face values
+  double *sX = sF + 10 * SP;   // [10][SH] each system's solution and explicit faces
+  const bool ns = (flags & SW_NS) != 0;
+  double *sV = sX + 10 * SH;   // [4][SV] viscous fluxes (NS)
+  double *sQ = sV + (ns ? 4 * SV : 0);  // [5][SQ] zeta: the stage state of the line
+  __shared__ double sRed[kLineThreads / 32];
+  const TileCtx T = decode_line<DIR>(blocks, tm, P);
+  const bool eig = (flags & SW_EIG) != 0;
+  unsigned st = 0, nres = 0;
+  double emax = 0.0;
+  // phases 1 and 3 run on the first kThreads threads in one round (the line's
+  // positions number at most kThreads); warp 9 joins the solve and the barriers
+  phase_split<DIR, SCH, false, kLineShape>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st,
+                                           emax, nullptr, DIR == 0 ? &nres : nullptr);
+  if (ns) phase_vis<DIR, SCH, kLineShape>(blocks, T, P, sV);
+  __syncthreads();
+  {
+    const int sys = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int v = sys >> 1, side = sys & 1;
+    const double *rowF = sF + (side ? 5 + v : v) * SP + R;  // c0 = 0
+    auto A = [rowF](int c) { return rowF[c]; };
+    double *x = sX + sys * SH;
+    const int L = T.G.L, ts = T.ts, m = L - 2 * ts + 1;
+    // explicit faces next to the block edges (f < ts, f > L - ts)
+    if (lane < 2 * ts) {
+      const int f = lane < ts ? lane : L - 2 * ts + 1 + lane;
+      x[f] = side ? recon_neg<SCH>(f, L, ts, T.physL, T.physR, A)
+                  : recon_pos<SCH>(f, L, ts, T.physL, T.physR, false, A);
+    }
+    auto row = [&](int r, double &a, double &b, double &c, double &d) {
+      const LineRow q = line_row<SCH>(rowF, ts + r, side, r == 0 || r == m - 1);
+      a = q.a;
+      b = q.b;
+      c = q.c;
+      d = q.d;
+    };
+    auto out = [x, ts](int r, double val) { x[ts + r] = val; };
+    warp_tridiag(m, row, out);
+  }
+  __syncthreads();
+  double *sH = sF;
+  for (int e = threadIdx.x; e < 5 * (T.G.L + 1); e += kLineThreads) {
+    const int v = e / (T.G.L + 1), f = e - v * (T.G.L + 1);
+    sH[v * SH + f] = sX[(2 * v) * SH + f] + sX[(2 * v + 1) * SH + f];
+  }
+  __syncthreads();
+  phase_cells<DIR, SCH, kLineShape>(T, P, S, stage, flags & ~SW_EIG, sH, sV, sQ, st, sRed);
+  if (eig) reduce_eig(emax, sRed, S);
+  if (st) atomicOr(&S->status, st);
+  if (nres) atomicAdd(&S->reset_cells, (unsigned long long)nres);
+}
+#endif  // NUC3D_FAST
+
 // ---------------------------------------------------------------------------------
 // Physical-face ghost fluxes: the reference's setBC (src/boundaryConditions.cpp:95-108)
 // fills the ghost slabs before its sweeps; here one thread per face cell evaluates
@@ -1754,6 +2014,16 @@ __host__ __device__ inline size_t compact_finish_smem_bytes(bool ns) {
 
 template <int DIR, int SCH, bool WHOLE = false>
 inline cudaError_t launch_compact_t(const Launch &L, int stage, int flags) {
+#if NUC3D_FAST
+  if (!WHOLE && ((L.line_dirs >> DIR) & 1)) {
+    const int nlines = L.tm_line[DIR].tile_start[L.tm_line[DIR].nblocks];
+    compact_line_kernel<DIR, SCH><<<nlines, kLineThreads,
+                                    compact_line_smem_bytes<DIR, SCH>((flags & SW_NS) != 0),
+                                    L.stream>>>(L.d_blocks, L.tm_line[DIR], L.P, L.d_state, stage,
+                                                flags);
+    return cudaGetLastError();
+  }
+#endif
   const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
   compact_rows_kernel<DIR, SCH, WHOLE>
       <<<ntiles, kThreads, compact_rows_smem_bytes<DIR, SCH>(), L.stream>>>(
@@ -1818,8 +2088,11 @@ cudaError_t run_residual(const Launch &L, bool cells) {
   cudaError_t e = cudaMemsetAsync(&L.d_state->res_bits, 0, sizeof(unsigned long long), L.stream);
   if (e != cudaSuccess) return e;
 #if NUC3D_FAST
-  residual_part_kernel<<<nb, 256, 0, L.stream>>>(L.d_blocks, cells ? L.tm_cells : L.tm_dir[2],
-                                                 L.P.res_part, L.d_res_last, L.d_state);
+  // the partial sums are per tile of the kernel that applied the last stage
+  const bool line = (L.line_dirs >> 2) & 1;
+  residual_part_kernel<<<nb, 256, 0, L.stream>>>(
+      L.d_blocks, cells ? L.tm_cells : (line ? L.tm_line[2] : L.tm_dir[2]), L.P.res_part,
+      L.d_res_last, L.d_state);
 #else
   (void)cells;
   residual_seq_kernel<<<nb, 256, 0, L.stream>>>(L.d_blocks, L.d_res_last, L.d_state);
@@ -1954,6 +2227,11 @@ inline cudaError_t configure_compact_t() {
                              (int)compact_rows_smem_bytes<DIR, SCH>());
     if (e != cudaSuccess) return e;
   }
+#if NUC3D_FAST
+  e = cudaFuncSetAttribute(compact_line_kernel<DIR, SCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)compact_line_smem_bytes<DIR, SCH>(true));
+  if (e != cudaSuccess) return e;
+#endif
   return cudaFuncSetAttribute(compact_finish_kernel<DIR, SCH>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)compact_finish_smem_bytes<DIR, SCH>(true));

@@ -118,6 +118,7 @@ struct nuc3d_ctx {
   // pipelined sweeps: tensor maps of every block and direction (built by build_maps)
   bool use_pipe = true;
   int pipe_mask = 7;  // directions to run pipelined where the grid allows (bit d)
+  bool compact_fused = true;  // throughput build: compact directions on compact_line_kernel
   CUtensorMap *d_maps = nullptr;
   // the residual of each step: per-tile partial sums, each block's previous residual root
   double *d_res_part = nullptr, *d_res_last = nullptr;
@@ -508,6 +509,22 @@ int build_maps(nuc3d_ctx *c) {
 
 extern "C" {
 
+// Directions whose compact scheme (crweno5, hccs; not the whole-line hccs77 system) runs
+// the fused compact_line_kernel: the throughput build, every block's line at most
+// kLineMax cells with at least 2 rows in its system.
+static void set_line_dirs(nuc3d_ctx *c) {
+  int dirs = 0;
+  for (int d = 0; d < 3 && !c->exact && c->compact_fused; ++d) {
+    const int sc = c->P.scheme[d];
+    if (sc != SCH_CRWENO5 && sc != SCH_HCCS) continue;
+    bool ok = true;
+    for (const HostBlock &b : c->blocks)
+      ok = ok && b.n[d] <= kLineMax && b.n[d] - 2 * c->P.ts[d] + 1 >= 2;
+    if (ok) dirs |= 1 << d;
+  }
+  c->L.line_dirs = dirs;
+}
+
 int nuc3d_finalize(nuc3d_ctx *c) {
   if (!c) return fail(NUC3D_EINVAL, "null context");
   if (c->finalized) return fail(NUC3D_ESTATE, "already finalized");
@@ -584,6 +601,8 @@ int nuc3d_finalize(nuc3d_ctx *c) {
     L.tm_dir[d].tile_start[0] = 0;
     L.tm_sys[d].nblocks = nbk;
     L.tm_sys[d].tile_start[0] = 0;
+    L.tm_line[d].nblocks = nbk;
+    L.tm_line[d].tile_start[0] = 0;
   }
   L.tm_cells.nblocks = nbk;
   L.tm_cells.tile_start[0] = 0;
@@ -594,6 +613,7 @@ int nuc3d_finalize(nuc3d_ctx *c) {
           L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, b.n, L.shape[d]);
       const long long nsys = 10 * (b.N / b.n[d]);
       L.tm_sys[d].tile_start[bi + 1] = L.tm_sys[d].tile_start[bi] + (int)((nsys + 255) / 256);
+      L.tm_line[d].tile_start[bi + 1] = L.tm_line[d].tile_start[bi] + (int)(b.N / b.n[d]);
     }
     L.tm_cells.tile_start[bi + 1] = L.tm_cells.tile_start[bi] + (int)((b.N + 255) / 256);
   }
@@ -618,9 +638,11 @@ int nuc3d_finalize(nuc3d_ctx *c) {
   CUDA_TRY(cudaMalloc(&c->d_jobs, sizeof(FaceJobs)));
   CUDA_TRY(cudaMemcpy(c->d_jobs, &J, sizeof(FaceJobs), cudaMemcpyHostToDevice));
   L.d_jobs = c->d_jobs;
-  // residual workspace: one partial sum per zeta tile (any tile shape) or per cell tile
+  set_line_dirs(c);
+  // residual workspace: one partial sum per zeta tile (any tile shape, or per line of the
+  // fused compact sweep) or per cell tile
   {
-    long long nt = L.tm_cells.tile_start[nbk];
+    long long nt = std::max(L.tm_cells.tile_start[nbk], L.tm_line[2].tile_start[nbk]);
     for (int sh = 0; sh < kTileShapes; ++sh) {
       long long z = 0;
       for (int bi = 0; bi < nbk; ++bi) z += nuc3d::exact::tile_count(2, c->blocks[bi].n, sh);
@@ -1178,8 +1200,8 @@ int nuc3d_kernels_per_step(nuc3d_ctx *c, int *kernels) {
   const Launch &L = c->L;
   int per_stage = (L.bc_tiles > 0 ? 1 : 0) + (L.P.model == MODEL_NS ? 2 : 0);
   for (int d = 0; d < 3; ++d)
-    per_stage += (L.P.scheme[d] == SCH_CRWENO5 || L.P.scheme[d] == SCH_HCCS ||
-                  L.P.scheme[d] == SCH_HCCS77) ? 3 : 1;
+    per_stage += ((L.P.scheme[d] == SCH_CRWENO5 || L.P.scheme[d] == SCH_HCCS ||
+                   L.P.scheme[d] == SCH_HCCS77) && !((L.line_dirs >> d) & 1)) ? 3 : 1;
   *kernels = 3 * per_stage + (L.d_res_last ? 1 : 0);  // + the residual after the last stage
   return NUC3D_OK;
 }
@@ -1193,6 +1215,23 @@ int nuc3d_set_pipeline(nuc3d_ctx *c, int on) {
   c->pipe_mask = on ? 7 : 0;
   c->drop_graph();
   return build_maps(c);
+}
+
+int nuc3d_set_compact_solver(nuc3d_ctx *c, int fused) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->compact_fused = fused != 0;
+  c->drop_graph();
+  set_line_dirs(c);
+  return NUC3D_OK;
+}
+
+int nuc3d_get_compact_solver(nuc3d_ctx *c, int *dirs) {
+  if (!c || !dirs) return fail(NUC3D_EINVAL, "null argument");
+  *dirs = c->L.line_dirs;
+  return NUC3D_OK;
 }
 
 int nuc3d_get_pipeline(nuc3d_ctx *c, int *on) {

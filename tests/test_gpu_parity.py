@@ -114,16 +114,22 @@ def test_two_blocks_equal_one(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name,expected", [                # + 1: the step's residual
-    ("sphere_euler_weno5z_ausm_outlet", 3 * (1 + 3) + 1),      # BC pass + 3 sweeps
-    ("tgv_ns_weno5js_lf", 3 * (2 + 3) + 1),                    # periodic: NS passes + 3 sweeps
-    ("hccs_ns_ausm_bc", 3 * (1 + 2 + 3 * 3) + 1),              # compact: 3 kernels per direction
-    ("mixed_compact_ausmp", 3 * (1 + 3 + 3 + 1) + 1),          # crweno5, hccs, weno5z
-    ("mixed_hccs77_euler_ausmp", 3 * (1 + 3 + 1 + 3) + 1),     # hccs77, weno5z, hccs77
+@pytest.mark.parametrize("name,exact,fast", [                 # + 1: the step's residual
+    ("sphere_euler_weno5z_ausm_outlet", 3 * (1 + 3) + 1, 3 * (1 + 3) + 1),  # BC pass + 3 sweeps
+    ("tgv_ns_weno5js_lf", 3 * (2 + 3) + 1, 3 * (2 + 3) + 1),  # periodic: NS passes + 3 sweeps
+    # compact: rows, Thomas, faces per direction; the throughput build fuses them
+    ("hccs_ns_ausm_bc", 3 * (1 + 2 + 3 * 3) + 1, 3 * (1 + 2 + 3) + 1),
+    ("mixed_compact_ausmp", 3 * (1 + 3 + 3 + 1) + 1, 3 * (1 + 3) + 1),  # crweno5, hccs, weno5z
+    ("mixed_hccs77_euler_ausmp", 3 * (1 + 3 + 1 + 3) + 1,     # hccs77 (one whole-line system,
+     3 * (1 + 3 + 1 + 3) + 1),                                # never fused), weno5z, hccs77
 ])
-def test_kernels_per_step(name, expected):
+def test_kernels_per_step(name, exact, fast):
     g = G.load(name)
-    assert G.solver(g, exact=False).kernels_per_step() == expected
+    assert G.solver(g, exact=True).kernels_per_step() == exact
+    s = G.solver(g, exact=False)
+    assert s.kernels_per_step() == fast
+    s.set_compact_solver(False)
+    assert s.kernels_per_step() == exact
 
 
 def _two_rank_solver(g, exact):
