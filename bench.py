@@ -574,6 +574,16 @@ def shock_turbulence(args, steps=10, warm=2):
     ms_p, rho_p, tiles_p = run("plain")
     s.set_sensor(SENS.load_weights(), SENS.DEFAULT_THRESHOLD)
     ms_h, rho_h, tiles_h = run("hybrid")
+    # the same hybrid deciding by hccs's hand-made theta switch instead of the network
+    theta = []
+    for tmin in (0.5, 0.9):
+        s.set_sensor_theta(tmin)
+        ms_t, rho_t, tiles_t = run("theta")
+        theta.append({"theta_min": tmin, "value": cells / (ms_t * 1e-3) / 1e6, "ms_per_step": ms_t,
+                      "vs_plain": ms_p / ms_t, "tile_shapes": list(tiles_t),
+                      "l1_density_error_vs_plain": float(np.abs(rho_t - rho_p).sum() / np.abs(rho_p).sum()),
+                      "shock_x": C.shock_position(rho_t, h)})
+        del rho_t
     s.set_sensor(None)
     s.close()
     vp = cells / (ms_p * 1e-3) / 1e6
@@ -587,15 +597,21 @@ def shock_turbulence(args, steps=10, warm=2):
             "l1_density_error_vs_plain": float(np.abs(rho_h - rho_p).sum() / np.abs(rho_p).sum()),
             "shock_x": {"initial": 0.5 * math.pi, "plain": C.shock_position(rho_p, h),
                         "hybrid": C.shock_position(rho_h, h)},
+            "theta_switch": theta,
+            "theta_switch_rule": "linear weights where the smallest hccs theta "
+                                 "(src/hccs.cpp:177-181) of the face's density and pressure "
+                                 "stencils, both splits, is at least theta_min",
             "sensor_training": "Taylor-Green vortex and spherical blast runs only (held out here)"}
 
 
-COMPACT_WORKLOAD = ("spherical Riemann 256^3, FP64 Euler, {scheme} in every direction, AUSM, "
-                    "outlet faces, TVD-RK3 CFL 0.5")
+COMPACT_WORKLOAD = ("smooth isentropic pressure pulse 256^3 (rho = 1 + 0.5 exp(-r^2/0.08^2), "
+                    "p = rho^1.4/1.4, at rest; the blast's discontinuity drives the compact schemes "
+                    "to negative pressure), FP64 Euler, {scheme} in every direction, AUSM, outlet "
+                    "faces, TVD-RK3 CFL 0.5")
 
 
 def compact256(args, steps=10, warm=3):
-    """The bench workload with the compact schemes (crweno5, hccs) in every direction: the
+    """The compact schemes (crweno5, hccs) in every direction on a 256^3 Euler block: the
     throughput build's fused line sweep (compact_line_kernel, one kernel per direction)
     against its three-kernel path (rows to HBM, Thomas per system, faces), step times and
     the fused sweep's per-launch roofline."""
@@ -604,7 +620,7 @@ def compact256(args, steps=10, warm=3):
     from nuc3d_b200 import cases as C
 
     torch.cuda.set_device(0)
-    q0, _ = C.spherical_riemann(SHAPE)
+    q0, _ = C.gaussian_pulse(SHAPE)
     cells = int(np.prod(SHAPE))
     stream = torch.cuda.Stream()
     peak = nb.fp64_peak_tflops(0)

@@ -226,6 +226,12 @@ int nuc3d_sensor_adam(float *params, const float *grad, float *m, float *v, floa
    params: NUC3D_SENSOR_PARAMS floats (copied, rounded to BF16 as in the training), or
    NULL to return to plain WENO-Z. */
 int nuc3d_set_sensor(nuc3d_ctx *ctx, const float *params, float logit_threshold);
+/* The same hybrid with the hand-made decision of the reference's hybrid compact scheme
+   instead of the network: theta = 1 / (1 + (sum_k alpha_k - 1)^2) of CRWENO5-Z weights
+   (src/hccs.cpp:154-181), evaluated on the face's density and pressure stencils (both
+   splits); a face takes the linear weights where the smallest of the four thetas is at
+   least theta_min.  nuc3d_set_sensor(ctx, NULL, 0) returns to plain WENO-Z. */
+int nuc3d_set_sensor_theta(nuc3d_ctx *ctx, float theta_min);
 
 /* ---- Sweep tile shapes (after nuc3d_finalize) ----------------------------------------
    No counterpart in the reference.  Each direction's sweep runs tiles of one of

@@ -42,7 +42,7 @@ EXPORTED = (
     "nuc3d_sensor_loss_grad", "nuc3d_sensor_adam", "nuc3d_set_sensor", "nuc3d_set_tiles",
     "nuc3d_get_tiles", "nuc3d_autotune", "nuc3d_get_energy_resets", "nuc3d_set_pipeline",
     "nuc3d_get_pipeline", "nuc3d_rhs_stage", "nuc3d_rk_stage", "nuc3d_get_residual",
-    "nuc3d_set_compact_solver", "nuc3d_get_compact_solver",
+    "nuc3d_set_compact_solver", "nuc3d_get_compact_solver", "nuc3d_set_sensor_theta",
 )
 
 
@@ -117,6 +117,7 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_set_pipeline.argtypes = [P, I]
     lib.nuc3d_get_pipeline.argtypes = [P, ctypes.POINTER(I)]
     lib.nuc3d_set_compact_solver.argtypes = [P, I]
+    lib.nuc3d_set_sensor_theta.argtypes = [P, ctypes.c_float]
     lib.nuc3d_get_compact_solver.argtypes = [P, ctypes.POINTER(I)]
     lib.nuc3d_rhs_stage.argtypes = [P, I, PD]
     lib.nuc3d_rk_stage.argtypes = [P, I, D]
@@ -428,6 +429,11 @@ class Solver:
         self._sensor_keep = p
         _check(self.lib.nuc3d_set_sensor(self._ctx, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                          float(logit_threshold)))
+
+    def set_sensor_theta(self, theta_min: float) -> None:
+        """Hybrid WENO-Z deciding by hccs's theta switch: linear weights where the face's
+        smallest density/pressure theta is at least theta_min (set_sensor(None): plain)."""
+        _check(self.lib.nuc3d_set_sensor_theta(self._ctx, float(theta_min)))
 
     def set_tiles(self, shape) -> None:
         """Sweep tile shape per direction: 0 = 4 x 64, 1 = 8 x 32, 2 = 2 x 128."""

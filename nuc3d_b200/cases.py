@@ -75,6 +75,20 @@ def spherical_riemann(shape, gamma=1.4, radius=0.2):
     return prim_to_q(np.stack([rho, zero, zero, zero, p]), m["jac"], gamma), m
 
 
+def gaussian_pulse(shape, gamma=1.4, amp=0.5, width=0.08):
+    """Smooth isentropic pressure pulse at rest in the unit box: rho = 1 + amp g,
+    p = rho^gamma / gamma, g = exp(-r^2 / width^2) about the centre (sound speed 1 in the
+    far field).  A case the compact schemes resolve without the oscillations a
+    discontinuity gives them."""
+    X, Y, Z = centres(shape)
+    g = np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2) / (width * width))
+    rho = 1.0 + amp * g
+    p = rho ** gamma / gamma
+    zero = np.zeros_like(rho)
+    m = uniform_metrics(shape)
+    return prim_to_q(np.stack([rho, zero, zero, zero, p]), m["jac"], gamma), m
+
+
 def taylor_green(shape, gamma=1.4, mach=0.1):
     lo, hi = (0.0,) * 3, (2.0 * math.pi,) * 3
     X, Y, Z = centres(shape, lo, hi)

@@ -151,6 +151,8 @@ struct SolverParams {
   double gamma, mach, reynolds, prandtl, t_ref, t_inf, t_wall, cfl;
   const SensorDev *sensor;  // hybrid WENO-Z: the face sensor, or null (plain WENO-Z)
   float sensor_threshold;   // logit below which a face takes the linear weights
+  int sensor_theta;         // 1: decide by hccs's theta switch instead of the network;
+                            // a face takes the linear weights where theta >= sensor_threshold
   double *res_part;         // throughput build: per-tile sums of (u - u_n)^2 of the step's
                             // last stage, for the residual (Launch::d_res_part)
 };

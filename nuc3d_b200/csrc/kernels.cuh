@@ -754,6 +754,26 @@ __device__ __forceinline__ void reduce_eig(double emax, double *sRed, StepState 
 #include "sensor.cuh"
 #include "sweep_pipe.cuh"
 
+// hccs's smoothness switch theta = 1 / (1 + (sum alpha - 1)^2), alpha_k the CRWENO5-Z
+// weights' numerators with eps 1e-40 (src/hccs.cpp:154-181), of one 5-point stencil.
+__device__ __forceinline__ double theta_stencil(double f0, double f1, double f2, double f3, double f4) {
+  const W5 r = w5_parts(f0, f1, f2, f3, f4, false);
+  const double ss = 1.0e-40, tau = fabs(r.is2 - r.is0);
+  const double s = kCR5[0] * (1.0 + sq(tau / (r.is0 + ss))) + kCR5[1] * (1.0 + sq(tau / (r.is1 + ss))) +
+                   kCR5[2] * (1.0 + sq(tau / (r.is2 + ss)));
+  return 1.0 / (1.0 + sq(s - 1.0));
+}
+// The theta switch as a face decision of the hybrid sweep: the smallest theta of the
+// face's density and pressure over its positive (f-3 .. f+1) and negative (f+2 .. f-2)
+// stencils; rho, p point at the face's position (the cell after it).
+__device__ __forceinline__ double theta_face(const double *rho, const double *p) {
+  const double a = theta_stencil(rho[-3], rho[-2], rho[-1], rho[0], rho[1]);
+  const double b = theta_stencil(rho[2], rho[1], rho[0], rho[-1], rho[-2]);
+  const double c = theta_stencil(p[-3], p[-2], p[-1], p[0], p[1]);
+  const double d = theta_stencil(p[2], p[1], p[0], p[-1], p[-2]);
+  return fmin(fmin(a, b), fmin(c, d));
+}
+
 // Explicit-scheme sweep: phases split -> faces -> cells in one CTA.  HYB: the hybrid
 // WENO-Z face loop of the throughput build (P.sensor set).
 template <int DIR, int SCH, bool HYB = false, int SHP = 0>
@@ -845,11 +865,19 @@ sweep_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, St
       nonzero |= zero ? 0 : 1;
     }
     // A tile whose every gap is zero (inside a uniform region) has all-zero features on
-    // every face: each face's decision is the network's zero-input one, and 1b is skipped.
+    // every face: each face's decision is the network's zero-input one (the theta switch's:
+    // theta = 1 on a uniform stencil), and 1b is skipped.
     hyb_any = __syncthreads_or(nonzero) != 0;
-    hyb_lin0 = sS->zero_logit < P.sensor_threshold;
-    // 1b: features, network, decision
-    if (hyb_any)
+    hyb_lin0 = P.sensor_theta ? 1.0f >= P.sensor_threshold : sS->zero_logit < P.sensor_threshold;
+    // 1b: features, network, decision; or hccs's theta switch on density and pressure
+    if (hyb_any && P.sensor_theta) {
+      for (int e = threadIdx.x; e < ei; e += kThreads) {
+        const int w = __float2int_rz(((float)e + 0.5f) * rni), fl = lo + (e - w * ni);
+        if (w < T.nw)
+          sLin[e] = theta_face(sRP + w * SP + (R + fl), sRP + (TW + w) * SP + (R + fl)) >=
+                            (double)P.sensor_threshold ? 1 : 0;
+      }
+    } else if (hyb_any)
     for (int base = 0; base < ei; base += kThreads) {
       const int e = base + threadIdx.x;
       int w = 0, fl = 0;

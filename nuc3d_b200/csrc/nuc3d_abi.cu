@@ -1191,6 +1191,25 @@ int nuc3d_set_sensor(nuc3d_ctx *c, const float *params, float logit_threshold) {
   CUDA_TRY(nuc3d::fast::run_sensor_zero(c->d_sensor, c->stream));
   c->P.sensor = c->L.P.sensor = c->d_sensor;
   c->P.sensor_threshold = c->L.P.sensor_threshold = logit_threshold;
+  c->P.sensor_theta = c->L.P.sensor_theta = 0;
+  return NUC3D_OK;
+}
+
+int nuc3d_set_sensor_theta(nuc3d_ctx *c, float theta_min) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  if (c->exact)
+    return fail(NUC3D_ENOTSUP, "the hybrid sweep exists in the throughput build only (exact = 0)");
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->drop_graph();
+  if (!c->d_sensor) {
+    CUDA_TRY(cudaMalloc(&c->d_sensor, sizeof(SensorDev)));
+    CUDA_TRY(cudaMemset(c->d_sensor, 0, sizeof(SensorDev)));
+  }
+  c->P.sensor = c->L.P.sensor = c->d_sensor;  // selects the hybrid sweep; weights unused
+  c->P.sensor_threshold = c->L.P.sensor_threshold = theta_min;
+  c->P.sensor_theta = c->L.P.sensor_theta = 1;
   return NUC3D_OK;
 }
 

@@ -105,3 +105,25 @@ def hybrid_rhs(q, m, gamma, compat, linear_mask):
             h = np.where(linear_mask[d], lin, full)
             rhs[v] += ln.at(h, 1) - h
     return rhs
+
+
+def theta_stencil(f0, f1, f2, f3, f4):
+    """hccs's switch theta = 1 / (1 + (sum alpha - 1)^2), CRWENO5-Z numerators with eps
+    1e-40 (src/hccs.cpp:154-181)."""
+    (is0, is1, is2), _ = parts(f0, f1, f2, f3, f4, False)
+    tau = np.abs(is2 - is0)
+    s = sum(c * (1 + (tau / (b + 1e-40)) ** 2) for c, b in zip((0.2, 0.5, 0.3), (is0, is1, is2)))
+    return 1.0 / (1.0 + (s - 1.0) ** 2)
+
+
+def theta_faces(q, m, d, gamma):
+    """Per face of the periodic line (faces 0..L-1): the smallest theta of density and
+    pressure over the positive (f-3 .. f+1) and negative (f+2 .. f-2) stencils."""
+    _, _, rho, p = lf_split(q, m, d, gamma)
+    ln = PeriodicLine(d, rho.shape)
+    out = None
+    for a in (rho, p):
+        for offs in ((-3, -2, -1, 0, 1), (2, 1, 0, -1, -2)):
+            t = theta_stencil(*[ln.at(a, c) for c in offs])
+            out = t if out is None else np.minimum(out, t)
+    return out

@@ -84,6 +84,39 @@ def test_hybrid_decisions_follow_the_trained_network():
 
 
 @pytest.mark.gpu
+def test_theta_switch_decisions():
+    """hccs's theta switch as the decision (nuc3d_set_sensor_theta): theta_min above 1
+    never selects the linear weights (plain), 0 always does, and a theta_min inside a gap
+    of the faces' thetas selects exactly the faces whose numpy theta reaches it."""
+    s0, _, _ = _solver()
+    s0.rhs()
+    plain = s0.get_rhs(0)
+    s, m, q = _solver()
+    s.set_sensor_theta(2.0)
+    s.rhs()
+    assert _rel(s.get_rhs(0), plain) <= 1e-15
+    s.set_sensor_theta(0.0)
+    s.rhs()
+    assert _rel(s.get_rhs(0), SN.hybrid_rhs(q, m, GAMMA, True, [np.ones(q.shape[1:], bool)] * 3)) <= 1e-12
+    th = [SN.theta_faces(q, m, d, GAMMA) for d in range(3)]
+    ts = np.sort(np.concatenate([t.ravel() for t in th]))
+    gaps = np.diff(ts)
+    idx = np.arange(len(gaps))
+    k = int(np.argmax(np.where((idx > len(ts) // 10) & (idx < 9 * len(ts) // 10), gaps, 0)))
+    tmin = float(0.5 * (ts[k] + ts[k + 1]))
+    assert gaps[k] > 1e-6 * max(tmin, 1e-300), gaps[k]
+    masks = [t >= tmin for t in th]
+    frac = float(np.mean(np.concatenate([mk.ravel() for mk in masks])))
+    assert 0.05 < frac < 0.95, frac
+    s.set_sensor_theta(tmin)
+    s.rhs()
+    assert _rel(s.get_rhs(0), SN.hybrid_rhs(q, m, GAMMA, True, masks)) <= 1e-12
+    s.set_sensor(None)
+    s.rhs()
+    assert _rel(s.get_rhs(0), plain) <= 1e-15
+
+
+@pytest.mark.gpu
 def test_exact_build_refuses_the_sensor():
     import nuc3d_b200 as nb
     from nuc3d_b200 import sensor as S
@@ -95,6 +128,9 @@ def test_exact_build_refuses_the_sensor():
     s.finalize()
     with pytest.raises(nb.Nuc3dError) as e:
         s.set_sensor(S.load_weights(), 0.0)
+    assert e.value.code == 5
+    with pytest.raises(nb.Nuc3dError) as e:
+        s.set_sensor_theta(0.5)
     assert e.value.code == 5
 
 
