@@ -605,9 +605,8 @@ def shock_turbulence(args, steps=10, warm=2):
 
 
 COMPACT_WORKLOAD = ("smooth isentropic pressure pulse 256^3 (rho = 1 + 0.5 exp(-r^2/0.08^2), "
-                    "p = rho^1.4/1.4, at rest; the blast's discontinuity drives the compact schemes "
-                    "to negative pressure), FP64 Euler, {scheme} in every direction, AUSM, outlet "
-                    "faces, TVD-RK3 CFL 0.5")
+                    "p = rho^1.4/1.4, at rest), periodic faces, FP64 Euler, {scheme} in every "
+                    "direction, AUSM, TVD-RK3 CFL 0.5")
 
 
 def compact256(args, steps=10, warm=3):
@@ -628,7 +627,10 @@ def compact256(args, steps=10, warm=3):
     for scheme in ("crweno5", "hccs"):
         s = nb.Solver(nb.Config(scheme_ivs=(scheme,) * 3, riemann="AUSM", model="Euler3d", mach=1.0,
                                 cfl=0.5, exact=False))
-        b = s.add_block(*SHAPE, *C.outlet_faces())
+        # periodic: with outlet faces on every side crweno5 goes unstable on this pulse
+        # within 15 steps (the reference-order build the same), and the blast's
+        # discontinuity drives the compact schemes to negative pressure
+        b = s.add_block(*SHAPE, *C.periodic_faces())
         s.set_nodes(b, *C.unit_box_nodes(SHAPE))
         s.finalize()
         s.set_stream(stream.cuda_stream)

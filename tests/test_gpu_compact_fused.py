@@ -82,38 +82,41 @@ def _pulse(shape, scheme, exact, fused=True, nblocks=1):
     return s
 
 
+def _err_vs_exact(shape, scheme, steps, nblocks=1):
+    """Relative max-norm distance from the reference-order build after `steps` steps of
+    the throughput build's three-kernel path and of its fused path."""
+    out = {}
+    for key, exact, fused in (("exact", True, False), ("three", False, False), ("fused", False, True)):
+        s = _pulse(shape, scheme, exact, fused, nblocks)
+        if key == "fused":
+            ts = 4 if scheme == "hccs" else 3
+            assert s.compact_solver() == sum(1 << d for d in range(3) if shape[d] <= 256
+                                             and shape[d] - 2 * ts + 1 >= 2)
+        s.step(steps)
+        out[key] = [s.get_q(b) for b in range(nblocks)]
+        s.close()
+    err = {k: max(rel_max(a, b) for a, b in zip(out[k], out["exact"])) for k in ("three", "fused")}
+    return err["three"], err["fused"]
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("scheme", ["crweno5", "hccs"])
-@pytest.mark.parametrize("shape", [(256, 24, 20), (96, 8, 9)])
+@pytest.mark.parametrize("scheme,shape", [("crweno5", (256, 24, 20)), ("crweno5", (96, 8, 9)),
+                                          ("hccs", (256, 24, 20)), ("hccs", (96, 10, 11))])
 def test_fused_line_lengths(scheme, shape):
     """Lines of 256 cells (the longest fused system: 32 lanes x 8 rows), of 24 and 20
-    (a few lanes of 2-3 rows) and of 8 and 9 (one lane; an hccs direction of 8 cells has
-    a single-row system and stays on the three-kernel path)."""
-    ref = _pulse(shape, scheme, exact=True)
-    ref.step(3)
-    qr = ref.get_q(0)
-    ref.close()
-    s = _pulse(shape, scheme, exact=False)
-    ts = 4 if scheme == "hccs" else 3
-    want = sum(1 << d for d in range(3) if shape[d] - 2 * ts + 1 >= 2)
-    assert s.compact_solver() == want
-    s.step(3)
-    assert rel_max(s.get_q(0), qr) < 1e-11
-    s.close()
+    (a few lanes of 2-3 rows) and of the shortest lines a block may have (8, 9 for crweno5;
+    10, 11 for hccs: 2 bfsize + 2 cells; one lane).  The bar is the throughput build's own
+    three-kernel path: hccs's switch theta (its weights' epsilon is 1e-40) turns the
+    round-off of any operation order into differences up to 1e-8 after 3 steps here, and
+    up to 2e-5 on a 64^3 block, with Thomas as with the fused solve."""
+    three, fused = _err_vs_exact(shape, scheme, 3)
+    assert fused <= max(1e-11, 4.0 * three), (fused, three)
 
 
 @pytest.mark.gpu
 def test_fused_two_blocks_and_long_lines():
     """Two blocks of one context (the line's halo from the neighbour block), and a grid
     whose xi lines exceed 256 cells (xi stays on the three-kernel path)."""
-    for shape, nb_, want in (((128, 32, 24), 2, 7), ((320, 16, 16), 1, 6)):
-        ref = _pulse(shape, "crweno5", exact=True, nblocks=nb_)
-        ref.step(2)
-        qr = [ref.get_q(b) for b in range(nb_)]
-        ref.close()
-        s = _pulse(shape, "crweno5", exact=False, nblocks=nb_)
-        assert s.compact_solver() == want
-        s.step(2)
-        for b in range(nb_):
-            assert rel_max(s.get_q(b), qr[b]) < 1e-11, (shape, b)
-        s.close()
+    for shape, nb_ in (((128, 32, 24), 2), ((320, 16, 16), 1)):
+        three, fused = _err_vs_exact(shape, "crweno5", 2, nb_)
+        assert fused <= max(1e-11, 4.0 * three), (shape, fused, three)
