@@ -286,6 +286,26 @@ int nuc3d_kernels_per_step(nuc3d_ctx *ctx, int *kernels);
 int nuc3d_block_get_prim(nuc3d_ctx *ctx, int block, double *prim);
 int nuc3d_block_get_vis(nuc3d_ctx *ctx, int block, double *vis);
 
+/* Debug taps of the inviscid path: one right-hand side's intermediates at the block's
+   current state (stage 0), for parity work against the reference's EulerFlux members
+   (src/euler3d.h:16-31, allocated at src/euler3d.cpp:12-20 and :62-83).  tap =
+   3 * kind + direction; out: 5 components, each in the reference's layout for that
+   direction: line position fastest, then (xi: j, k; eta: k, i; zeta: i, j).
+     FLUXL / FLUXR   Flux_<dir>.FluxL / FluxR, the split fluxes: 5N doubles
+     RFLUXL / RFLUXR Flux_<dir>.reconstFluxL / R, the reconstructions: 5 (n_dir + 1) N / n_dir
+     DF              dfdxi / dgdeta / dhdzeta, the flux differences: 5N
+   The step state (status bits, energy-reset count) is left as it was.  Explicit schemes
+   use the reference-order boundary switch in either build; compact schemes the
+   three-kernel solve. */
+enum {
+  NUC3D_TAP_FLUXL_XI = 0, NUC3D_TAP_FLUXL_ETA = 1, NUC3D_TAP_FLUXL_ZETA = 2,
+  NUC3D_TAP_FLUXR_XI = 3, NUC3D_TAP_FLUXR_ETA = 4, NUC3D_TAP_FLUXR_ZETA = 5,
+  NUC3D_TAP_RFLUXL_XI = 6, NUC3D_TAP_RFLUXL_ETA = 7, NUC3D_TAP_RFLUXL_ZETA = 8,
+  NUC3D_TAP_RFLUXR_XI = 9, NUC3D_TAP_RFLUXR_ETA = 10, NUC3D_TAP_RFLUXR_ZETA = 11,
+  NUC3D_TAP_DF_XI = 12, NUC3D_TAP_DF_ETA = 13, NUC3D_TAP_DF_ZETA = 14
+};
+int nuc3d_debug_get(nuc3d_ctx *ctx, int block, int tap, double *out);
+
 /* ---- Allocation-free right-hand side -------------------------------------------
    No counterpart in the reference: it exists for callers that cannot allocate device
    memory where they evaluate the right-hand side (a host framework that owns every

@@ -43,6 +43,7 @@ EXPORTED = (
     "nuc3d_get_tiles", "nuc3d_autotune", "nuc3d_get_energy_resets", "nuc3d_set_pipeline",
     "nuc3d_get_pipeline", "nuc3d_rhs_stage", "nuc3d_rk_stage", "nuc3d_get_residual",
     "nuc3d_set_compact_solver", "nuc3d_get_compact_solver", "nuc3d_set_sensor_theta",
+    "nuc3d_debug_get",
 )
 
 
@@ -118,6 +119,7 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_get_pipeline.argtypes = [P, ctypes.POINTER(I)]
     lib.nuc3d_set_compact_solver.argtypes = [P, I]
     lib.nuc3d_set_sensor_theta.argtypes = [P, ctypes.c_float]
+    lib.nuc3d_debug_get.argtypes = [P, I, I, PD]
     lib.nuc3d_get_compact_solver.argtypes = [P, ctypes.POINTER(I)]
     lib.nuc3d_rhs_stage.argtypes = [P, I, PD]
     lib.nuc3d_rk_stage.argtypes = [P, I, D]
@@ -429,6 +431,21 @@ class Solver:
         self._sensor_keep = p
         _check(self.lib.nuc3d_set_sensor(self._ctx, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                          float(logit_threshold)))
+
+    TAP_KINDS = ("FluxL", "FluxR", "rFluxL", "rFluxR", "df")
+
+    def debug_get(self, block: int, kind: str, direction: int) -> np.ndarray:
+        """One debug tap (nuc3d_debug_get): kind in TAP_KINDS, shaped as the reference's
+        Field for that direction, (5, n_c, n_b, n_a) with n_a the line axis (+1 for the
+        face values): xi (nz, ny, nx), eta (nx, nz, ny), zeta (ny, nx, nz)."""
+        k = self.TAP_KINDS.index(kind)
+        nx, ny, nz = self.blocks[block]
+        dims = [(nz, ny, nx), (nx, nz, ny), (ny, nx, nz)][direction]
+        if k in (2, 3):
+            dims = dims[:2] + (dims[2] + 1,)
+        out = np.empty((5,) + dims, dtype=np.float64)
+        _check(self.lib.nuc3d_debug_get(self._ctx, block, 3 * k + direction, _pd(out)))
+        return out
 
     def set_sensor_theta(self, theta_min: float) -> None:
         """Hybrid WENO-Z deciding by hccs's theta switch: linear weights where the face's

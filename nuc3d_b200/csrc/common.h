@@ -240,6 +240,9 @@ cudaError_t run_metrics(const double *x, const double *y, const double *z, const
                         double *jac, double *met, double *dxyz, unsigned *bad, cudaStream_t st);
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
+// run_taps(): debug taps of direction dir for one block (nl: its lines along dir);
+// out = FluxL, FluxR (5N), reconstFluxL, reconstFluxR (5 (L+1) nl), dF (5N), device.
+cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const out[5]);
 cudaError_t configure();
 int tile_count(int dir, const int n[3], int shape);
 }
@@ -254,6 +257,9 @@ cudaError_t run_metrics(const double *x, const double *y, const double *z, const
                         double *jac, double *met, double *dxyz, unsigned *bad, cudaStream_t st);
 cudaError_t run_diag(const Launch &L, const DiagDev *dd, double *sums, double *parts);
 cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
+// run_taps(): debug taps of direction dir for one block (nl: its lines along dir);
+// out = FluxL, FluxR (5N), reconstFluxL, reconstFluxR (5 (L+1) nl), dF (5N), device.
+cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const out[5]);
 cudaError_t configure();
 int tile_count(int dir, const int n[3], int shape);
 }

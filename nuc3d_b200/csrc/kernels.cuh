@@ -2284,6 +2284,166 @@ cudaError_t configure() {
   return configure_dir<2>();
 }
 
+// ---------------------------------------------------------------------------------
+// Debug taps: the inviscid intermediates of one right-hand side at the current state,
+// in the reference's EulerFlux layouts (src/euler3d.cpp:12-20, :62-83): per direction the
+// split fluxes FluxL/FluxR (cells), the reconstructions reconstFluxL/R (faces) and the
+// difference dfdxi/dgdeta/dhdzeta (cells), each stored line position fastest, then
+// (xi: j, k; eta: k, i; zeta: i, j).  Explicit schemes: the reconstructions of the
+// reference-order switch (recon_pos / recon_neg); compact schemes: the three-kernel
+// path's face values (fh).
+// ---------------------------------------------------------------------------------
+template <int DIR>
+__device__ __forceinline__ long long tap_index(int pos, int w, int o, int len, const Geo &G) {
+  return DIR == 1 ? pos + (long long)len * (o + (long long)G.nO * w)
+                  : pos + (long long)len * (w + (long long)G.nW * o);
+}
+
+template <int DIR, int SCH, int SHP, bool FACES>
+__global__ void __launch_bounds__(kThreads)
+tap_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, int want, double *fl,
+           double *fr, double *rl, double *rr, double *df) {
+  using M = TileSmem<DIR, SCH, SHP>;
+  constexpr int R = M::R, TW = M::TW, TL = M::TL, SP = M::SP, SH = M::SH;
+  extern __shared__ double smem[];
+  double *sF = smem;               // [10][TW][SP]
+  double *sH = sF + 10 * TW * SP;  // [5][TW][SH]
+  const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P);
+  if (T.b != want) return;  // the same for the whole CTA
+  unsigned st = 0;
+  double emax = 0.0;
+  phase_split<DIR, SCH, false, SHP>(blocks, T, P, 0, false, sF, nullptr, st, emax);
+  __syncthreads();
+  const Geo &G = T.G;
+  const long long N = T.N, NF = (long long)(G.L + 1) * G.nW * G.nO;
+  for (int e = threadIdx.x; e < TW * TL; e += kThreads) {
+    const int c = e % TL, w = e / TL;
+    if (w >= T.nw || c >= T.cl) continue;
+    const long long i = tap_index<DIR>(T.c0 + c, T.w0 + w, T.o, G.L, G);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      fl[v * N + i] = sF[(v * TW + w) * SP + R + c];
+      fr[v * N + i] = sF[((5 + v) * TW + w) * SP + R + c];
+    }
+  }
+  if constexpr (FACES) {
+    const bool compat = P.weno5z_compat != 0;
+    for (int e = threadIdx.x; e < TW * (TL + 1); e += kThreads) {
+      const int fc = e % (TL + 1), w = e / (TL + 1);
+      if (w >= T.nw || fc > T.cl) continue;
+      const int f = T.c0 + fc;
+      const long long i = tap_index<DIR>(f, T.w0 + w, T.o, G.L + 1, G);
+      for (int v = 0; v < 5; ++v) {
+        const double *rowP = sF + (v * TW + w) * SP + (R - T.c0);
+        const double *rowN = sF + ((5 + v) * TW + w) * SP + (R - T.c0);
+        auto Pacc = [rowP](int cc) { return rowP[cc]; };
+        auto Nacc = [rowN](int cc) { return rowN[cc]; };
+        const double hp = recon_pos<SCH>(f, G.L, T.ts, T.physL, T.physR, compat, Pacc);
+        const double hn = recon_neg<SCH>(f, G.L, T.ts, T.physL, T.physR, Nacc);
+        rl[v * NF + i] = hp;
+        rr[v * NF + i] = hn;
+        sH[(v * TW + w) * SH + fc] = hp + hn;
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < TW * TL; e += kThreads) {
+      const int c = e % TL, w = e / TL;
+      if (w >= T.nw || c >= T.cl) continue;
+      const long long i = tap_index<DIR>(T.c0 + c, T.w0 + w, T.o, G.L, G);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) df[v * N + i] = sH[(v * TW + w) * SH + c + 1] - sH[(v * TW + w) * SH + c];
+    }
+  }
+}
+
+// Compact directions: face values of one block from fh (compact_rows + compact_thomas).
+template <int DIR>
+__global__ void __launch_bounds__(256)
+tap_fh_kernel(const BlockDev *__restrict__ blocks, int want, double *rl, double *rr, double *df) {
+  const BlockDev &B = blocks[want];
+  const int n[3] = {B.n[0], B.n[1], B.n[2]};
+  const Geo G = make_geo(DIR, n);
+  const long long nl = (long long)G.nW * G.nO, NF = (long long)(G.L + 1) * nl;
+  const long long t = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (t >= 5 * nl) return;
+  const int v = (int)(t / nl);
+  const long long line = t - v * nl;
+  const int w = (int)(line % G.nW), o = (int)(line / G.nW);
+  const double *hp = B.fh + ((2 * v) * nl + line) * (G.L + 1);
+  const double *hn = B.fh + ((2 * v + 1) * nl + line) * (G.L + 1);
+  double prev = 0.0;
+  for (int f = 0; f <= G.L; ++f) {
+    const long long i = tap_index<DIR>(f, w, o, G.L + 1, G);
+    rl[v * NF + i] = hp[f];
+    rr[v * NF + i] = hn[f];
+    const double h = hp[f] + hn[f];
+    if (f > 0) df[v * B.N + tap_index<DIR>(f - 1, w, o, G.L, G)] = h - prev;
+    prev = h;
+  }
+}
+
+template <int DIR, int SCH, int SHP, bool FACES>
+inline cudaError_t launch_tap(const Launch &L, int block, double *const out[5]) {
+  using M = TileSmem<DIR, SCH, SHP>;
+  const size_t smem = ((size_t)10 * M::TW * M::SP + (size_t)5 * M::TW * M::SH) * sizeof(double);
+  const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
+  tap_kernel<DIR, SCH, SHP, FACES><<<ntiles, kThreads, smem, L.stream>>>(
+      L.d_blocks, L.tm_dir[DIR], L.P, block, out[0], out[1], out[2], out[3], out[4]);
+  return cudaGetLastError();
+}
+
+template <int DIR, int SCH, bool FACES>
+inline cudaError_t launch_tap_s(const Launch &L, int block, double *const out[5]) {
+  switch (L.shape[DIR]) {
+    case 0: return launch_tap<DIR, SCH, 0, FACES>(L, block, out);
+    case 1: return launch_tap<DIR, SCH, 1, FACES>(L, block, out);
+    case 2: return launch_tap<DIR, SCH, 2, FACES>(L, block, out);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int DIR, int SCH, bool WHOLE>
+inline cudaError_t launch_tap_compact(const Launch &L, int block, const int nl, double *const out[5]) {
+  cudaError_t e = launch_tap_s<DIR, SCH, false>(L, block, out);
+  if (e != cudaSuccess) return e;
+  const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
+  compact_rows_kernel<DIR, SCH, WHOLE><<<ntiles, kThreads, compact_rows_smem_bytes<DIR, SCH>(), L.stream>>>(
+      L.d_blocks, L.tm_dir[DIR], L.P, L.d_state, 0, 0);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int nsys = L.tm_sys[DIR].tile_start[L.tm_sys[DIR].nblocks];
+  compact_thomas_kernel<DIR><<<nsys, 256, 0, L.stream>>>(L.d_blocks, L.tm_sys[DIR], L.P,
+                                                         WHOLE ? 0 : L.P.ts[DIR]);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  tap_fh_kernel<DIR><<<(5 * nl + 255) / 256, 256, 0, L.stream>>>(L.d_blocks, block, out[2], out[3], out[4]);
+  return cudaGetLastError();
+}
+
+template <int DIR>
+inline cudaError_t run_taps_d(const Launch &L, int block, int nl, double *const out[5]) {
+  switch (L.P.scheme[DIR]) {
+    case SCH_WENO5JS: return launch_tap_s<DIR, SCH_WENO5JS, true>(L, block, out);
+    case SCH_WENO5Z: return launch_tap_s<DIR, SCH_WENO5Z, true>(L, block, out);
+    case SCH_WENO7JS: return launch_tap_s<DIR, SCH_WENO7JS, true>(L, block, out);
+    case SCH_WENO3JS: return launch_tap_s<DIR, SCH_WENO3JS, true>(L, block, out);
+    case SCH_UPWIND1: return launch_tap_s<DIR, SCH_UPWIND1, true>(L, block, out);
+    case SCH_CRWENO5: return launch_tap_compact<DIR, SCH_CRWENO5, false>(L, block, nl, out);
+    case SCH_HCCS: return launch_tap_compact<DIR, SCH_HCCS, false>(L, block, nl, out);
+    case SCH_HCCS77: return launch_tap_compact<DIR, SCH_HCCS, true>(L, block, nl, out);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const out[5]) {
+  if (L.bc_tiles > 0) {  // the physical faces' ghost fluxes at the current state
+    bc_ghost_kernel<<<L.bc_tiles, 256, 0, L.stream>>>(L.d_blocks, L.d_jobs, L.P, L.d_state, 0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (dir == 0) return run_taps_d<0>(L, block, nl, out);
+  if (dir == 1) return run_taps_d<1>(L, block, nl, out);
+  return run_taps_d<2>(L, block, nl, out);
+}
+
 int tile_count(int dir, const int n[3], int shape) { return sweep_tiles(dir, n, shape); }
 
 }  // namespace NUC3D_NS

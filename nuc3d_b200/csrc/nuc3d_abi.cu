@@ -707,6 +707,31 @@ int nuc3d_block_get_vis(nuc3d_ctx *c, int bi, double *vis) {
   return copy_out(c, bi, vis, c->blocks[bi].vis, 12);
 }
 
+int nuc3d_debug_get(nuc3d_ctx *c, int bi, int tap, double *out) {
+  if (!c || !out || bi < 0 || bi >= (int)c->blocks.size() || tap < 0 || tap >= 15)
+    return fail(NUC3D_EINVAL, "bad argument");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  const int dir = tap % 3, kind = tap / 3;
+  const HostBlock &b = c->blocks[bi];
+  const long long N = b.N, nl = b.N / b.n[dir], NF = (long long)(b.n[dir] + 1) * nl;
+  cudaSetDevice(c->device);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  StepState s0;  // the taps leave the step state (status, reset count) as it was
+  CUDA_TRY(cudaMemcpy(&s0, c->d_state, sizeof(s0), cudaMemcpyDeviceToHost));
+  double *buf = nullptr;
+  CUDA_TRY(cudaMalloc(&buf, sizeof(double) * (size_t)(15 * N + 10 * NF)));
+  double *const o[5] = {buf, buf + 5 * N, buf + 10 * N, buf + 10 * N + 5 * NF, buf + 10 * N + 10 * NF};
+  cudaError_t e = c->exact ? nuc3d::exact::run_taps(c->L, bi, dir, (int)nl, o)
+                           : nuc3d::fast::run_taps(c->L, bi, dir, (int)nl, o);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  const size_t n = (size_t)5 * (kind == 2 || kind == 3 ? NF : N);
+  if (e == cudaSuccess) e = cudaMemcpy(out, o[kind], n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_state, &s0, sizeof(s0), cudaMemcpyHostToDevice);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(NUC3D_ECUDA, "debug taps: %s", cudaGetErrorString(e));
+  return NUC3D_OK;
+}
+
 static int check_status(nuc3d_ctx *c) {
   StepState s;
   CUDA_TRY(cudaMemcpy(&s, c->d_state, sizeof(s), cudaMemcpyDeviceToHost));
