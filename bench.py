@@ -939,7 +939,8 @@ def turbulence24(args, with_cpu=False):
 def profile_case(args):
     """--profile-case: the workload at a chosen size, untimed -- the command ncu captures.
     Euler: the spherical Riemann problem (this file's workload); --ns: the Navier-Stokes
-    Taylor-Green vortex (WENO5-JS, LF, periodic).  --sweeps R launches each direction's
+    Taylor-Green vortex (WENO5-JS, LF, periodic); --scheme S: S in every direction on the
+    periodic smooth pulse (the compact key's workload).  --sweeps R launches each direction's
     right-hand-side sweep 1 + R times (the launches the roofline times) instead of stepping;
     --hybrid sets the learned face sensor."""
     import nuc3d_b200 as nb
@@ -949,6 +950,12 @@ def profile_case(args):
         cfg = nb.Config(scheme_ivs=("weno5js",) * 3, riemann="LF", model="NavierStokes3d",
                         mach=0.1, reynolds=1600.0, exact=args.exact)
         q, m = C.taylor_green(shape)
+        faces = C.periodic_faces()
+    elif args.scheme:
+        # the compact bench key's workload: the periodic smooth pulse at CFL 0.2
+        cfg = nb.Config(scheme_ivs=(args.scheme,) * 3, riemann="AUSM", model="Euler3d", mach=1.0,
+                        cfl=0.2, exact=args.exact)
+        q, m = C.gaussian_pulse(shape)
         faces = C.periodic_faces()
     else:
         cfg = nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="Euler3d", mach=1.0,
@@ -999,6 +1006,9 @@ def main():
     ap.add_argument("--sweeps", type=int, default=0, help="--profile-case: sweep launches")
     ap.add_argument("--ns", action="store_true", help="--profile-case: NS Taylor-Green")
     ap.add_argument("--hybrid", action="store_true", help="--profile-case: learned sensor")
+    ap.add_argument("--scheme", default=None,
+                    help="--profile-case: this scheme in every direction on the smooth pulse "
+                         "(the compact key's workload)")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args)

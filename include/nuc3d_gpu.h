@@ -162,8 +162,17 @@ int nuc3d_step(nuc3d_ctx *ctx, int nsteps);
    nuc3d_block_set_q layout) and writing the new Q back there.  The download of a step and
    the upload of the next run at the same time in 16 MiB chunks (PCIe is full duplex), so
    q_host should be pinned (cudaHostAlloc / cudaHostRegister).  Synchronous: returns
-   when q_host holds the last step's state, with nuc3d_sync's status check. */
+   when q_host holds the last step's state, with nuc3d_sync's status check.
+   A context of one Euler block with explicit schemes and at least two z-chunks of the zeta
+   sweep's tile runs the steps as a pipeline over those z-slabs instead: each slab's
+   upload is followed at once by stage 0's work on it (the xi and eta lines lie in a
+   z-plane), and each slab's download follows stage 2's zeta sweep over it, so the copy
+   engines move the other slabs while the GPU computes; the kernels and their tiles are
+   those of nuc3d_step (bitwise the same results).  nuc3d_set_host_pipeline(ctx, 0) turns
+   that off; nuc3d_get_host_pipeline gives the slab count in use (0: the chunked copies). */
 int nuc3d_solve_host(nuc3d_ctx *ctx, double *const *q_host, int nsteps);
+int nuc3d_set_host_pipeline(nuc3d_ctx *ctx, int on);
+int nuc3d_get_host_pipeline(nuc3d_ctx *ctx, int *slabs);
 int nuc3d_sync(nuc3d_ctx *ctx);
 /* time accumulated over the steps and the dt of the last step */
 int nuc3d_get_time(nuc3d_ctx *ctx, double *time, double *dt);

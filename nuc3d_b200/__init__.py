@@ -43,7 +43,7 @@ EXPORTED = (
     "nuc3d_get_tiles", "nuc3d_autotune", "nuc3d_get_energy_resets", "nuc3d_set_pipeline",
     "nuc3d_get_pipeline", "nuc3d_rhs_stage", "nuc3d_rk_stage", "nuc3d_get_residual",
     "nuc3d_set_compact_solver", "nuc3d_get_compact_solver", "nuc3d_set_sensor_theta",
-    "nuc3d_debug_get",
+    "nuc3d_debug_get", "nuc3d_set_host_pipeline", "nuc3d_get_host_pipeline",
 )
 
 
@@ -120,6 +120,8 @@ def load_library() -> ctypes.CDLL:
     lib.nuc3d_set_compact_solver.argtypes = [P, I]
     lib.nuc3d_set_sensor_theta.argtypes = [P, ctypes.c_float]
     lib.nuc3d_debug_get.argtypes = [P, I, I, PD]
+    lib.nuc3d_set_host_pipeline.argtypes = [P, I]
+    lib.nuc3d_get_host_pipeline.argtypes = [P, ctypes.POINTER(I)]
     lib.nuc3d_get_compact_solver.argtypes = [P, ctypes.POINTER(I)]
     lib.nuc3d_rhs_stage.argtypes = [P, I, PD]
     lib.nuc3d_rk_stage.argtypes = [P, I, D]
@@ -320,6 +322,16 @@ class Solver:
         _check(self.lib.nuc3d_step(self._ctx, int(n)))
         if sync:
             self.sync()
+
+    def set_host_pipeline(self, on: bool) -> None:
+        """solve_host as a copy/compute pipeline over z-slabs where it applies (default)."""
+        _check(self.lib.nuc3d_set_host_pipeline(self._ctx, 1 if on else 0))
+
+    def host_pipeline(self) -> int:
+        """z-slabs solve_host pipelines over (0: whole-state chunked copies)."""
+        v = ctypes.c_int()
+        _check(self.lib.nuc3d_get_host_pipeline(self._ctx, ctypes.byref(v)))
+        return v.value
 
     def solve_host(self, host_ptrs, n: int = 1) -> None:
         """n steps on host arrays, in place: every step reads each block's Q from its host

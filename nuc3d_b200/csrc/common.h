@@ -75,12 +75,25 @@ struct BlockDev {
 // tile_l(s) cells along them; 0: 4 x 64, 1: 8 x 32, 2: 2 x 128.  All hold 256 cells, so
 // every sweep CTA has the same 288 threads.  Compact schemes use shape 0.
 constexpr int kTileShapes = 3;
-// Shape kLineShape (1 x 256, one whole line of at most 256 cells) is not an autotuner
-// choice: it is the tile of the fused compact sweep (compact_line_kernel).
+// Shapes kLineShape (1 x 256) and kLineShape4 (kLineLanes x 256: whole lines of at most
+// 256 cells) are not autotuner choices: they are the tiles of the fused compact sweep
+// (compact_line_kernel), one line per CTA along xi, kLineLanes neighbouring lines along
+// eta and zeta so that the strided loads fill 32-byte sectors.
 constexpr int kLineShape = 3;
+constexpr int kLineShape4 = 4;
+#ifndef NUC3D_LINE_LANES
+#define NUC3D_LINE_LANES 4
+#endif
+constexpr int kLineLanes = NUC3D_LINE_LANES;
 constexpr int kLineMax = 256;
-__host__ __device__ constexpr int tile_w(int s) { return s == 1 ? 8 : (s == 2 ? 2 : (s == 3 ? 1 : 4)); }
-__host__ __device__ constexpr int tile_l(int s) { return s == 1 ? 32 : (s == 2 ? 128 : (s == 3 ? 256 : 64)); }
+constexpr size_t kSmemOptin = 227 * 1024;  // dynamic shared memory per CTA (opt-in maximum)
+__host__ __device__ constexpr int line_shape(int dir) { return dir == 0 ? kLineShape : kLineShape4; }
+__host__ __device__ constexpr int tile_w(int s) {
+  return s == 1 ? 8 : (s == 2 ? 2 : (s == 3 ? 1 : (s == 4 ? kLineLanes : 4)));
+}
+__host__ __device__ constexpr int tile_l(int s) {
+  return s == 1 ? 32 : (s == 2 ? 128 : (s >= 3 ? 256 : 64));
+}
 
 // Boxes of the pipelined sweep's tensor-map loads (pipe_sweep_kernel), for direction d, a
 // tile of tw lines x tl cells and a scheme reaching r cells: the halo box covers line
@@ -162,6 +175,10 @@ constexpr int kMaxBlocks = 512;
 struct TileMap {
   int nblocks;
   int tile_start[kMaxBlocks + 1];  // prefix sums of tiles per block
+  // the tiles base .. end-1 of a launch over part of the map (end 0: to the last tile);
+  // kernels keep the global tile index, so per-tile outputs and "tile 0" duties are as
+  // in a launch over all tiles
+  int base, end;
 };
 
 // Device-resident scalars of the time loop.
@@ -233,6 +250,13 @@ namespace exact {
 cudaError_t run_rk_stage(const Launch &L, int stage, double dt);
 cudaError_t run_residual(const Launch &L, bool cells);
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+// run_bc(): the physical faces' ghost fluxes at stage `stage` for the cells k0 <= k < k1.
+// Pieces of one Euler step over z-slabs (nuc3d_solve_host's copy/compute pipeline).
+cudaError_t run_stage0_slab(const Launch &L, int k0, int k1, int tx0, int tx1, int ty0, int ty1);
+cudaError_t run_stage0_zeta(const Launch &L);
+cudaError_t run_stage2_head(const Launch &L);
+cudaError_t run_stage2_zeta(const Launch &L, int t0, int t1);
+cudaError_t run_bc(const Launch &L, int stage, int k0, int k1);
 cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
                             long long *where, unsigned long long *count, unsigned long long cap);
@@ -243,6 +267,8 @@ cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 // run_taps(): debug taps of direction dir for one block (nl: its lines along dir);
 // out = FluxL, FluxR (5N), reconstFluxL, reconstFluxR (5 (L+1) nl), dF (5N), device.
 cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const out[5]);
+// compact_line_smem(): dynamic shared memory of the fused compact sweep (0: none).
+size_t compact_line_smem(int dir, int sch, bool ns);
 cudaError_t configure();
 int tile_count(int dir, const int n[3], int shape);
 }
@@ -250,6 +276,13 @@ namespace fast {
 cudaError_t run_rk_stage(const Launch &L, int stage, double dt);
 cudaError_t run_residual(const Launch &L, bool cells);
 cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
+// run_bc(): the physical faces' ghost fluxes at stage `stage` for the cells k0 <= k < k1.
+// Pieces of one Euler step over z-slabs (nuc3d_solve_host's copy/compute pipeline).
+cudaError_t run_stage0_slab(const Launch &L, int k0, int k1, int tx0, int tx1, int ty0, int ty1);
+cudaError_t run_stage0_zeta(const Launch &L);
+cudaError_t run_stage2_head(const Launch &L);
+cudaError_t run_stage2_zeta(const Launch &L, int t0, int t1);
+cudaError_t run_bc(const Launch &L, int stage, int k0, int k1);
 cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
                             long long *where, unsigned long long *count, unsigned long long cap);
@@ -260,6 +293,8 @@ cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 // run_taps(): debug taps of direction dir for one block (nl: its lines along dir);
 // out = FluxL, FluxR (5N), reconstFluxL, reconstFluxR (5 (L+1) nl), dF (5N), device.
 cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const out[5]);
+// compact_line_smem(): dynamic shared memory of the fused compact sweep (0: none).
+size_t compact_line_smem(int dir, int sch, bool ns);
 cudaError_t configure();
 int tile_count(int dir, const int n[3], int shape);
 }

@@ -42,7 +42,7 @@ namespace NUC3D_NS {
 constexpr int kThreads = 256 + 32;
 template <int SHP> struct Tile {
   static constexpr int TW = tile_w(SHP), TL = tile_l(SHP);
-  static_assert(TW * TL == 256, "every tile shape holds 256 cells");
+  static_assert(TW * TL == 256 || SHP >= kLineShape, "every sweep tile shape holds 256 cells");
 };
 
 template <int SCH> struct Halo {
@@ -491,11 +491,15 @@ __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ bloc
   T.physR = T.B->face[2 * DIR + 1].type < 0;
   return T;
 }
-// The tile of this CTA (one tile per CTA).
+// The tile of this CTA (one tile per CTA, counted from the map's base).
 template <int DIR, int SHP = 0>
 __device__ __forceinline__ TileCtx decode_tile(const BlockDev *__restrict__ blocks, const TileMap &tm,
                                                const SolverParams &P) {
-  return decode_tile<DIR, SHP>(blocks, tm, P, (int)blockIdx.x);
+  return decode_tile<DIR, SHP>(blocks, tm, P, tm.base + (int)blockIdx.x);
+}
+// Tiles a launch over the map covers.
+__host__ __device__ inline int tile_range(const TileMap &tm) {
+  return (tm.end > 0 ? tm.end : tm.tile_start[tm.nblocks]) - tm.base;
 }
 
 // Shared-memory row strides of a sweep tile.
@@ -1308,8 +1312,8 @@ __device__ __forceinline__ LineRow line_row(const double *rowF, int f, int side,
   return q;
 }
 
-// The line of tile t (lines numbered lane-fastest, then outer index).
-template <int DIR>
+// The lines of tile t: tile = (group of TW neighbouring lanes) + groups * (outer index).
+template <int DIR, int TW>
 __device__ __forceinline__ TileCtx decode_line(const BlockDev *__restrict__ blocks, const TileMap &tm,
                                                const SolverParams &P) {
   TileCtx T;
@@ -1319,9 +1323,10 @@ __device__ __forceinline__ TileCtx decode_line(const BlockDev *__restrict__ bloc
   for (int d = 0; d < 3; ++d) T.n[d] = T.B->n[d];
   T.G = make_geo(DIR, T.n);
   const int lt = T.t - tm.tile_start[T.b];
-  T.o = lt / T.G.nW;
-  T.w0 = lt - T.o * T.G.nW;
-  T.nw = 1;
+  const int ng = (T.G.nW + TW - 1) / TW;
+  T.o = lt / ng;
+  T.w0 = (lt - T.o * ng) * TW;
+  T.nw = min(TW, T.G.nW - T.w0);
   T.c0 = 0;
   T.cl = T.G.L;
   T.N = T.B->N;
@@ -1333,68 +1338,78 @@ __device__ __forceinline__ TileCtx decode_line(const BlockDev *__restrict__ bloc
 
 template <int DIR, int SCH>
 __host__ __device__ inline size_t compact_line_smem_bytes(bool ns) {
-  using M = TileSmem<DIR, SCH, kLineShape>;
-  size_t n = (size_t)10 * M::SP + (size_t)10 * M::SH;
-  if (ns) n += (size_t)4 * M::SV;
-  if (DIR == 2) n += (size_t)5 * M::SQ;
+  using M = TileSmem<DIR, SCH, line_shape(DIR)>;
+  size_t n = (size_t)10 * M::TW * M::SP + (size_t)10 * M::TW * M::SH;
+  if (ns) n += (size_t)4 * M::TW * M::SV;
+  if (DIR == 2) n += (size_t)5 * M::TW * M::SQ;
   return n * sizeof(double);
 }
 
 template <int DIR, int SCH>
-__global__ void __launch_bounds__(kLineThreads, 2)
+__global__ void __launch_bounds__(kLineThreads, DIR == 0 || kLineLanes <= 2 ? 2 : 1)
 compact_line_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P, StepState *S,
                     int stage, int flags) {
-  using M = TileSmem<DIR, SCH, kLineShape>;
-  constexpr int R = M::R, SP = M::SP, SH = M::SH, SV = M::SV;
-  static_assert(M::TL >= kLineMax && M::TW == 1, "one whole line per CTA");
+  constexpr int SHP = line_shape(DIR);
+  using M = TileSmem<DIR, SCH, SHP>;
+  constexpr int R = M::R, TW = M::TW, SP = M::SP, SH = M::SH, SV = M::SV;
+  static_assert(M::TL >= kLineMax, "whole lines per CTA");
   extern __shared__ double smem[];
-  double *sF = smem;           // [10][SP] split fluxes; later [5][SH] the face values
-  double *sX = sF + 10 * SP;   // [10][SH] each system's solution and explicit faces
+  double *sF = smem;                // [10][TW][SP] split fluxes; later [5][TW][SH] face values
+  double *sX = sF + 10 * TW * SP;   // [10][TW][SH] each system's solution and explicit faces
   const bool ns = (flags & SW_NS) != 0;
-  double *sV = sX + 10 * SH;   // [4][SV] viscous fluxes (NS)
-  double *sQ = sV + (ns ? 4 * SV : 0);  // [5][SQ] zeta: the stage state of the line
+  double *sV = sX + 10 * TW * SH;   // [4][TW][SV] viscous fluxes (NS)
+  double *sQ = sV + (ns ? 4 * TW * SV : 0);  // [5][TW][SQ] zeta: the stage state of the lines
   __shared__ double sRed[kLineThreads / 32];
-  const TileCtx T = decode_line<DIR>(blocks, tm, P);
+  const TileCtx T = decode_line<DIR, TW>(blocks, tm, P);
+  // phases 1 and 3 run on the first kThreads threads (their loops stride by kThreads and
+  // phase 1 writes every item it visits); warp 9 takes part in the solve and the barriers
+  // only, and in phase 3 as a tile with no lanes, which skips every item
+  TileCtx Tp = T;
+  if (threadIdx.x >= kThreads) Tp.nw = 0;
   const bool eig = (flags & SW_EIG) != 0;
   unsigned st = 0, nres = 0;
   double emax = 0.0;
-  // phases 1 and 3 run on the first kThreads threads in one round (the line's
-  // positions number at most kThreads); warp 9 joins the solve and the barriers
-  phase_split<DIR, SCH, false, kLineShape>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st,
-                                           emax, nullptr, DIR == 0 ? &nres : nullptr);
-  if (ns) phase_vis<DIR, SCH, kLineShape>(blocks, T, P, sV);
+  if (threadIdx.x < kThreads) {
+    phase_split<DIR, SCH, false, SHP>(blocks, T, P, stage, eig, sF, DIR == 2 ? sQ : nullptr, st, emax,
+                                      nullptr, DIR == 0 ? &nres : nullptr);
+    if (ns) phase_vis<DIR, SCH, SHP>(blocks, T, P, sV);
+  }
   __syncthreads();
   {
     const int sys = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int v = sys >> 1, side = sys & 1;
-    const double *rowF = sF + (side ? 5 + v : v) * SP + R;  // c0 = 0
-    auto A = [rowF](int c) { return rowF[c]; };
-    double *x = sX + sys * SH;
     const int L = T.G.L, ts = T.ts, m = L - 2 * ts + 1;
-    // explicit faces next to the block edges (f < ts, f > L - ts)
-    if (lane < 2 * ts) {
-      const int f = lane < ts ? lane : L - 2 * ts + 1 + lane;
-      x[f] = side ? recon_neg<SCH>(f, L, ts, T.physL, T.physR, A)
-                  : recon_pos<SCH>(f, L, ts, T.physL, T.physR, false, A);
+    for (int w = 0; w < T.nw; ++w) {
+      const double *rowF = sF + ((side ? 5 + v : v) * TW + w) * SP + R;  // c0 = 0
+      auto A = [rowF](int c) { return rowF[c]; };
+      double *x = sX + (sys * TW + w) * SH;
+      // explicit faces next to the block edges (f < ts, f > L - ts)
+      if (lane < 2 * ts) {
+        const int f = lane < ts ? lane : L - 2 * ts + 1 + lane;
+        x[f] = side ? recon_neg<SCH>(f, L, ts, T.physL, T.physR, A)
+                    : recon_pos<SCH>(f, L, ts, T.physL, T.physR, false, A);
+      }
+      auto row = [&](int r, double &a, double &b, double &c, double &d) {
+        const LineRow q = line_row<SCH>(rowF, ts + r, side, r == 0 || r == m - 1);
+        a = q.a;
+        b = q.b;
+        c = q.c;
+        d = q.d;
+      };
+      auto out = [x, ts](int r, double val) { x[ts + r] = val; };
+      warp_tridiag(m, row, out);
     }
-    auto row = [&](int r, double &a, double &b, double &c, double &d) {
-      const LineRow q = line_row<SCH>(rowF, ts + r, side, r == 0 || r == m - 1);
-      a = q.a;
-      b = q.b;
-      c = q.c;
-      d = q.d;
-    };
-    auto out = [x, ts](int r, double val) { x[ts + r] = val; };
-    warp_tridiag(m, row, out);
   }
   __syncthreads();
   double *sH = sF;
-  for (int e = threadIdx.x; e < 5 * (T.G.L + 1); e += kLineThreads) {
-    const int v = e / (T.G.L + 1), f = e - v * (T.G.L + 1);
-    sH[v * SH + f] = sX[(2 * v) * SH + f] + sX[(2 * v + 1) * SH + f];
+  const int nf = T.G.L + 1;
+  for (int e = threadIdx.x; e < 5 * TW * nf; e += kLineThreads) {
+    const int vw = e / nf, f = e - vw * nf, v = vw / TW, w = vw - v * TW;
+    if (w < T.nw)
+      sH[(v * TW + w) * SH + f] = sX[((2 * v) * TW + w) * SH + f] + sX[((2 * v + 1) * TW + w) * SH + f];
   }
   __syncthreads();
-  phase_cells<DIR, SCH, kLineShape>(T, P, S, stage, flags & ~SW_EIG, sH, sV, sQ, st, sRed);
+  phase_cells<DIR, SCH, SHP>(Tp, P, S, stage, flags & ~SW_EIG, sH, sV, sQ, st, sRed);
   if (eig) reduce_eig(emax, sRed, S);
   if (st) atomicOr(&S->status, st);
   if (nres) atomicAdd(&S->reset_cells, (unsigned long long)nres);
@@ -1408,7 +1423,7 @@ compact_line_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParam
 // ---------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 bc_ghost_kernel(const BlockDev *__restrict__ blocks, const FaceJobs *__restrict__ jobs,
-                SolverParams P, StepState *S, int stage) {
+                SolverParams P, StepState *S, int stage, int k0 = 0, int k1 = 0x7fffffff) {
   int lo = 0, hi = jobs->njobs - 1;
   const int t = blockIdx.x;
   while (lo < hi) {
@@ -1427,6 +1442,7 @@ bc_ghost_kernel(const BlockDev *__restrict__ blocks, const FaceJobs *__restrict_
   if (d == 0) { i = pos; j = a; k = b; }
   else if (d == 1) { i = b; j = pos; k = a; }
   else { i = a; j = b; k = pos; }
+  if (k < k0 || k >= k1) return;  // a z-slab's share (nuc3d_solve_host's pipelined steps)
   const long long eidx = ((long long)k * B.n[1] + j) * B.n[0] + i;
   unsigned st = 0;
   double out[5];
@@ -1992,7 +2008,8 @@ __host__ __device__ inline size_t hybrid_smem_bytes(bool ns) {
 
 template <int DIR, int SCH, int SHP>
 inline cudaError_t launch_sweep_s(const Launch &L, int stage, int flags) {
-  const int ntiles = L.tm_dir[DIR].tile_start[L.tm_dir[DIR].nblocks];
+  const int ntiles = tile_range(L.tm_dir[DIR]);
+  if (ntiles <= 0) return cudaSuccess;
   const bool ns = (flags & SW_NS) != 0;
 #if NUC3D_FAST
   if constexpr (SCH == SCH_WENO5Z) {
@@ -2142,6 +2159,44 @@ cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig) {
   return launch_stage(L, stage, rk, eig);
 }
 
+// Pieces of one Euler step for nuc3d_solve_host's slab pipeline; together, in this order,
+// they launch exactly the kernels of one_step over the same tiles (the same results):
+//   stage-0 slab s (BC of k0 <= k < k1; xi and eta over the slab's tiles, xi reducing the
+//   eigenvalue maximum) for every slab, then zeta of stage 0, stage 1, the stage-2 head
+//   (BC, xi, eta), stage-2 zeta over each z-chunk's tiles, and the residual.
+static TileMap tile_part(TileMap tm, int t0, int t1) {
+  tm.base = t0;
+  tm.end = t1;
+  return tm;
+}
+cudaError_t run_stage0_slab(const Launch &L, int k0, int k1, int tx0, int tx1, int ty0, int ty1) {
+  cudaError_t e = run_bc(L, 0, k0, k1);
+  if (e != cudaSuccess) return e;
+  Launch P = L;
+  P.tm_dir[0] = tile_part(L.tm_dir[0], tx0, tx1);
+  if ((e = launch_sweep<0>(P, 0, SW_EIG)) != cudaSuccess) return e;
+  P.tm_dir[1] = tile_part(L.tm_dir[1], ty0, ty1);
+  return launch_sweep<1>(P, 0, 0);
+}
+cudaError_t run_stage0_zeta(const Launch &L) { return launch_sweep<2>(L, 0, SW_RK); }
+cudaError_t run_stage2_head(const Launch &L) {
+  cudaError_t e = run_bc(L, 2, 0, 0x7fffffff);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_sweep<0>(L, 2, 0)) != cudaSuccess) return e;
+  return launch_sweep<1>(L, 2, 0);
+}
+cudaError_t run_stage2_zeta(const Launch &L, int t0, int t1) {
+  Launch P = L;
+  P.tm_dir[2] = tile_part(L.tm_dir[2], t0, t1);
+  return launch_sweep<2>(P, 2, SW_RK | (L.d_res_last ? SW_RES : 0));
+}
+
+cudaError_t run_bc(const Launch &L, int stage, int k0, int k1) {
+  if (L.bc_tiles <= 0) return cudaSuccess;
+  bc_ghost_kernel<<<L.bc_tiles, 256, 0, L.stream>>>(L.d_blocks, L.d_jobs, L.P, L.d_state, stage, k0, k1);
+  return cudaGetLastError();
+}
+
 cudaError_t run_metrics(const double *x, const double *y, const double *z, const int n[3],
                         double *jac, double *met, double *dxyz, unsigned *bad, cudaStream_t st) {
   const long long N = (long long)n[0] * n[1] * n[2];
@@ -2256,8 +2311,9 @@ inline cudaError_t configure_compact_t() {
     if (e != cudaSuccess) return e;
   }
 #if NUC3D_FAST
+  // (a Navier-Stokes tile of kLineLanes lines may not fit: compact_line_smem tells the host)
   e = cudaFuncSetAttribute(compact_line_kernel<DIR, SCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)compact_line_smem_bytes<DIR, SCH>(true));
+                           (int)std::min<size_t>(compact_line_smem_bytes<DIR, SCH>(true), kSmemOptin));
   if (e != cudaSuccess) return e;
 #endif
   return cudaFuncSetAttribute(compact_finish_kernel<DIR, SCH>,
@@ -2445,6 +2501,19 @@ cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const 
 }
 
 int tile_count(int dir, const int n[3], int shape) { return sweep_tiles(dir, n, shape); }
+
+size_t compact_line_smem(int dir, int sch, bool ns) {
+#if NUC3D_FAST
+  if (sch != SCH_CRWENO5 && sch != SCH_HCCS) return 0;
+  const bool c = sch == SCH_CRWENO5;
+  if (dir == 0) return c ? compact_line_smem_bytes<0, SCH_CRWENO5>(ns) : compact_line_smem_bytes<0, SCH_HCCS>(ns);
+  if (dir == 1) return c ? compact_line_smem_bytes<1, SCH_CRWENO5>(ns) : compact_line_smem_bytes<1, SCH_HCCS>(ns);
+  return c ? compact_line_smem_bytes<2, SCH_CRWENO5>(ns) : compact_line_smem_bytes<2, SCH_HCCS>(ns);
+#else
+  (void)dir; (void)sch; (void)ns;
+  return 0;
+#endif
+}
 
 }  // namespace NUC3D_NS
 }  // namespace nuc3d

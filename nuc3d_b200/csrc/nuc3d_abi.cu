@@ -126,6 +126,9 @@ struct nuc3d_ctx {
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t ev_start = nullptr, ev_h2d = nullptr, ev_step = nullptr, ev_end = nullptr;
   std::vector<cudaEvent_t> ev_chunk;
+  // nuc3d_solve_host's slab pipeline: per z-slab, upload done / stage-2 zeta done / download done
+  std::vector<cudaEvent_t> ev_up, ev_zeta, ev_down;
+  bool host_pipeline = true;
 
   cudaError_t stage(int s, bool rk, bool eig) {
     return exact ? nuc3d::exact::run_stage(L, s, rk, eig) : nuc3d::fast::run_stage(L, s, rk, eig);
@@ -237,6 +240,8 @@ int nuc3d_destroy(nuc3d_ctx *c) {
   if (c->d_jobs) cudaFree(c->d_jobs);
   if (c->d_state) cudaFree(c->d_state);
   for (auto ev : c->ev_chunk) cudaEventDestroy(ev);
+  for (auto *v : {&c->ev_up, &c->ev_zeta, &c->ev_down})
+    for (auto ev : *v) cudaEventDestroy(ev);
   for (auto ev : {c->ev_start, c->ev_h2d, c->ev_step, c->ev_end})
     if (ev) cudaEventDestroy(ev);
   for (auto st : {c->h2d, c->d2h})
@@ -511,13 +516,14 @@ extern "C" {
 
 // Directions whose compact scheme (crweno5, hccs; not the whole-line hccs77 system) runs
 // the fused compact_line_kernel: the throughput build, every block's line at most
-// kLineMax cells with at least 2 rows in its system.
+// kLineMax cells with at least 2 rows in its system, and the kernel's tile fitting in
+// shared memory (a Navier-Stokes tile of several lines may not).
 static void set_line_dirs(nuc3d_ctx *c) {
   int dirs = 0;
   for (int d = 0; d < 3 && !c->exact && c->compact_fused; ++d) {
     const int sc = c->P.scheme[d];
     if (sc != SCH_CRWENO5 && sc != SCH_HCCS) continue;
-    bool ok = true;
+    bool ok = nuc3d::fast::compact_line_smem(d, sc, c->P.model == MODEL_NS) <= kSmemOptin;
     for (const HostBlock &b : c->blocks)
       ok = ok && b.n[d] <= kLineMax && b.n[d] - 2 * c->P.ts[d] + 1 >= 2;
     if (ok) dirs |= 1 << d;
@@ -613,7 +619,11 @@ int nuc3d_finalize(nuc3d_ctx *c) {
           L.tm_dir[d].tile_start[bi] + nuc3d::exact::tile_count(d, b.n, L.shape[d]);
       const long long nsys = 10 * (b.N / b.n[d]);
       L.tm_sys[d].tile_start[bi + 1] = L.tm_sys[d].tile_start[bi] + (int)((nsys + 255) / 256);
-      L.tm_line[d].tile_start[bi + 1] = L.tm_line[d].tile_start[bi] + (int)(b.N / b.n[d]);
+      {  // fused compact sweep: groups of tile_w(line_shape(d)) lanes per outer index
+        const long long nW = d == 0 ? b.n[1] : b.n[0], nO = d == 2 ? b.n[1] : b.n[2];
+        const long long lw = tile_w(line_shape(d));
+        L.tm_line[d].tile_start[bi + 1] = L.tm_line[d].tile_start[bi] + (int)(((nW + lw - 1) / lw) * nO);
+      }
     }
     L.tm_cells.tile_start[bi + 1] = L.tm_cells.tile_start[bi] + (int)((b.N + 255) / 256);
   }
@@ -825,6 +835,102 @@ struct EventPair {
 #endif
 constexpr size_t kHostChunk = (size_t)NUC3D_HOST_CHUNK_MB << 20;
 
+// nuc3d_solve_host for one Euler block with explicit schemes, as a copy/compute pipeline
+// over z-slabs (the zeta sweep's z-chunks): the upload of slab s is followed at once by
+// stage 0's BC, xi and eta work on that slab (their lines stay inside a z-plane), and the
+// download of slab s follows stage 2's zeta sweep over that slab, while the copy engines
+// move the other slabs.  The kernels and tiles are one_step's, so the results are too.
+static bool slab_pipeline_ok(const nuc3d_ctx *c) {
+  if (!c->host_pipeline || c->blocks.size() != 1 || c->P.model != MODEL_EULER || c->P.sensor)
+    return false;
+  for (int d = 0; d < 3; ++d)
+    if (c->P.scheme[d] == SCH_CRWENO5 || c->P.scheme[d] == SCH_HCCS || c->P.scheme[d] == SCH_HCCS77)
+      return false;
+  return c->blocks[0].n[2] >= 2 * tile_l(c->L.shape[2]);
+}
+
+static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
+  const HostBlock &b = c->blocks[0];
+  const int nx = b.n[0], ny = b.n[1], nz = b.n[2];
+  const int *sh = c->L.shape;
+  const int TLz = tile_l(sh[2]), ns = (nz + TLz - 1) / TLz;
+  const int zper = ((nx + tile_w(sh[2]) - 1) / tile_w(sh[2])) * ny;                      // zeta tiles per chunk
+  const int xper = ((nx + tile_l(sh[0]) - 1) / tile_l(sh[0])) * ((ny + tile_w(sh[0]) - 1) / tile_w(sh[0]));
+  const int yper = ((ny + tile_l(sh[1]) - 1) / tile_l(sh[1])) * ((nx + tile_w(sh[1]) - 1) / tile_w(sh[1]));
+  for (auto *v : {&c->ev_up, &c->ev_zeta, &c->ev_down})
+    while ((int)v->size() < ns) {
+      cudaEvent_t ev;
+      CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      v->push_back(ev);
+    }
+  const size_t plane = (size_t)nx * ny;
+  auto copy_slab = [&](int s, bool up, cudaStream_t st) -> cudaError_t {
+    const int k0 = s * TLz, k1 = std::min(nz, k0 + TLz);
+    for (int v = 0; v < 5; ++v) {
+      const size_t off = (size_t)v * b.N + (size_t)k0 * plane, n = (size_t)(k1 - k0) * plane;
+      cudaError_t e = up ? cudaMemcpyAsync(b.q[0] + off, q_host + off, n * sizeof(double),
+                                           cudaMemcpyHostToDevice, st)
+                         : cudaMemcpyAsync(q_host + off, b.q[0] + off, n * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  const Launch &L = c->L;
+  auto run = [&](auto fast_fn, auto exact_fn) { return c->exact ? exact_fn() : fast_fn(); };
+  CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
+  CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_start, 0));
+  for (int step = 0; step < nsteps; ++step) {
+    for (int s = 0; s < ns; ++s) {
+      // the host slab is read only once the previous step's download has written it
+      if (step > 0) CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_down[s], 0));
+      CUDA_TRY(copy_slab(s, true, c->h2d));
+      CUDA_TRY(cudaEventRecord(c->ev_up[s], c->h2d));
+    }
+    CUDA_TRY(cudaMemsetAsync(&c->d_state->max_eig_bits, 0, sizeof(unsigned long long), c->stream));
+    for (int s = 0; s < ns; ++s) {
+      const int k0 = s * TLz, k1 = std::min(nz, k0 + TLz);
+      CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_up[s], 0));
+      CUDA_TRY(run([&] { return nuc3d::fast::run_stage0_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper, k1 * yper); },
+                   [&] { return nuc3d::exact::run_stage0_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper, k1 * yper); }));
+    }
+    CUDA_TRY(run([&] { return nuc3d::fast::run_stage0_zeta(L); }, [&] { return nuc3d::exact::run_stage0_zeta(L); }));
+    CUDA_TRY(run([&] { return nuc3d::fast::run_stage(L, 1, true, false); },
+                 [&] { return nuc3d::exact::run_stage(L, 1, true, false); }));
+    CUDA_TRY(run([&] { return nuc3d::fast::run_stage2_head(L); }, [&] { return nuc3d::exact::run_stage2_head(L); }));
+    for (int s = 0; s < ns; ++s) {
+      CUDA_TRY(run([&] { return nuc3d::fast::run_stage2_zeta(L, s * zper, (s + 1) * zper); },
+                   [&] { return nuc3d::exact::run_stage2_zeta(L, s * zper, (s + 1) * zper); }));
+      CUDA_TRY(cudaEventRecord(c->ev_zeta[s], c->stream));
+    }
+    if (L.d_res_last)
+      CUDA_TRY(run([&] { return nuc3d::fast::run_residual(L, false); },
+                   [&] { return nuc3d::exact::run_residual(L, false); }));
+    for (int s = 0; s < ns; ++s) {
+      CUDA_TRY(cudaStreamWaitEvent(c->d2h, c->ev_zeta[s], 0));
+      CUDA_TRY(copy_slab(s, false, c->d2h));
+      CUDA_TRY(cudaEventRecord(c->ev_down[s], c->d2h));
+    }
+  }
+  CUDA_TRY(cudaEventRecord(c->ev_end, c->d2h));
+  CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_end, 0));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+int nuc3d_set_host_pipeline(nuc3d_ctx *c, int on) {
+  if (!c) return fail(NUC3D_EINVAL, "null context");
+  c->host_pipeline = on != 0;
+  return NUC3D_OK;
+}
+
+int nuc3d_get_host_pipeline(nuc3d_ctx *c, int *on) {
+  if (!c || !on) return fail(NUC3D_EINVAL, "null argument");
+  if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
+  *on = slab_pipeline_ok(c) ? (c->blocks[0].n[2] + tile_l(c->L.shape[2]) - 1) / tile_l(c->L.shape[2]) : 0;
+  return NUC3D_OK;
+}
+
 int nuc3d_solve_host(nuc3d_ctx *c, double *const *q_host, int nsteps) {
   if (!c || !q_host) return fail(NUC3D_EINVAL, "null argument");
   if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
@@ -832,18 +938,19 @@ int nuc3d_solve_host(nuc3d_ctx *c, double *const *q_host, int nsteps) {
   for (size_t b = 0; b < c->blocks.size(); ++b)
     if (!q_host[b]) return fail(NUC3D_EINVAL, "q_host[%zu] is null", b);
   cudaSetDevice(c->device);
+  if (!c->h2d) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+    for (cudaEvent_t *ev : {&c->ev_start, &c->ev_h2d, &c->ev_step, &c->ev_end})
+      CUDA_TRY(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  }
+  if (slab_pipeline_ok(c)) return solve_host_slabs(c, q_host[0], nsteps);
   struct Chunk { int b; size_t off, bytes; };
   std::vector<Chunk> chunks;
   for (size_t b = 0; b < c->blocks.size(); ++b) {
     const size_t total = 5 * (size_t)c->blocks[b].N * sizeof(double);
     for (size_t off = 0; off < total; off += kHostChunk)
       chunks.push_back({(int)b, off, std::min(kHostChunk, total - off)});
-  }
-  if (!c->h2d) {
-    CUDA_TRY(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
-    CUDA_TRY(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
-    for (cudaEvent_t *ev : {&c->ev_start, &c->ev_h2d, &c->ev_step, &c->ev_end})
-      CUDA_TRY(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
   }
   while (c->ev_chunk.size() < chunks.size()) {
     cudaEvent_t ev;

@@ -166,6 +166,19 @@ __device__ __forceinline__ void crweno5_row(const double f[5], double &lo, doubl
                                             double &rhs) {
   W5 r = w5_parts(f[0], f[1], f[2], f[3], f[4], false);
   const double ss = 1.0e-6;
+#if NUC3D_FAST
+  // The row scaled by sum_k alpha_k * prod_k (ss+is_k)^2 (its solution is unchanged): the
+  // weights become n_k = c_k prod_{j!=k} (ss+is_j)^2, with no division at all.
+  {
+    const double d0 = sq(ss + r.is0), d1 = sq(ss + r.is1), d2 = sq(ss + r.is2);
+    const double n0 = kCR5[0] * (d1 * d2), n1 = kCR5[1] * (d0 * d2), n2 = kCR5[2] * (d0 * d1);
+    lo = 2.0 / 3.0 * n0 + 1.0 / 3.0 * n1;
+    di = 1.0 / 3.0 * n0 + 2.0 / 3.0 * (n1 + n2);
+    up = 1.0 / 3.0 * n2;
+    rhs = 1.0 / 6.0 * n0 * f[1] + (5.0 * (n0 + n1) + n2) * (1.0 / 6.0) * f[2] + (n1 + 5.0 * n2) * (1.0 / 6.0) * f[3];
+    return;
+  }
+#endif
   double a0 = kCR5[0] / sq(ss + r.is0);
   double a1 = kCR5[1] / sq(ss + r.is1);
   double a2 = kCR5[2] / sq(ss + r.is2);
@@ -184,6 +197,28 @@ __device__ __forceinline__ void hccs_row(const double f[5], double &lo, double &
                                          double &rhs) {
   W5 r = w5_parts(f[0], f[1], f[2], f[3], f[4], false);
   const double ss = 1.0e-40;
+#if NUC3D_FAST
+  // alpha_k = c_k (e_k + tau^2) / e_k, e_k = (is_k + ss)^2: with den = e0 e1 e2 the
+  // numerators m_k = c_k (e_k + tau^2) prod_{j!=k} e_j sum to S = den * sum alpha, so theta
+  // takes one division (sum alpha = S / den) and its reciprocal a second; the WENO part of
+  // the row is scaled by S and the central part by S as well (the solution is unchanged).
+  {
+    const double tau = fabs(r.is2 - r.is0), t2 = tau * tau;
+    const double e0 = sq(r.is0 + ss), e1 = sq(r.is1 + ss), e2 = sq(r.is2 + ss);
+    const double m0 = kCR5[0] * (e0 + t2) * (e1 * e2), m1 = kCR5[1] * (e1 + t2) * (e0 * e2),
+                 m2 = kCR5[2] * (e2 + t2) * (e0 * e1);
+    const double S = m0 + m1 + m2;
+    const double sa = qdiv(S, e0 * (e1 * e2));
+    const double theta = qdiv(1.0, 1.0 + sq(sa - 1.0)), omt = 1.0 - theta, ts = theta * S;
+    const double q7 = (-f[0] + 19.0 * f[1] + 239.0 * f[2] + 159.0 * f[3] + 4.0 * f[4]) * (1.0 / 420.0);
+    lo = (2.0 / 3.0 * m0 + 1.0 / 3.0 * m1) * omt + 2.0 / 7.0 * ts;
+    di = (1.0 / 3.0 * m0 + 2.0 / 3.0 * (m1 + m2)) * omt + 4.0 / 7.0 * ts;
+    up = (1.0 / 3.0 * m2) * omt + 1.0 / 7.0 * ts;
+    rhs = (1.0 / 6.0 * m0 * f[1] + (5.0 * (m0 + m1) + m2) * (1.0 / 6.0) * f[2] +
+           (m1 + 5.0 * m2) * (1.0 / 6.0) * f[3]) * omt + q7 * ts;
+    return;
+  }
+#endif
   double q7 = (-f[0] + 19.0 * f[1] + 239.0 * f[2] + 159.0 * f[3] + 4.0 * f[4]) / 420.0;
   double tau = fabs(r.is2 - r.is0);
   double a0 = kCR5[0] * (1.0 + sq(tau / (r.is0 + ss)));

@@ -231,7 +231,7 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
   const bool rk = (flags & SW_RK) != 0;
   const bool need_r = DIR != 0;                      // RHS read (eta += , zeta +=)
   const bool need_n = DIR == 2 && rk && stage != 0;  // u_n read (RK stages 1, 2)
-  const int ntile = tm.tile_start[tm.nblocks];
+  const int ntile = tile_range(tm);  // tiles tm.base .. tm.base + ntile - 1
   const int nmine = (int)blockIdx.x < ntile ? (ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int tid = threadIdx.x;
   // The tensor copies need 128-byte aligned shared-memory destinations; every offset above
@@ -259,7 +259,7 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
     unsigned nq[2] = {0, 0}, nr = 0;  // phases armed per barrier
     bool ok = true;
     auto issue_q = [&](int k, int s) {
-      const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P, (int)blockIdx.x + k * (int)gridDim.x);
+      const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P, tm.base + (int)blockIdx.x + k * (int)gridDim.x);
       unsigned char *slot = psm + s * L::SLOT;
       const CUtensorMap *mp = maps + ((size_t)T.b * 3 + DIR) * PM_COUNT;
       if (lane == 0) {
@@ -282,7 +282,7 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
     };
     auto issue_r = [&](int k) {
       if (lane == 0) {
-        const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P, (int)blockIdx.x + k * (int)gridDim.x);
+        const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P, tm.base + (int)blockIdx.x + k * (int)gridDim.x);
         const CUtensorMap *mp = maps + ((size_t)T.b * 3 + DIR) * PM_COUNT;
         int x, y, z;
         pipe_origin<DIR, SCH, SHP>(T, false, x, y, z);
@@ -322,7 +322,7 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
   bool ok = true;
   for (int k = 0; k < nmine; ++k) {
     const int s = k & 1;
-    const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P, (int)blockIdx.x + k * (int)gridDim.x);
+    const TileCtx T = decode_tile<DIR, SHP>(blocks, tm, P, tm.base + (int)blockIdx.x + k * (int)gridDim.x);
     const BlockDev &B = *T.B;
     const unsigned char *slot = psm + s * L::SLOT;
     const double *Qh = reinterpret_cast<const double *>(slot + L::Q);

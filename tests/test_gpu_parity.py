@@ -296,3 +296,44 @@ def test_autotune_picks_and_caches():
     assert r3["shape"][0] == 0 and r3["shape"][1] == 0 and r3["ms"][0] == [None] * 3
     with pytest.raises(nb.Nuc3dError):
         s3.set_tiles((1, 0, 0))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("exact", [True, False])
+def test_solve_host_slab_pipeline_equals_device_steps(exact):
+    """nuc3d_solve_host's copy/compute pipeline over z-slabs (a 48 x 40 x 136 block: the
+    zeta sweep's 64-cell z-chunks make three slabs, the last one short) equals the same
+    steps on the device-resident state bit for bit, residual and time included, and so
+    does the whole-state chunked path it replaces."""
+    import torch
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+    shape = (48, 40, 136)
+    q0, m = C.spherical_riemann(shape)
+
+    def make():
+        s = nb.Solver(nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="Euler3d",
+                                mach=1.0, exact=exact, weno5z_compat=True))
+        b = s.add_block(*shape, *C.outlet_faces())
+        s.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
+        s.finalize()
+        s.set_q(b, q0)
+        s.set_tiles((0, 0, 0))
+        return s, b
+
+    s1, b1 = make()
+    s1.step(5)
+    ref = s1.get_q(b1), s1.time_dt(), s1.residual()
+    s1.close()
+    for pipe, slabs in ((True, 3), (False, 0)):
+        s2, b2 = make()
+        s2.set_host_pipeline(pipe)
+        assert s2.host_pipeline() == slabs
+        host = torch.empty(q0.size, dtype=torch.float64, pin_memory=True)
+        host.numpy()[:] = q0.reshape(-1)
+        s2.solve_host([host.data_ptr()], 5)
+        got = host.numpy().reshape(q0.shape).copy()
+        assert np.array_equal(got, ref[0]), (pipe, rel_max(got, ref[0]))
+        assert s2.time_dt() == ref[1] and s2.residual() == ref[2]
+        assert np.array_equal(s2.get_q(b2), ref[0])
+        s2.close()
