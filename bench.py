@@ -320,6 +320,8 @@ def ours(args):
     if args.tiles:
         s.set_tiles(args.tiles)
         tiles = s.get_tiles()
+        if args.pipe_mask is not None:
+            s.set_pipeline(args.pipe_mask if args.pipe_mask > 1 else bool(args.pipe_mask))
     else:
         tiles = s.autotune(reps=3)["shape"]
 
@@ -994,6 +996,8 @@ def main():
                     help="leave out the 24-block Navier-Stokes line of the default run")
     ap.add_argument("--tiles", type=lambda x: tuple(int(v) for v in x.split(",")), default=None,
                     help="sweep tile shapes per direction, e.g. 2,0,0 (default: nuc3d_autotune)")
+    ap.add_argument("--pipe-mask", type=int, default=None,
+                    help="with --tiles: pipelined directions, bit d = direction d (e.g. 4: zeta)")
     ap.add_argument("--workload", default="sphere256",
                     choices=["sphere256", "turbulence24", "shock_turbulence", "boundary_layer",
                              "compact"],

@@ -373,9 +373,11 @@ class Solver:
         _check(self.lib.nuc3d_get_residual(self._ctx, ctypes.byref(r)))
         return r.value
 
-    def set_pipeline(self, on: bool) -> None:
-        """Persistent TMA-fed sweeps on (default) or off; results are identical."""
-        _check(self.lib.nuc3d_set_pipeline(self._ctx, 1 if on else 0))
+    def set_pipeline(self, on) -> None:
+        """Persistent TMA-fed sweeps on (default) or off, or an int bitmask of directions
+        (bit d: direction d; values above 1); results are identical."""
+        v = int(on) if not isinstance(on, bool) else (1 if on else 0)
+        _check(self.lib.nuc3d_set_pipeline(self._ctx, v))
 
     def pipeline(self) -> int:
         """Directions (bit d) whose sweeps run pipelined (Euler, even nx, switched on);

@@ -612,6 +612,8 @@ int nuc3d_finalize(nuc3d_ctx *c) {
   }
   L.tm_cells.nblocks = nbk;
   L.tm_cells.tile_start[0] = 0;
+  L.tm_grad.nblocks = nbk;
+  L.tm_grad.tile_start[0] = 0;
   for (int bi = 0; bi < nbk; ++bi) {
     const HostBlock &b = c->blocks[bi];
     for (int d = 0; d < 3; ++d) {
@@ -626,6 +628,7 @@ int nuc3d_finalize(nuc3d_ctx *c) {
       }
     }
     L.tm_cells.tile_start[bi + 1] = L.tm_cells.tile_start[bi] + (int)((b.N + 255) / 256);
+    L.tm_grad.tile_start[bi + 1] = L.tm_grad.tile_start[bi] + nuc3d::exact::grad_tiles(b.n);
   }
   // physical faces for the BC ghost pass
   std::vector<FaceJobs> jv(1);
@@ -1363,7 +1366,7 @@ int nuc3d_set_pipeline(nuc3d_ctx *c, int on) {
   cudaSetDevice(c->device);
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->use_pipe = on != 0;
-  c->pipe_mask = on ? 7 : 0;
+  c->pipe_mask = on == 1 ? 7 : (on & 7);  // 1: every direction; else a bitmask of directions
   c->drop_graph();
   return build_maps(c);
 }
