@@ -86,7 +86,9 @@ constexpr int kLineShape4 = 4;
 #endif
 constexpr int kLineLanes = NUC3D_LINE_LANES;
 constexpr int kLineMax = 256;
-constexpr size_t kSmemOptin = 227 * 1024;  // dynamic shared memory per CTA (opt-in maximum)
+// dynamic shared memory a CTA may opt in to: the 227 KB per-block maximum less 1 KB for the
+// kernels' static shared memory (the attribute must leave room for it)
+constexpr size_t kSmemOptin = 227 * 1024 - 1024;
 __host__ __device__ constexpr int line_shape(int dir) { return dir == 0 ? kLineShape : kLineShape4; }
 __host__ __device__ constexpr int tile_w(int s) {
   return s == 1 ? 8 : (s == 2 ? 2 : (s == 3 ? 1 : (s == 4 ? kLineLanes : 4)));
