@@ -82,7 +82,7 @@ constexpr int kTileShapes = 3;
 constexpr int kLineShape = 3;
 constexpr int kLineShape4 = 4;
 #ifndef NUC3D_LINE_LANES
-#define NUC3D_LINE_LANES 4
+#define NUC3D_LINE_LANES 2  // 4: one CTA per SM, measured slower
 #endif
 constexpr int kLineLanes = NUC3D_LINE_LANES;
 constexpr int kLineMax = 256;
@@ -206,7 +206,6 @@ struct Launch {
   TileMap tm_sys[3];       // compact schemes: 256-system tiles per direction
   TileMap tm_cells;
   TileMap tm_line[3];      // fused compact sweeps: one tile per line
-  TileMap tm_grad;         // z-marching slabs of the Navier-Stokes gradient kernel
   int line_dirs;           // bit d: direction d's compact scheme runs compact_line_kernel
   const FaceJobs *d_jobs;  // device copy
   int bc_tiles;            // CTAs of the BC ghost pass (0: no physical faces)
@@ -271,8 +270,6 @@ cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 // out = FluxL, FluxR (5N), reconstFluxL, reconstFluxR (5 (L+1) nl), dF (5N), device.
 cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const out[5]);
 // compact_line_smem(): dynamic shared memory of the fused compact sweep (0: none).
-// grad_tiles(): CTAs of the slab gradient kernel over a block of n cells.
-int grad_tiles(const int n[3]);
 size_t compact_line_smem(int dir, int sch, bool ns);
 cudaError_t configure();
 int tile_count(int dir, const int n[3], int shape);
@@ -299,8 +296,6 @@ cudaError_t run_sweep(const Launch &L, int dir, int stage, int flags);
 // out = FluxL, FluxR (5N), reconstFluxL, reconstFluxR (5 (L+1) nl), dF (5N), device.
 cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const out[5]);
 // compact_line_smem(): dynamic shared memory of the fused compact sweep (0: none).
-// grad_tiles(): CTAs of the slab gradient kernel over a block of n cells.
-int grad_tiles(const int n[3]);
 size_t compact_line_smem(int dir, int sch, bool ns);
 cudaError_t configure();
 int tile_count(int dir, const int n[3], int shape);

@@ -1696,107 +1696,6 @@ __device__ __forceinline__ void visc_flux_cell(const BlockDev &B, const SolverPa
 #endif
 }
 
-// The same gradients and fluxes by z-marching slabs (NaiverStokesData3d::solveGrads,
-// src/NaiverStokes3d.cpp:63-128): a CTA of kGradTX x kGradTY threads owns that many
-// (i, j) columns of a block and walks kGradKZ planes of them.  Each thread keeps its
-// column's primitives of the planes k - H .. k + H in a shared ring (the zeta
-// differences); the current plane with its x and y halos sits in a shared tile (the xi and
-// eta differences), filled from the ring inside the CTA's columns and from global memory
-// on the halo band.  So each value is read from global memory about twice instead of the
-// 19 reads of the one-thread-per-cell kernel.  Cells whose stencil leaves the block take the
-// same out-of-line edge path (neighbour ghosts, one-sided schemes); the differences are the
-// same operations on the same values, so the results are too.
-#ifndef NUC3D_GRAD_SLAB
-#define NUC3D_GRAD_SLAB 1  // 0: the one-thread-per-cell grad_kernel
-#endif
-constexpr int kGradTX = 32, kGradTY = 8, kGradKZ = 32, kGradH = kVisHalo;
-constexpr int kGradHX = kGradTX + 2 * kGradH, kGradHY = kGradTY + 2 * kGradH;
-constexpr int kGradRing = 2 * kGradH + 1, kGradCols = kGradTX * kGradTY;
-constexpr size_t kGradSmem = sizeof(double) * (size_t)4 * (kGradHX * kGradHY + kGradRing * kGradCols);
-
-// The direction's scheme_vis operator on values V(o) at offsets o along the line.
-template <class Acc>
-__device__ __forceinline__ double diff_acc(Acc V, int vis) {
-  if (vis == VIS_CD2) return cd2(V(-1), V(1));
-  if (vis == VIS_CD8) return cd8(V(-4), V(-3), V(-2), V(-1), V(1), V(2), V(3), V(4));
-  return cd6(V(-3), V(-2), V(-1), V(1), V(2), V(3));
-}
-
-__host__ __device__ inline int grad_slab_tiles(const int n[3]) {
-  return ((n[0] + kGradTX - 1) / kGradTX) * ((n[1] + kGradTY - 1) / kGradTY) *
-         ((n[2] + kGradKZ - 1) / kGradKZ);
-}
-
-__global__ void __launch_bounds__(kGradCols, 2)
-grad_slab_kernel(const BlockDev *__restrict__ blocks, TileMap tm, SolverParams P) {
-  extern __shared__ double gsm[];
-  double *hp = gsm;                                    // [4][HY][HX]: plane k with halos
-  double *ring = gsm + 4 * kGradHX * kGradHY;          // [ring][4][cols]: planes k-H .. k+H
-  const int b = find_block(tm, blockIdx.x);
-  const BlockDev &B = blocks[b];
-  const int nx = B.n[0], ny = B.n[1], nz = B.n[2];
-  const long long N = B.N, plane = (long long)nx * ny;
-  const int gx = (nx + kGradTX - 1) / kGradTX, gy = (ny + kGradTY - 1) / kGradTY;
-  const int lt = (int)blockIdx.x - tm.tile_start[b];
-  const int txi = lt % gx, r0 = lt / gx, tyi = r0 % gy, tzi = r0 / gy;
-  const int i0 = txi * kGradTX, j0 = tyi * kGradTY, k0 = tzi * kGradKZ;
-  const int k1 = min(nz, k0 + kGradKZ);
-  const int tx = (int)threadIdx.x % kGradTX, ty = (int)threadIdx.x / kGradTX;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = i < nx && j < ny;
-  auto slot = [](int kk) { return ((kk % kGradRing) + kGradRing) % kGradRing; };
-  auto ring_load = [&](int kk) {  // this thread's column at plane kk (inside the block)
-    if (!own || kk < 0 || kk >= nz) return;
-    double *rs = ring + slot(kk) * 4 * kGradCols + threadIdx.x;
-    const long long g = kk * plane + (long long)j * nx + i;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) rs[c * kGradCols] = __ldg(B.prim + c * N + g);
-  };
-  for (int kk = k0 - kGradH; kk < k0 + kGradH; ++kk) ring_load(kk);
-  for (int k = k0; k < k1; ++k) {
-    ring_load(k + kGradH);
-    __syncthreads();  // plane k in the ring is complete (and plane k-1's tile is no longer read)
-    const double *rk = ring + slot(k) * 4 * kGradCols;
-    for (int e = threadIdx.x; e < kGradHX * kGradHY; e += kGradCols) {
-      const int x = e % kGradHX, y = e / kGradHX, ii = i0 - kGradH + x, jj = j0 - kGradH + y;
-      const bool in = x >= kGradH && x < kGradH + kGradTX && y >= kGradH && y < kGradH + kGradTY;
-      if (ii < 0 || ii >= nx || jj < 0 || jj >= ny) continue;  // never read (edge path)
-      const long long g = k * plane + (long long)jj * nx + ii;
-      const int col = (y - kGradH) * kGradTX + (x - kGradH);
-#pragma unroll
-      for (int c = 0; c < 4; ++c)
-        hp[(c * kGradHY + y) * kGradHX + x] = in ? rk[c * kGradCols + col] : __ldg(B.prim + c * N + g);
-    }
-    __syncthreads();
-    if (own) {
-      double gr[4][3];
-      const int pos[3] = {i, j, k};
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        if (pos[d] >= P.ts[d] && pos[d] < B.n[d] - P.ts[d]) {
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            if (d == 2) {
-              const double *rc = ring + c * kGradCols + threadIdx.x;
-              gr[c][2] = diff_acc([&](int o) { return rc[slot(k + o) * 4 * kGradCols]; }, P.vis[2]);
-            } else {
-              const double *f = hp + (c * kGradHY + ty + kGradH) * kGradHX + tx + kGradH;
-              const int st = d == 0 ? 1 : kGradHX;
-              gr[c][d] = diff_acc([&](int o) { return f[o * st]; }, P.vis[d]);
-            }
-          }
-        } else {
-          double g4[4];
-          prim_grad_edge(blocks, B, P, d, i, j, k, 0, 4, g4);
-#pragma unroll
-          for (int c = 0; c < 4; ++c) gr[c][d] = g4[c];
-        }
-      }
-      visc_flux_cell(B, P, (long long)k * plane + (long long)j * nx + i, gr);
-    }
-  }
-}
-
 // NaiverStokesData3d::solveGrads + solveViscousFlux (src/NaiverStokes3d.cpp:63-326)
 // with physicsModel::sutherland (src/physicsModel.cpp:199-234).
 #ifndef NUC3D_GRAD_MINB
@@ -2240,12 +2139,7 @@ inline cudaError_t launch_stage(const Launch &L, int stage, bool rk, bool eig) {
     const int nt = L.tm_cells.tile_start[L.tm_cells.nblocks];
     prim_kernel<<<nt, kCellTile, 0, L.stream>>>(L.d_blocks, L.tm_cells, L.P, L.d_state, stage);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-#if NUC3D_GRAD_SLAB
-    grad_slab_kernel<<<L.tm_grad.tile_start[L.tm_grad.nblocks], kGradCols, kGradSmem, L.stream>>>(
-        L.d_blocks, L.tm_grad, L.P);
-#else
     grad_kernel<<<nt, kCellTile, 0, L.stream>>>(L.d_blocks, L.tm_cells, L.P);
-#endif
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   const int nsf = ns ? SW_NS : 0;
@@ -2464,9 +2358,7 @@ inline cudaError_t configure_dir() {
 }
 
 cudaError_t configure() {
-  cudaError_t e = cudaFuncSetAttribute(grad_slab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kGradSmem);
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
   if ((e = configure_dir<0>()) != cudaSuccess) return e;
   if ((e = configure_dir<1>()) != cudaSuccess) return e;
   return configure_dir<2>();
@@ -2633,8 +2525,6 @@ cudaError_t run_taps(const Launch &L, int block, int dir, int nl, double *const 
 }
 
 int tile_count(int dir, const int n[3], int shape) { return sweep_tiles(dir, n, shape); }
-
-int grad_tiles(const int n[3]) { return grad_slab_tiles(n); }
 
 size_t compact_line_smem(int dir, int sch, bool ns) {
 #if NUC3D_FAST

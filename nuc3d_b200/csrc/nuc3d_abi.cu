@@ -612,8 +612,6 @@ int nuc3d_finalize(nuc3d_ctx *c) {
   }
   L.tm_cells.nblocks = nbk;
   L.tm_cells.tile_start[0] = 0;
-  L.tm_grad.nblocks = nbk;
-  L.tm_grad.tile_start[0] = 0;
   for (int bi = 0; bi < nbk; ++bi) {
     const HostBlock &b = c->blocks[bi];
     for (int d = 0; d < 3; ++d) {
@@ -628,7 +626,6 @@ int nuc3d_finalize(nuc3d_ctx *c) {
       }
     }
     L.tm_cells.tile_start[bi + 1] = L.tm_cells.tile_start[bi] + (int)((b.N + 255) / 256);
-    L.tm_grad.tile_start[bi + 1] = L.tm_grad.tile_start[bi] + nuc3d::exact::grad_tiles(b.n);
   }
   // physical faces for the BC ghost pass
   std::vector<FaceJobs> jv(1);
@@ -852,6 +849,11 @@ static bool slab_pipeline_ok(const nuc3d_ctx *c) {
   return c->blocks[0].n[2] >= 2 * tile_l(c->L.shape[2]);
 }
 
+#ifndef NUC3D_HOST_PIECES
+#define NUC3D_HOST_PIECES 4  // copy pieces per slab
+#endif
+constexpr int kHostPieces = NUC3D_HOST_PIECES;
+
 static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
   const HostBlock &b = c->blocks[0];
   const int nx = b.n[0], ny = b.n[1], nz = b.n[2];
@@ -860,15 +862,26 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
   const int zper = ((nx + tile_w(sh[2]) - 1) / tile_w(sh[2])) * ny;                      // zeta tiles per chunk
   const int xper = ((nx + tile_l(sh[0]) - 1) / tile_l(sh[0])) * ((ny + tile_w(sh[0]) - 1) / tile_w(sh[0]));
   const int yper = ((ny + tile_l(sh[1]) - 1) / tile_l(sh[1])) * ((nx + tile_w(sh[1]) - 1) / tile_w(sh[1]));
+  // copies move pieces of kHostPieces z-ranges per slab: the upload of a piece waits only
+  // for the download of the same piece, so the last slab's round trip is short
+  const int np = ns * kHostPieces;
   for (auto *v : {&c->ev_up, &c->ev_zeta, &c->ev_down})
-    while ((int)v->size() < ns) {
+    while ((int)v->size() < np) {
       cudaEvent_t ev;
       CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
       v->push_back(ev);
     }
   const size_t plane = (size_t)nx * ny;
-  auto copy_slab = [&](int s, bool up, cudaStream_t st) -> cudaError_t {
-    const int k0 = s * TLz, k1 = std::min(nz, k0 + TLz);
+  auto piece_range = [&](int p, int &k0, int &k1) {
+    const int s = p / kHostPieces, q = p % kHostPieces;
+    const int s0 = s * TLz, s1 = std::min(nz, s0 + TLz), len = s1 - s0;
+    k0 = s0 + len * q / kHostPieces;
+    k1 = s0 + len * (q + 1) / kHostPieces;
+  };
+  auto copy_piece = [&](int p, bool up, cudaStream_t st) -> cudaError_t {
+    int k0, k1;
+    piece_range(p, k0, k1);
+    if (k1 <= k0) return cudaSuccess;
     for (int v = 0; v < 5; ++v) {
       const size_t off = (size_t)v * b.N + (size_t)k0 * plane, n = (size_t)(k1 - k0) * plane;
       cudaError_t e = up ? cudaMemcpyAsync(b.q[0] + off, q_host + off, n * sizeof(double),
@@ -884,16 +897,17 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
   CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
   CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_start, 0));
   for (int step = 0; step < nsteps; ++step) {
-    for (int s = 0; s < ns; ++s) {
-      // the host slab is read only once the previous step's download has written it
-      if (step > 0) CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_down[s], 0));
-      CUDA_TRY(copy_slab(s, true, c->h2d));
-      CUDA_TRY(cudaEventRecord(c->ev_up[s], c->h2d));
+    for (int p = 0; p < np; ++p) {
+      // the host piece is read only once the previous step's download has written it
+      if (step > 0) CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_down[p], 0));
+      CUDA_TRY(copy_piece(p, true, c->h2d));
+      CUDA_TRY(cudaEventRecord(c->ev_up[p], c->h2d));
     }
     CUDA_TRY(cudaMemsetAsync(&c->d_state->max_eig_bits, 0, sizeof(unsigned long long), c->stream));
     for (int s = 0; s < ns; ++s) {
       const int k0 = s * TLz, k1 = std::min(nz, k0 + TLz);
-      CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_up[s], 0));
+      // the slab's last piece (the copy stream runs the pieces in order)
+      CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_up[(s + 1) * kHostPieces - 1], 0));
       CUDA_TRY(run([&] { return nuc3d::fast::run_stage0_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper, k1 * yper); },
                    [&] { return nuc3d::exact::run_stage0_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper, k1 * yper); }));
     }
@@ -909,10 +923,10 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
     if (L.d_res_last)
       CUDA_TRY(run([&] { return nuc3d::fast::run_residual(L, false); },
                    [&] { return nuc3d::exact::run_residual(L, false); }));
-    for (int s = 0; s < ns; ++s) {
-      CUDA_TRY(cudaStreamWaitEvent(c->d2h, c->ev_zeta[s], 0));
-      CUDA_TRY(copy_slab(s, false, c->d2h));
-      CUDA_TRY(cudaEventRecord(c->ev_down[s], c->d2h));
+    for (int p = 0; p < np; ++p) {
+      if (p % kHostPieces == 0) CUDA_TRY(cudaStreamWaitEvent(c->d2h, c->ev_zeta[p / kHostPieces], 0));
+      CUDA_TRY(copy_piece(p, false, c->d2h));
+      CUDA_TRY(cudaEventRecord(c->ev_down[p], c->d2h));
     }
   }
   CUDA_TRY(cudaEventRecord(c->ev_end, c->d2h));
