@@ -263,8 +263,9 @@ int nuc3d_autotune(nuc3d_ctx *ctx, int reps, int shape_out[3], double ms_out[9])
 /* Pipelined sweeps (after nuc3d_finalize; on by default).  No counterpart in the reference.
    With it on, each explicit-scheme sweep is a persistent kernel (two CTAs per SM) whose
    producer warp loads the next tiles' state, Jacobian and metric with tensor-map (TMA)
-   copies while the other warps compute; results are identical either way.  It applies to
-   Euler3d contexts whose blocks all have an even nx (16-byte rows); elsewhere, or with
+   copies while the other warps compute (Navier-Stokes: the viscous fluxes by plain loads);
+   results are identical either way.  It applies to contexts whose blocks all have an even
+   nx (16-byte rows), for the explicit-scheme directions; elsewhere, or with
    on = 0, every sweep CTA loads its own tile.  on = 1: every direction; on > 1: the
    directions of its bits 0..2 (bit d: direction d).  nuc3d_autotune also chooses, per
    direction, between the two.  nuc3d_get_pipeline: the directions that run pipelined

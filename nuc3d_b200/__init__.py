@@ -380,7 +380,7 @@ class Solver:
         _check(self.lib.nuc3d_set_pipeline(self._ctx, v))
 
     def pipeline(self) -> int:
-        """Directions (bit d) whose sweeps run pipelined (Euler, even nx, switched on);
+        """Directions (bit d) whose sweeps run pipelined (even nx, explicit schemes, switched on);
         0 for none."""
         v = ctypes.c_int()
         _check(self.lib.nuc3d_get_pipeline(self._ctx, ctypes.byref(v)))

@@ -2044,11 +2044,16 @@ inline cudaError_t launch_sweep_s(const Launch &L, int stage, int flags) {
     }
   }
 #endif
-  if (L.d_maps && L.pipe_grid > 0 && !ns && ((L.pipe_dirs >> DIR) & 1)) {
+  if (L.d_maps && L.pipe_grid > 0 && ((L.pipe_dirs >> DIR) & 1)) {
     // persistent sweep fed by tensor-map loads (sweep_pipe.cuh)
     const int grid = ntiles < L.pipe_grid ? ntiles : L.pipe_grid;
-    pipe_sweep_kernel<DIR, SCH, SHP><<<grid, kPipeThreads, PipeSmem<DIR, SCH, SHP>::TOTAL, L.stream>>>(
-        L.d_blocks, L.d_maps, L.tm_dir[DIR], L.P, L.d_state, stage, flags);
+    if (ns)
+      pipe_sweep_kernel<DIR, SCH, SHP, true><<<grid, kPipeThreads, PipeSmem<DIR, SCH, SHP, true>::TOTAL,
+                                               L.stream>>>(L.d_blocks, L.d_maps, L.tm_dir[DIR], L.P,
+                                                           L.d_state, stage, flags);
+    else
+      pipe_sweep_kernel<DIR, SCH, SHP><<<grid, kPipeThreads, PipeSmem<DIR, SCH, SHP>::TOTAL, L.stream>>>(
+          L.d_blocks, L.d_maps, L.tm_dir[DIR], L.P, L.d_state, stage, flags);
     return cudaGetLastError();
   }
   const size_t smem = sweep_smem_bytes<DIR, SCH, SHP>(ns) + rhs_stage_bytes<DIR>(ns);
@@ -2306,9 +2311,14 @@ inline cudaError_t configure_s() {
 #endif
   const size_t euler = sweep_smem_bytes<DIR, SCH, SHP>(false) + rhs_stage_bytes<DIR>(false);
   const size_t ns = sweep_smem_bytes<DIR, SCH, SHP>(true) + rhs_stage_bytes<DIR>(true);
-  const cudaError_t e = cudaFuncSetAttribute(pipe_sweep_kernel<DIR, SCH, SHP>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)PipeSmem<DIR, SCH, SHP>::TOTAL);
+  cudaError_t e = cudaFuncSetAttribute(pipe_sweep_kernel<DIR, SCH, SHP>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)PipeSmem<DIR, SCH, SHP>::TOTAL);
+  if (e != cudaSuccess) return e;
+  static_assert(PipeSmem<DIR, SCH, SHP, true>::TOTAL <= kSmemOptin, "NS pipelined tile fits");
+  e = cudaFuncSetAttribute(pipe_sweep_kernel<DIR, SCH, SHP, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)PipeSmem<DIR, SCH, SHP, true>::TOTAL);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(sweep_kernel<DIR, SCH, false, SHP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(euler > ns ? euler : ns));

@@ -473,7 +473,7 @@ int build_maps(nuc3d_ctx *c) {
   Launch &L = c->L;
   L.d_maps = nullptr;
   L.pipe_grid = 0;
-  bool ok = c->use_pipe && c->P.model == MODEL_EULER;
+  bool ok = c->use_pipe;
   for (const HostBlock &b : c->blocks) ok = ok && b.n[0] % 2 == 0;
   if (!ok) return NUC3D_OK;
   if (!tensor_map_encoder()) return NUC3D_OK;  // no TMA encoder in this driver: plain sweeps

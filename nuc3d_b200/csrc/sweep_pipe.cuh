@@ -61,7 +61,7 @@ template <int DIR, int SCH, int SHP> struct PipeGeo {
 __host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
 
 // Shared-memory carve-up of the pipelined sweep (byte offsets from a 128-byte aligned base).
-template <int DIR, int SCH, int SHP> struct PipeSmem {
+template <int DIR, int SCH, int SHP, bool NSV = false> struct PipeSmem {
   using G = PipeGeo<DIR, SCH, SHP>;
   using M = TileSmem<DIR, SCH, SHP>;
   // one slot: state, Jacobian and direction metric over the halo box, [xi] the other two
@@ -79,7 +79,8 @@ template <int DIR, int SCH, int SHP> struct PipeSmem {
   static constexpr size_t QN = RHS + (DIR != 0 ? align128((size_t)5 * G::OWN * 8) : 0);  // [5][OWN]
   static constexpr size_t F = QN + (DIR == 2 ? align128((size_t)5 * G::OWN * 8) : 0);
   static constexpr size_t H = F + align128((size_t)10 * G::TW * M::SP * 8);
-  static constexpr size_t RED = H + align128((size_t)5 * G::TW * M::SH * 8);  // [kThreads / 32]
+  static constexpr size_t V = H + align128((size_t)5 * G::TW * M::SH * 8);    // NS: [4][TW][SV]
+  static constexpr size_t RED = V + (NSV ? align128((size_t)4 * G::TW * M::SV * 8) : 0);  // [kThreads / 32]
   static constexpr size_t BAR = RED + align128((size_t)(kThreads / 32) * 8);  // 5 mbarriers
   static constexpr size_t TOTAL = BAR + 64;
 };
@@ -210,14 +211,16 @@ __device__ __forceinline__ void pipe_gather(const BlockDev *__restrict__ blocks,
   }
 }
 
-template <int DIR, int SCH, int SHP>
+// NSV: the Navier-Stokes sweep: the consumers also load the direction's viscous fluxes
+// (phase_vis, plain loads) and phase 3 applies the viscous differences as sweep_kernel does.
+template <int DIR, int SCH, int SHP, bool NSV = false>
 __global__ void __launch_bounds__(kPipeThreads, 2)
 pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__restrict__ maps,
                   TileMap tm, SolverParams P, StepState *S, int stage, int flags) {
   using G = PipeGeo<DIR, SCH, SHP>;
   using M = TileSmem<DIR, SCH, SHP>;
-  using L = PipeSmem<DIR, SCH, SHP>;
-  constexpr int R = G::R, TW = G::TW, TL = G::TL, NP = G::NP, SP = M::SP, SH = M::SH;
+  using L = PipeSmem<DIR, SCH, SHP, NSV>;
+  constexpr int R = G::R, TW = G::TW, TL = G::TL, NP = G::NP, SP = M::SP, SH = M::SH, SV = M::SV;
   extern __shared__ __align__(128) unsigned char psm[];
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(psm + L::BAR);
   unsigned long long *full_q = bar, *done = bar + 2, *full_r = bar + 4;
@@ -226,6 +229,7 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
   double *sRed = reinterpret_cast<double *>(psm + L::RED);
   double *rbuf = reinterpret_cast<double *>(psm + L::RHS);
   double *nbuf = reinterpret_cast<double *>(psm + L::QN);
+  double *sV = reinterpret_cast<double *>(psm + L::V);  // NSV only
 
   const bool eig = DIR == 0 && (flags & SW_EIG) != 0;
   const bool rk = (flags & SW_RK) != 0;
@@ -401,6 +405,10 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
     }
     consumer_sync();
 
+    // NS: the direction's viscous fluxes of the tile's line positions into sV (after the
+    // barrier above: phase 3 of the previous tile has read sV)
+    if constexpr (NSV) phase_vis<DIR, SCH, SHP>(blocks, T, P, sV);
+
     // ---- phase 2: the ten reconstructions of each face c0 .. c0+cl ----
     {
       const int nf = T.cl + 1;
@@ -479,12 +487,43 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
         const double *h = sH + (v * TW + w) * SH;
         d[v] = h[c + 1] - h[c];
       }
+      double dv[4] = {0.0, 0.0, 0.0, 0.0};
+      if constexpr (NSV) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const double *row = sV + (v * TW + w) * SV + (kVisHalo - T.c0);
+          auto Vacc = [row](int cc) { return row[cc]; };
+          dv[v] = diff_at(g, T.G.L, T.ts, T.physL, T.physR, P.vis[DIR], Vacc);
+        }
+      }
       if (DIR == 0) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) B.rhs[v * N + idx] = d[v];
-      } else if (DIR == 1 || !rk) {
+        if constexpr (NSV) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v) B.dvis[v * N + idx] = dv[v];
+        }
+      } else if (DIR == 1) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) B.rhs[v * N + idx] = rbuf[v * G::OWN + oi] + d[v];
+        if constexpr (NSV) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v) B.dvis[(4 + v) * N + idx] = dv[v];
+        }
+      } else if (!rk) {
+        double r[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) r[v] = rbuf[v * G::OWN + oi] + d[v];
+        if constexpr (NSV) {
+#pragma unroll
+          for (int v = 1; v < 5; ++v) {
+            r[v] = r[v] - B.dvis[(v - 1) * N + idx];
+            r[v] = r[v] - B.dvis[(4 + v - 1) * N + idx];
+            r[v] = r[v] - dv[v - 1];
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) B.rhs[v * N + idx] = r[v];
       } else {
         double *__restrict__ qo = B.q[(stage + 1) % 3];
         const int h = G::hidx(c + R, w);
@@ -498,11 +537,23 @@ pipe_sweep_kernel(const BlockDev *__restrict__ blocks, const CUtensorMap *__rest
           con2prim(un, Jh[h], P.gamma, P.mach, sn, stn);
           un[4] = sn.q4;
         }
+        double r[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) r[v] = rbuf[v * G::OWN + oi] + d[v];
+        if constexpr (NSV) {
+          // the reference's RHS order: inviscid sum, then minus each direction's viscous
+          // part (sweep_kernel's phase_cells)
+#pragma unroll
+          for (int v = 1; v < 5; ++v) {
+            r[v] = r[v] - B.dvis[(v - 1) * N + idx];
+            r[v] = r[v] - B.dvis[(4 + v - 1) * N + idx];
+            r[v] = r[v] - dv[v - 1];
+          }
+        }
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const double r = rbuf[v * G::OWN + oi] + d[v];
           const double ui = v < 4 ? Qh[v * G::BOX + h] : sQ4[oi];
-          const double x = rk3_update(stage, r, ui, un[v], dt);
+          const double x = rk3_update(stage, r[v], ui, un[v], dt);
           if (!isfinite(x)) st |= ST_NONFINITE;
           qo[v * N + idx] = x;
           if (flags & SW_RES) res_value(B, v, idx, x, un[v], racc);

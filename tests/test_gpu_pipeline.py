@@ -1,14 +1,16 @@
 """The pipelined sweeps (persistent kernels fed by tensor-map loads, sweep_pipe.cuh) give
 exactly what the one-tile-per-CTA sweeps give, which the parity tests pin to the
-reference: right-hand side, dt and steps on every Euler golden case, with every tile
-shape, across block faces (two blocks), with the energy reset, and in both builds."""
+reference: right-hand side, dt and steps on every explicit-scheme golden case, Euler and
+Navier-Stokes (the viscous fluxes loaded by the consumers, the viscous differences in
+phase 3), with every tile shape, across block faces (two blocks), with the energy reset,
+and in both builds."""
 import numpy as np
 import pytest
 
 from tests import golden_cases as G
 
-EULER = [n for n in G.names() if G.load(n).cfg["model"] == "Euler3d"
-         and not any(s in ("crweno5", "hccs", "hccs77") for s in G.load(n).cfg["schemes"])]
+EXPLICIT = [n for n in G.names()
+            if not any(s in ("crweno5", "hccs", "hccs77") for s in G.load(n).cfg["schemes"])]
 
 
 def _run(g, exact, pipe, shape=None, nsteps=None):
@@ -26,7 +28,7 @@ def _run(g, exact, pipe, shape=None, nsteps=None):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", EULER)
+@pytest.mark.parametrize("name", EXPLICIT)
 def test_pipelined_sweeps_bitwise_reference(name):
     g = G.load(name)
     dt, rhs, q, (t, dtl), resets, _, res = _run(g, exact=True, pipe=True)
@@ -43,7 +45,8 @@ def _rel(a, b):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["sphere_euler_weno5z_ausm_outlet", "mixed_euler_lf_outlet_symm",
-                                  "sphere_reset_euler_weno5z_ausm", "mixed_low_order_ausmp"])
+                                  "sphere_reset_euler_weno5z_ausm", "mixed_low_order_ausmp",
+                                  "tgv_ns_weno5js_lf", "bc_ns_weno7js_ausmp", "ns_cd8_weno7js_lf"])
 @pytest.mark.parametrize("shape", [(0, 0, 0), (1, 1, 1), (2, 2, 2), (2, 0, 1)])
 @pytest.mark.parametrize("exact", [True, False])
 def test_pipelined_equals_plain(name, shape, exact):
@@ -93,14 +96,23 @@ def test_pipelined_two_blocks_bitwise():
 
 @pytest.mark.gpu
 def test_pipeline_applies_where_it_can():
-    """Navier-Stokes contexts keep the one-tile-per-CTA sweeps (their viscous tiles are
-    not staged); switching it off and on again works."""
-    g = G.load("tgv_ns_weno5js_lf")
-    s = G.solver(g, exact=True)
-    assert not s.pipeline()
+    """Euler and Navier-Stokes contexts run pipelined; a block with an odd nx (rows not
+    16-byte multiples) keeps the one-tile-per-CTA sweeps; switching it off and on again
+    works, and a mask selects directions."""
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+    assert G.solver(G.load("tgv_ns_weno5js_lf"), exact=True).pipeline() == 7
     e = G.solver(G.load("sphere_euler_weno5z_ausm_outlet"), exact=True)
-    assert e.pipeline()
+    assert e.pipeline() == 7
     e.set_pipeline(False)
-    assert not e.pipeline()
+    assert e.pipeline() == 0
     e.set_pipeline(True)
-    assert e.pipeline()
+    assert e.pipeline() == 7
+    e.set_pipeline(4)
+    assert e.pipeline() == 4
+    q, m = C.spherical_riemann((13, 12, 12))
+    o = nb.Solver(nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="Euler3d", mach=1.0))
+    b = o.add_block(13, 12, 12, *C.outlet_faces())
+    o.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
+    o.finalize()
+    assert o.pipeline() == 0
