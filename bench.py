@@ -571,7 +571,7 @@ def shock_turbulence(args, steps=10, warm=2):
         s.sync()
         ms = ev0.elapsed_time(ev1) / steps
         rho = s.get_q(b)[0] * (1.0 / (h * h * h))  # U/J -> rho on the uniform mesh
-        return ms, rho, tiles
+        return ms, rho, {"tile_shapes": list(tiles), "pipelined_dirs": s.pipeline()}
 
     ms_p, rho_p, tiles_p = run("plain")
     s.set_sensor(SENS.load_weights(), SENS.DEFAULT_THRESHOLD)
@@ -582,7 +582,7 @@ def shock_turbulence(args, steps=10, warm=2):
         s.set_sensor_theta(tmin)
         ms_t, rho_t, tiles_t = run("theta")
         theta.append({"theta_min": tmin, "value": cells / (ms_t * 1e-3) / 1e6, "ms_per_step": ms_t,
-                      "vs_plain": ms_p / ms_t, "tile_shapes": list(tiles_t),
+                      "vs_plain": ms_p / ms_t, **tiles_t,
                       "l1_density_error_vs_plain": float(np.abs(rho_t - rho_p).sum() / np.abs(rho_p).sum()),
                       "shock_x": C.shock_position(rho_t, h)})
         del rho_t
@@ -592,9 +592,9 @@ def shock_turbulence(args, steps=10, warm=2):
     vh = cells / (ms_h * 1e-3) / 1e6
     return {"workload": SHOCK_WORKLOAD, "cells": cells, "steps_compared": warm + steps,
             "plain": {"value": vp, "unit": "Mcell-RK3-steps/s", "ms_per_step": ms_p,
-                      "tile_shapes": list(tiles_p)},
+                      **tiles_p},
             "hybrid": {"value": vh, "unit": "Mcell-RK3-steps/s", "ms_per_step": ms_h,
-                       "tile_shapes": list(tiles_h), "logit_threshold": SENS.DEFAULT_THRESHOLD},
+                       **tiles_h, "logit_threshold": SENS.DEFAULT_THRESHOLD},
             "vs_plain": vh / vp,
             "l1_density_error_vs_plain": float(np.abs(rho_h - rho_p).sum() / np.abs(rho_p).sum()),
             "shock_x": {"initial": 0.5 * math.pi, "plain": C.shock_position(rho_p, h),
@@ -732,7 +732,8 @@ def _bl_compare(shape, steps, warm, thresholds, autotune=True):
         s.sync()
         mass = np.concatenate([s.get_q(r)[0].ravel() for r in range(len(blocks))])
         return {"ms_per_step": ev0.elapsed_time(ev1) / steps, "tile_shapes": tiles,
-                "status_bits": s.status(), "time": s.time_dt()[0]}, mass
+                "pipelined_dirs": s.pipeline(), "status_bits": s.status(),
+                "time": s.time_dt()[0]}, mass
 
     s = solver("weno5z")
     plain, m_p = run(s)
@@ -919,7 +920,7 @@ def turbulence24(args, with_cpu=False):
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": TURB_WORKLOAD, "cells_per_gpu": cells, "blocks": len(boxes),
-                   "tile_shapes": list(tiles), "status_bits": s.status(),
+                   "tile_shapes": list(tiles), "pipelined_dirs": s.pipeline(), "status_bits": s.status(),
                    "l2": "no flush: 40.1M cells x 5 doubles = 1.6 GB per state buffer > 126 MB L2"},
         "clocks": clk.summary(),
         "e2e": {"value": whole_job_rate(1, cells, e2e_steps, e2e_ms), "unit": "Mcell-RK3-steps/s",
