@@ -337,3 +337,43 @@ def test_solve_host_slab_pipeline_equals_device_steps(exact):
         assert s2.time_dt() == ref[1] and s2.residual() == ref[2]
         assert np.array_equal(s2.get_q(b2), ref[0])
         s2.close()
+
+
+@pytest.mark.gpu
+def test_solve_host_slab_pipeline_all_boundary_types():
+    """The slab pipeline's per-slab BC passes (cells k0 <= k < k1 of every physical face:
+    x and y faces by rows, z faces in the first and last slab) with an inlet, a wall, a
+    symmetry face and outlets on a 40 x 24 x 130 block (three slabs, the last two planes
+    long): bitwise the device-resident steps in the reference-order build."""
+    import torch
+    import nuc3d_b200 as nb
+    from nuc3d_b200 import cases as C
+    shape = (40, 24, 130)
+    q0, m = C.spherical_riemann(shape)
+    types = [-1] * 6
+    ids = [0, 1, 2, 3, 1, 1]  # inlet x-, outlet x+, wall y-, symmetry y+, outlets z
+    vals = np.zeros((6, 5))
+    vals[0] = [1.0, 0.3, 0.0, 0.0, 0.7]
+
+    def make():
+        s = nb.Solver(nb.Config(scheme_ivs=("weno5z", "weno5js", "weno5z"), riemann="AUSM",
+                                model="Euler3d", mach=1.0, exact=True, weno5z_compat=True))
+        b = s.add_block(*shape, types, ids, vals)
+        s.set_metrics(b, m["jac"], m["xi_xyz"], m["eta_xyz"], m["zeta_xyz"], m["dxyz"])
+        s.finalize()
+        s.set_q(b, q0)
+        s.set_tiles((2, 0, 0))
+        return s, b
+
+    s1, b1 = make()
+    s1.step(4)
+    ref = s1.get_q(b1), s1.time_dt(), s1.residual(), s1.energy_resets()
+    s1.close()
+    s2, b2 = make()
+    assert s2.host_pipeline() == 3
+    host = torch.empty(q0.size, dtype=torch.float64, pin_memory=True)
+    host.numpy()[:] = q0.reshape(-1)
+    s2.solve_host([host.data_ptr()], 4)
+    assert np.array_equal(host.numpy().reshape(q0.shape), ref[0])
+    assert s2.time_dt() == ref[1] and s2.residual() == ref[2] and s2.energy_resets() == ref[3]
+    s2.close()
