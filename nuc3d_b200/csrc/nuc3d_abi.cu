@@ -837,9 +837,10 @@ constexpr size_t kHostChunk = (size_t)NUC3D_HOST_CHUNK_MB << 20;
 
 // nuc3d_solve_host for one Euler block with explicit schemes, as a copy/compute pipeline
 // over z-slabs (the zeta sweep's z-chunks): the upload of slab s is followed at once by
-// stage 0's BC, xi and eta work on that slab (their lines stay inside a z-plane), and the
-// download of slab s follows stage 2's zeta sweep over that slab, while the copy engines
-// move the other slabs.  The kernels and tiles are one_step's, so the results are too.
+// stage 0's BC, xi and eta work on that slab (their lines stay inside a z-plane), and
+// stage 2 runs slab by slab (BC, xi, eta, then zeta over the slab: it reads the slab's own
+// RHS and the stage state stage 1 completed), each slab's download following its zeta
+// sweep, while the copy engines move the other slabs.  The kernels and tiles are one_step's, so the results are too.
 static bool slab_pipeline_ok(const nuc3d_ctx *c) {
   if (!c->host_pipeline || c->blocks.size() != 1 || c->P.model != MODEL_EULER || c->P.sensor)
     return false;
@@ -914,10 +915,12 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
     CUDA_TRY(run([&] { return nuc3d::fast::run_stage0_zeta(L); }, [&] { return nuc3d::exact::run_stage0_zeta(L); }));
     CUDA_TRY(run([&] { return nuc3d::fast::run_stage(L, 1, true, false); },
                  [&] { return nuc3d::exact::run_stage(L, 1, true, false); }));
-    CUDA_TRY(run([&] { return nuc3d::fast::run_stage2_head(L); }, [&] { return nuc3d::exact::run_stage2_head(L); }));
     for (int s = 0; s < ns; ++s) {
-      CUDA_TRY(run([&] { return nuc3d::fast::run_stage2_zeta(L, s * zper, (s + 1) * zper); },
-                   [&] { return nuc3d::exact::run_stage2_zeta(L, s * zper, (s + 1) * zper); }));
+      const int k0 = s * TLz, k1 = std::min(nz, k0 + TLz);
+      CUDA_TRY(run([&] { return nuc3d::fast::run_stage2_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper,
+                                                             k1 * yper, s * zper, (s + 1) * zper); },
+                   [&] { return nuc3d::exact::run_stage2_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper,
+                                                              k1 * yper, s * zper, (s + 1) * zper); }));
       CUDA_TRY(cudaEventRecord(c->ev_zeta[s], c->stream));
     }
     if (L.d_res_last)
