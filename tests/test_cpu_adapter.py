@@ -1,4 +1,4 @@
-"""The C++ adapter INTEGRATION.md shows a NUC3d maintainer (GpuBlockData, GpuRK3) compiles
+"""The C++ adapter the integration guide shows a NUC3d maintainer (GpuBlockData, GpuRK3) compiles
 against the reference's own headers and links against the reference's objects and
 libnuc3d_b200.so: the drop-in classes override the reference's virtual interfaces
 (EulerData3D::solve, integration::integrationAll) with the signatures they have there.
@@ -40,7 +40,7 @@ def _adapter_source() -> str:
     text = (ROOT / "INTEGRATION.md").read_text()
     blocks = re.findall(r"```cpp\n(.*?)```", text, re.S)
     src = [b for b in blocks if "class GpuRK3" in b]
-    assert src, "INTEGRATION.md has no GpuRK3 adapter block"
+    assert src, "the integration guide has no GpuRK3 adapter block"
     return src[0]
 
 

@@ -9,7 +9,7 @@ in the interior loop of weno5z only, and the faces next to a rank boundary take 
 boundary routines' textbook stencil (src/weno5z.cpp:275-282).  So the GPU runs the same
 split, one block per rank in one context; the reference-order build must reproduce every
 block's state, every step's dt and the count of reset cells bit for bit, and the throughput
-build must stay within 1e-10 relative max-norm of it, the north star's bar.
+build must stay within 1e-10 relative max-norm of it.
 """
 import os
 
