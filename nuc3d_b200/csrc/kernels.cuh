@@ -81,7 +81,7 @@ __host__ __device__ inline int sweep_tiles(int dir, const int n[3], int shape) {
 }
 
 template <int DIR, int SCH, int SHP = 0>
-__host__ __device__ inline size_t sweep_smem_bytes(bool ns) {
+__host__ __device__ constexpr size_t sweep_smem_bytes(bool ns) {
   constexpr int R = Halo<SCH>::R, TW = Tile<SHP>::TW, TL = Tile<SHP>::TL;
   size_t n = (size_t)10 * TW * pad_row(TL + 2 * R) + (size_t)5 * TW * pad_row(TL + 1);
   if (ns) n += (size_t)4 * TW * pad_row(TL + 2 * kVisHalo);
@@ -110,7 +110,7 @@ __host__ __device__ constexpr bool rhs_prefetch(bool ns) {
          (!ns || NUC3D_RHS_PREFETCH_NS);
 }
 template <int DIR>
-__host__ __device__ inline size_t rhs_stage_bytes(bool ns) {
+__host__ __device__ constexpr size_t rhs_stage_bytes(bool ns) {
   return rhs_prefetch<DIR>(ns) ? (size_t)5 * 256 * sizeof(double) : 0;
 }
 
@@ -1337,7 +1337,7 @@ __device__ __forceinline__ TileCtx decode_line(const BlockDev *__restrict__ bloc
 }
 
 template <int DIR, int SCH>
-__host__ __device__ inline size_t compact_line_smem_bytes(bool ns) {
+__host__ __device__ constexpr size_t compact_line_smem_bytes(bool ns) {
   using M = TileSmem<DIR, SCH, line_shape(DIR)>;
   size_t n = (size_t)10 * M::TW * M::SP + (size_t)10 * M::TW * M::SH;
   if (ns) n += (size_t)4 * M::TW * M::SV;
@@ -2024,7 +2024,7 @@ metrics_kernel(const double *__restrict__ x, const double *__restrict__ y,
 // ---------------------------------------------------------------------------------
 // Shared memory of the hybrid sweep: the plain sweep's plus rho and p per position.
 template <int DIR, int SCH, int SHP = 0>
-__host__ __device__ inline size_t hybrid_smem_bytes(bool ns) {
+__host__ __device__ constexpr size_t hybrid_smem_bytes(bool ns) {
   using M = TileSmem<DIR, SCH, SHP>;
   return sweep_smem_bytes<DIR, SCH, SHP>(ns) + (size_t)2 * M::TW * M::SP * sizeof(double) + kHybSmem +
          (NUC3D_HYB_PREFETCH ? rhs_stage_bytes<DIR>(ns) : 0);
@@ -2073,12 +2073,12 @@ inline cudaError_t launch_sweep_t(const Launch &L, int stage, int flags) {
 }
 
 template <int DIR, int SCH>
-__host__ __device__ inline size_t compact_rows_smem_bytes() {
+__host__ __device__ constexpr size_t compact_rows_smem_bytes() {
   using M = TileSmem<DIR, SCH>;
   return (size_t)10 * M::TW * M::SP * sizeof(double);
 }
 template <int DIR, int SCH>
-__host__ __device__ inline size_t compact_finish_smem_bytes(bool ns) {
+__host__ __device__ constexpr size_t compact_finish_smem_bytes(bool ns) {
   using M = TileSmem<DIR, SCH>;
   size_t n = (size_t)5 * M::TW * M::SH;
   if (ns) n += (size_t)4 * M::TW * M::SV;
@@ -2312,8 +2312,12 @@ inline cudaError_t configure_s() {
     if (e != cudaSuccess) return e;
   }
 #endif
-  const size_t euler = sweep_smem_bytes<DIR, SCH, SHP>(false) + rhs_stage_bytes<DIR>(false);
-  const size_t ns = sweep_smem_bytes<DIR, SCH, SHP>(true) + rhs_stage_bytes<DIR>(true);
+  constexpr size_t euler = sweep_smem_bytes<DIR, SCH, SHP>(false) + rhs_stage_bytes<DIR>(false);
+  constexpr size_t ns = sweep_smem_bytes<DIR, SCH, SHP>(true) + rhs_stage_bytes<DIR>(true);
+  // every dynamic shared-memory request below fits what a CTA may opt in to
+  static_assert(euler <= kSmemOptin && ns <= kSmemOptin, "sweep tile fits");
+  static_assert(PipeSmem<DIR, SCH, SHP>::TOTAL <= kSmemOptin, "pipelined tile fits");
+  static_assert(hybrid_smem_bytes<DIR, SCH, SHP>(true) <= kSmemOptin, "hybrid tile fits");
   cudaError_t e = cudaFuncSetAttribute(pipe_sweep_kernel<DIR, SCH, SHP>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)PipeSmem<DIR, SCH, SHP>::TOTAL);
@@ -2348,6 +2352,9 @@ inline cudaError_t configure_compact_t() {
     if (e != cudaSuccess) return e;
   }
 #if NUC3D_FAST
+  static_assert(compact_line_smem_bytes<DIR, SCH>(false) <= kSmemOptin, "Euler line tile fits");
+  static_assert(compact_rows_smem_bytes<DIR, SCH>() <= kSmemOptin &&
+                compact_finish_smem_bytes<DIR, SCH>(true) <= kSmemOptin, "compact tiles fit");
   // (a Navier-Stokes tile of kLineLanes lines may not fit: compact_line_smem tells the host)
   e = cudaFuncSetAttribute(compact_line_kernel<DIR, SCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)std::min<size_t>(compact_line_smem_bytes<DIR, SCH>(true), kSmemOptin));
