@@ -255,9 +255,9 @@ cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
 // run_bc(): the physical faces' ghost fluxes at stage `stage` for the cells k0 <= k < k1.
 // Pieces of one Euler step over z-slabs (nuc3d_solve_host's copy/compute pipeline).
 cudaError_t run_stage0_slab(const Launch &L, int k0, int k1, int tx0, int tx1, int ty0, int ty1);
-cudaError_t run_stage0_zeta(const Launch &L);
-cudaError_t run_stage2_slab(const Launch &L, int k0, int k1, int tx0, int tx1, int ty0, int ty1, int tz0,
-                            int tz1);
+cudaError_t run_stage0_zeta(const Launch &L, int tz0, int tz1);
+cudaError_t run_stage_slab(const Launch &L, int stage, int k0, int k1, int tx0, int tx1, int ty0, int ty1,
+                           int tz0, int tz1);
 cudaError_t run_bc(const Launch &L, int stage, int k0, int k1);
 cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
@@ -281,9 +281,9 @@ cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig);
 // run_bc(): the physical faces' ghost fluxes at stage `stage` for the cells k0 <= k < k1.
 // Pieces of one Euler step over z-slabs (nuc3d_solve_host's copy/compute pipeline).
 cudaError_t run_stage0_slab(const Launch &L, int k0, int k1, int tx0, int tx1, int ty0, int ty1);
-cudaError_t run_stage0_zeta(const Launch &L);
-cudaError_t run_stage2_slab(const Launch &L, int k0, int k1, int tx0, int tx1, int ty0, int ty1, int tz0,
-                            int tz1);
+cudaError_t run_stage0_zeta(const Launch &L, int tz0, int tz1);
+cudaError_t run_stage_slab(const Launch &L, int stage, int k0, int k1, int tx0, int tx1, int ty0, int ty1,
+                           int tz0, int tz1);
 cudaError_t run_bc(const Launch &L, int stage, int k0, int k1);
 cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,

@@ -2188,11 +2188,13 @@ cudaError_t run_stage(const Launch &L, int stage, bool rk, bool eig) {
   return launch_stage(L, stage, rk, eig);
 }
 
-// Pieces of one Euler step for nuc3d_solve_host's slab pipeline; together, in this order,
-// they launch exactly the kernels of one_step over the same tiles (the same results):
+// Pieces of one Euler step for nuc3d_solve_host's slab pipeline; together they launch
+// exactly the kernels of one_step over the same tiles (the same results):
 //   stage-0 slab s (BC of k0 <= k < k1; xi and eta over the slab's tiles, xi reducing the
-//   eigenvalue maximum) for every slab, then zeta of stage 0, stage 1, stage-2 slab s
-//   (BC, xi, eta and zeta over the slab's tiles) for every slab, and the residual.
+//   eigenvalue maximum) for every slab; then, per slab, the zeta sweep of stage 0 and
+//   stages 1 and 2 (BC, xi, eta, zeta over the slab's tiles) in any order that runs a
+//   slab's stage-s zeta sweep after the stage-(s-1) zeta sweeps of the slab and of the
+//   slabs whose cells its stencils reach; then the residual.
 static TileMap tile_part(TileMap tm, int t0, int t1) {
   tm.base = t0;
   tm.end = t1;
@@ -2207,20 +2209,27 @@ cudaError_t run_stage0_slab(const Launch &L, int k0, int k1, int tx0, int tx1, i
   P.tm_dir[1] = tile_part(L.tm_dir[1], ty0, ty1);
   return launch_sweep<1>(P, 0, 0);
 }
-cudaError_t run_stage0_zeta(const Launch &L) { return launch_sweep<2>(L, 0, SW_RK); }
-// Stage 2 of one z-slab: BC, xi and eta over the slab's tiles, then zeta over its z-chunk
-// (zeta reads the slab's own RHS and the whole stage state, complete after stage 1).
-cudaError_t run_stage2_slab(const Launch &L, int k0, int k1, int tx0, int tx1, int ty0, int ty1, int tz0,
-                            int tz1) {
-  cudaError_t e = run_bc(L, 2, k0, k1);
+// Stage 0's zeta sweep over the zeta tiles tz0 <= t < tz1 (every cell's eigenvalue must be
+// in the maximum: the stage fixes dt from it).
+cudaError_t run_stage0_zeta(const Launch &L, int tz0, int tz1) {
+  Launch P = L;
+  P.tm_dir[2] = tile_part(L.tm_dir[2], tz0, tz1);
+  return launch_sweep<2>(P, 0, SW_RK);
+}
+// Stage 1 or 2 of one z-slab: BC, xi and eta over the slab's tiles, then zeta over its
+// z-chunks (zeta reads the slab's own RHS and the stage state of its cells and of the
+// neighbouring slabs' planes its stencils reach).
+cudaError_t run_stage_slab(const Launch &L, int stage, int k0, int k1, int tx0, int tx1, int ty0, int ty1,
+                           int tz0, int tz1) {
+  cudaError_t e = run_bc(L, stage, k0, k1);
   if (e != cudaSuccess) return e;
   Launch P = L;
   P.tm_dir[0] = tile_part(L.tm_dir[0], tx0, tx1);
   P.tm_dir[1] = tile_part(L.tm_dir[1], ty0, ty1);
   P.tm_dir[2] = tile_part(L.tm_dir[2], tz0, tz1);
-  if ((e = launch_sweep<0>(P, 2, 0)) != cudaSuccess) return e;
-  if ((e = launch_sweep<1>(P, 2, 0)) != cudaSuccess) return e;
-  return launch_sweep<2>(P, 2, SW_RK | (L.d_res_last ? SW_RES : 0));
+  if ((e = launch_sweep<0>(P, stage, 0)) != cudaSuccess) return e;
+  if ((e = launch_sweep<1>(P, stage, 0)) != cudaSuccess) return e;
+  return launch_sweep<2>(P, stage, SW_RK | (stage == 2 && L.d_res_last ? SW_RES : 0));
 }
 
 cudaError_t run_bc(const Launch &L, int stage, int k0, int k1) {

@@ -841,13 +841,19 @@ constexpr size_t kHostChunk = (size_t)NUC3D_HOST_CHUNK_MB << 20;
 // stage 2 runs slab by slab (BC, xi, eta, then zeta over the slab: it reads the slab's own
 // RHS and the stage state stage 1 completed), each slab's download following its zeta
 // sweep, while the copy engines move the other slabs.  The kernels and tiles are one_step's, so the results are too.
+// nuc3d_solve_host's slab pipeline runs the zeta sweep in 8 x 32 tiles whatever the
+// context's zeta shape: slabs of 32 planes instead of 64 halve the stretch between a step's
+// last upload and its first download, when the copy engines idle (the 256^3 Euler step:
+// 17.8 against 19.6 ms; the shape changes which CTA computes a cell, not the results).
+constexpr int kHostZetaShape = 1;
+
 static bool slab_pipeline_ok(const nuc3d_ctx *c) {
   if (!c->host_pipeline || c->blocks.size() != 1 || c->P.model != MODEL_EULER || c->P.sensor)
     return false;
   for (int d = 0; d < 3; ++d)
     if (c->P.scheme[d] == SCH_CRWENO5 || c->P.scheme[d] == SCH_HCCS || c->P.scheme[d] == SCH_HCCS77)
       return false;
-  return c->blocks[0].n[2] >= 2 * tile_l(c->L.shape[2]);
+  return c->blocks[0].n[2] >= 2 * tile_l(kHostZetaShape);
 }
 
 #ifndef NUC3D_HOST_PIECES
@@ -855,14 +861,36 @@ static bool slab_pipeline_ok(const nuc3d_ctx *c) {
 #endif
 constexpr int kHostPieces = NUC3D_HOST_PIECES;
 
+// The slabs of nuc3d_solve_host's pipeline are whole zeta chunks; a last chunk thinner than
+// kSlabMin planes joins the slab before it, so that every slab holds more planes than a
+// zeta stencil reaches (4) and a slab's stencils touch only its two neighbours' cells (and
+// the z faces' ghost fluxes only in the end slabs).
+constexpr int kSlabMin = 8;
+static int host_slab_count(const nuc3d_ctx *c) {
+  const int nz = c->blocks[0].n[2], TLz = tile_l(kHostZetaShape), nchunk = (nz + TLz - 1) / TLz;
+  return (nchunk > 1 && nz - (nchunk - 1) * TLz < kSlabMin) ? nchunk - 1 : nchunk;
+}
+
+static int apply_shapes(nuc3d_ctx *c, const int shape[3]);
+
 static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
   const HostBlock &b = c->blocks[0];
   const int nx = b.n[0], ny = b.n[1], nz = b.n[2];
   const int *sh = c->L.shape;
-  const int TLz = tile_l(sh[2]), ns = (nz + TLz - 1) / TLz;
+  const int TLz = tile_l(sh[2]), nchunk = (nz + TLz - 1) / TLz, ns = host_slab_count(c);
   const int zper = ((nx + tile_w(sh[2]) - 1) / tile_w(sh[2])) * ny;                      // zeta tiles per chunk
   const int xper = ((nx + tile_l(sh[0]) - 1) / tile_l(sh[0])) * ((ny + tile_w(sh[0]) - 1) / tile_w(sh[0]));
   const int yper = ((ny + tile_l(sh[1]) - 1) / tile_l(sh[1])) * ((nx + tile_w(sh[1]) - 1) / tile_w(sh[1]));
+  auto slab_chunks = [&](int s, int &c0, int &c1) {
+    c0 = s;
+    c1 = s == ns - 1 ? nchunk : s + 1;
+  };
+  // with both z faces physical, a slab's stage-s zeta sweep needs the stage-(s-1) state of
+  // its own and its neighbours' cells only, so the stages run as a wavefront over the
+  // slabs and the first slab's download starts after 3 slabs of stage 0's zeta sweep, 2 of
+  // stage 1 and 1 of stage 2; a z face joined to the block itself makes every slab depend
+  // on every other, and then stages 0 (zeta) and 1 run over the whole block first
+  const bool wave = b.bc_type[4] < 0 && b.bc_type[5] < 0;
   // copies move pieces of kHostPieces z-ranges per slab: the upload of a piece waits only
   // for the download of the same piece, so the last slab's round trip is short
   const int np = ns * kHostPieces;
@@ -873,9 +901,17 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
       v->push_back(ev);
     }
   const size_t plane = (size_t)nx * ny;
+  auto slab_range = [&](int s, int &k0, int &k1) {
+    int c0, c1;
+    slab_chunks(s, c0, c1);
+    k0 = c0 * TLz;
+    k1 = std::min(nz, c1 * TLz);
+  };
   auto piece_range = [&](int p, int &k0, int &k1) {
-    const int s = p / kHostPieces, q = p % kHostPieces;
-    const int s0 = s * TLz, s1 = std::min(nz, s0 + TLz), len = s1 - s0;
+    const int q = p % kHostPieces;
+    int s0, s1;
+    slab_range(p / kHostPieces, s0, s1);
+    const int len = s1 - s0;
     k0 = s0 + len * q / kHostPieces;
     k1 = s0 + len * (q + 1) / kHostPieces;
   };
@@ -895,6 +931,26 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
   };
   const Launch &L = c->L;
   auto run = [&](auto fast_fn, auto exact_fn) { return c->exact ? exact_fn() : fast_fn(); };
+  auto zeta0 = [&](int s) {
+    int c0, c1;
+    slab_chunks(s, c0, c1);
+    return run([&] { return nuc3d::fast::run_stage0_zeta(L, c0 * zper, c1 * zper); },
+               [&] { return nuc3d::exact::run_stage0_zeta(L, c0 * zper, c1 * zper); });
+  };
+  auto stage_slab = [&](int stage, int s) {
+    int k0, k1, c0, c1;
+    slab_range(s, k0, k1);
+    slab_chunks(s, c0, c1);
+    return run([&] { return nuc3d::fast::run_stage_slab(L, stage, k0, k1, k0 * xper, k1 * xper, k0 * yper,
+                                                        k1 * yper, c0 * zper, c1 * zper); },
+               [&] { return nuc3d::exact::run_stage_slab(L, stage, k0, k1, k0 * xper, k1 * xper, k0 * yper,
+                                                         k1 * yper, c0 * zper, c1 * zper); });
+  };
+  auto stage2_slab = [&](int s) -> cudaError_t {
+    cudaError_t e = stage_slab(2, s);
+    if (e != cudaSuccess) return e;
+    return cudaEventRecord(c->ev_zeta[s], c->stream);
+  };
   CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
   CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_start, 0));
   for (int step = 0; step < nsteps; ++step) {
@@ -906,22 +962,25 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
     }
     CUDA_TRY(cudaMemsetAsync(&c->d_state->max_eig_bits, 0, sizeof(unsigned long long), c->stream));
     for (int s = 0; s < ns; ++s) {
-      const int k0 = s * TLz, k1 = std::min(nz, k0 + TLz);
+      int k0, k1;
+      slab_range(s, k0, k1);
       // the slab's last piece (the copy stream runs the pieces in order)
       CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_up[(s + 1) * kHostPieces - 1], 0));
       CUDA_TRY(run([&] { return nuc3d::fast::run_stage0_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper, k1 * yper); },
                    [&] { return nuc3d::exact::run_stage0_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper, k1 * yper); }));
     }
-    CUDA_TRY(run([&] { return nuc3d::fast::run_stage0_zeta(L); }, [&] { return nuc3d::exact::run_stage0_zeta(L); }));
-    CUDA_TRY(run([&] { return nuc3d::fast::run_stage(L, 1, true, false); },
-                 [&] { return nuc3d::exact::run_stage(L, 1, true, false); }));
-    for (int s = 0; s < ns; ++s) {
-      const int k0 = s * TLz, k1 = std::min(nz, k0 + TLz);
-      CUDA_TRY(run([&] { return nuc3d::fast::run_stage2_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper,
-                                                             k1 * yper, s * zper, (s + 1) * zper); },
-                   [&] { return nuc3d::exact::run_stage2_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper,
-                                                              k1 * yper, s * zper, (s + 1) * zper); }));
-      CUDA_TRY(cudaEventRecord(c->ev_zeta[s], c->stream));
+    if (wave) {
+      for (int w = 0; w < ns + 2; ++w) {
+        if (w < ns) CUDA_TRY(zeta0(w));
+        if (w >= 1 && w - 1 < ns) CUDA_TRY(stage_slab(1, w - 1));
+        if (w >= 2) CUDA_TRY(stage2_slab(w - 2));
+      }
+    } else {
+      CUDA_TRY(run([&] { return nuc3d::fast::run_stage0_zeta(L, 0, nchunk * zper); },
+                   [&] { return nuc3d::exact::run_stage0_zeta(L, 0, nchunk * zper); }));
+      CUDA_TRY(run([&] { return nuc3d::fast::run_stage(L, 1, true, false); },
+                   [&] { return nuc3d::exact::run_stage(L, 1, true, false); }));
+      for (int s = 0; s < ns; ++s) CUDA_TRY(stage2_slab(s));
     }
     if (L.d_res_last)
       CUDA_TRY(run([&] { return nuc3d::fast::run_residual(L, false); },
@@ -947,7 +1006,7 @@ int nuc3d_set_host_pipeline(nuc3d_ctx *c, int on) {
 int nuc3d_get_host_pipeline(nuc3d_ctx *c, int *on) {
   if (!c || !on) return fail(NUC3D_EINVAL, "null argument");
   if (!c->finalized) return fail(NUC3D_ESTATE, "call nuc3d_finalize first");
-  *on = slab_pipeline_ok(c) ? (c->blocks[0].n[2] + tile_l(c->L.shape[2]) - 1) / tile_l(c->L.shape[2]) : 0;
+  *on = slab_pipeline_ok(c) ? host_slab_count(c) : 0;
   return NUC3D_OK;
 }
 
@@ -964,7 +1023,18 @@ int nuc3d_solve_host(nuc3d_ctx *c, double *const *q_host, int nsteps) {
     for (cudaEvent_t *ev : {&c->ev_start, &c->ev_h2d, &c->ev_step, &c->ev_end})
       CUDA_TRY(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
   }
-  if (slab_pipeline_ok(c)) return solve_host_slabs(c, q_host[0], nsteps);
+  if (slab_pipeline_ok(c)) {
+    const int keep[3] = {c->L.shape[0], c->L.shape[1], c->L.shape[2]};
+    const int host[3] = {keep[0], keep[1], kHostZetaShape};
+    if (keep[2] != kHostZetaShape)
+      if (int r = apply_shapes(c, host)) return r;
+    int r = solve_host_slabs(c, q_host[0], nsteps);
+    if (keep[2] != kHostZetaShape) {
+      const int r2 = apply_shapes(c, keep);
+      if (r == NUC3D_OK) r = r2;
+    }
+    return r;
+  }
   struct Chunk { int b; size_t off, bytes; };
   std::vector<Chunk> chunks;
   for (size_t b = 0; b < c->blocks.size(); ++b) {
