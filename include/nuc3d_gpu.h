@@ -166,7 +166,7 @@ int nuc3d_step(nuc3d_ctx *ctx, int nsteps);
    A context of one Euler block with explicit schemes and at least 64 z-planes runs the
    steps as a pipeline over z-slabs of 32 planes instead (the zeta sweep in 8 x 32 tiles
    for the call, whatever the context's zeta shape, which is restored): each slab's
-   upload is followed at once by stage 0's work on it (the xi and eta lines lie in a
+   upload is followed at once by stage 0's work on it, piece by piece (the xi and eta lines lie in a
    z-plane); with both z faces physical the three stages then advance slab by slab as a
    wavefront (a slab's zeta sweep needs the previous stage's state of its neighbours
    only), and each slab's download follows stage 2's zeta sweep over it, so the copy

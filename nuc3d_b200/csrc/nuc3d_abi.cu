@@ -961,11 +961,13 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
       CUDA_TRY(cudaEventRecord(c->ev_up[p], c->h2d));
     }
     CUDA_TRY(cudaMemsetAsync(&c->d_state->max_eig_bits, 0, sizeof(unsigned long long), c->stream));
-    for (int s = 0; s < ns; ++s) {
+    // stage 0's xi/eta lines lie in z-planes: each piece's share runs as soon as it is in,
+    // so only the last piece's remains between the step's last upload and its dt
+    for (int p = 0; p < np; ++p) {
       int k0, k1;
-      slab_range(s, k0, k1);
-      // the slab's last piece (the copy stream runs the pieces in order)
-      CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_up[(s + 1) * kHostPieces - 1], 0));
+      piece_range(p, k0, k1);
+      if (k1 <= k0) continue;
+      CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_up[p], 0));
       CUDA_TRY(run([&] { return nuc3d::fast::run_stage0_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper, k1 * yper); },
                    [&] { return nuc3d::exact::run_stage0_slab(L, k0, k1, k0 * xper, k1 * xper, k0 * yper, k1 * yper); }));
     }
