@@ -165,16 +165,17 @@ int nuc3d_step(nuc3d_ctx *ctx, int nsteps);
    when q_host holds the last step's state, with nuc3d_sync's status check.
    A context of one Euler block with explicit schemes and at least 64 z-planes runs the
    steps as a pipeline over z-slabs of 32 planes instead (the zeta sweep in 8 x 32 tiles
-   for the call, whatever the context's zeta shape, which is restored): each slab's
-   upload is followed at once by stage 0's work on it, piece by piece (the xi and eta lines lie in a
-   z-plane); with both z faces physical the three stages then advance slab by slab as a
-   wavefront (a slab's zeta sweep needs the previous stage's state of its neighbours
-   only), and each slab's download follows stage 2's zeta sweep over it, so the copy
-   engines move the other slabs while the GPU computes; the kernels are those of
-   nuc3d_step and the state is bitwise the same (in the throughput build the residual's
-   partial sums follow the zeta tiles, so its last bits can differ from nuc3d_step's with
-   another zeta shape).  A last z-chunk thinner than 8 planes joins the slab before it.  nuc3d_set_host_pipeline(ctx, 0) turns
-   that off; nuc3d_get_host_pipeline gives the slab count in use (0: the chunked copies). */
+   for the call, whatever the context's zeta shape, which is restored): stage 0's work
+   on each uploaded piece of a slab follows its upload at once (the xi and eta lines lie
+   in a z-plane); with both z faces physical the three stages then advance slab by slab
+   as a wavefront (a slab's zeta sweep needs the previous stage's state of its
+   neighbours only), and each slab's download follows stage 2's zeta sweep over it, so
+   the copy engines move the other slabs while the GPU computes; the kernels are those
+   of nuc3d_step and the state is bitwise the same (in the throughput build the
+   residual's partial sums follow the zeta tiles, so its last bits can differ from
+   nuc3d_step's with another zeta shape).  A last z-chunk thinner than 8 planes joins
+   the slab before it.  nuc3d_set_host_pipeline(ctx, 0) turns that off;
+   nuc3d_get_host_pipeline gives the slab count in use (0: the chunked copies). */
 int nuc3d_solve_host(nuc3d_ctx *ctx, double *const *q_host, int nsteps);
 int nuc3d_set_host_pipeline(nuc3d_ctx *ctx, int on);
 int nuc3d_get_host_pipeline(nuc3d_ctx *ctx, int *slabs);
