@@ -262,10 +262,22 @@ __device__ __forceinline__ float rel_jump_f(float a, float b) {
 // all seven values are zero (a gap inside a uniform region).
 __device__ __forceinline__ bool sensor_gap(const double *const rowF[5], const double *rr,
                                            const double *pp, int p, float *out, int gs) {
+  // A difference at the round-off level of the split fluxes counts as none: metrics
+  // computed from a mesh (block::getJacobians) carry relative noise near 1e-14 even on a
+  // uniform grid, so a uniform region's fluxes differ in their last bits, and a component
+  // whose exact value is zero (a transverse metric term) is noise alone.  The scale is the
+  // pair's largest flux component: below 2^-32 of it a difference moves the features by
+  // far less than BF16 resolves, and counting it as zero keeps such regions on the
+  // zero-input decision (and its shortcuts).
+  double scale = 0.0;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) scale = fmax(scale, fmax(fabs(rowF[v][p]), fabs(rowF[v][p + 1])));
+  const double tiny = 0x1p-32 * scale;
   bool zero = true;
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
-    const float d = (float)(rowF[v][p + 1] - rowF[v][p]);
+    const double dd = rowF[v][p + 1] - rowF[v][p];
+    const float d = fabs(dd) <= tiny ? 0.0f : (float)dd;
     out[v * gs] = d;
     zero = zero && d == 0.0f;
   }
