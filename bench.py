@@ -494,7 +494,9 @@ def ours(args):
                 "serial_copies_value": e2e_serial_value},
         "gpu_launches": launches,
         "roofline": {
-            "bound": "fp64", "kernel": f"sweep_kernel<{dom}> ({'xi eta zeta'.split()[dom]})",
+            "bound": "fp64",
+            "kernel": (f"{'pipe_sweep_kernel' if (pipelined >> dom) & 1 else 'sweep_kernel'}<{dom}> "
+                       f"({'xi eta zeta'.split()[dom]}, right-hand side)"),
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured live: libnuc3d_probe DFMA microbenchmark",
             "flops_per_cell": sweep_flops_per_cell(dom), "ms_per_launch": per[dom],
