@@ -930,7 +930,9 @@ def turbulence24(args, with_cpu=False):
                 "steps": e2e_steps, "api": "nuc3d_solve_host (24 host arrays in place, every step)"},
         "gpu_launches": s.kernels_per_step() * args.steps,
         "sweep_ms_per_launch": per,
-        "roofline": {"bound": "fp64", "kernel": f"sweep_kernel<{dom}> ({'xi eta zeta'.split()[dom]}, NS)",
+        "roofline": {"bound": "fp64",
+                     "kernel": (f"{'pipe_sweep_kernel' if (s.pipeline() >> dom) & 1 else 'sweep_kernel'}"
+                                f"<{dom}> ({'xi eta zeta'.split()[dom]}, NS)"),
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": "measured live: libnuc3d_probe DFMA microbenchmark",
                      "flops_per_cell": sweep_flops_per_cell(dom, ns=True),
