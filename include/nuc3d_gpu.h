@@ -174,7 +174,9 @@ int nuc3d_step(nuc3d_ctx *ctx, int nsteps);
    of nuc3d_step and the state is bitwise the same (in the throughput build the
    residual's partial sums follow the zeta tiles, so its last bits can differ from
    nuc3d_step's with another zeta shape).  A last z-chunk thinner than 8 planes joins
-   the slab before it.  nuc3d_set_host_pipeline(ctx, 0) turns that off;
+   the slab before it.  A context of several blocks (explicit schemes, no learned sensor)
+   runs stage 2 block by block instead, each block's download following its own zeta
+   sweep (bitwise the same).  nuc3d_set_host_pipeline(ctx, 0) turns both off;
    nuc3d_get_host_pipeline gives the slab count in use (0: the chunked copies). */
 int nuc3d_solve_host(nuc3d_ctx *ctx, double *const *q_host, int nsteps);
 int nuc3d_set_host_pipeline(nuc3d_ctx *ctx, int on);

@@ -259,6 +259,8 @@ cudaError_t run_stage0_zeta(const Launch &L, int tz0, int tz1);
 cudaError_t run_stage_slab(const Launch &L, int stage, int k0, int k1, int tx0, int tx1, int ty0, int ty1,
                            int tz0, int tz1);
 cudaError_t run_bc(const Launch &L, int stage, int k0, int k1);
+cudaError_t run_stage_pre(const Launch &L, int stage);
+cudaError_t run_stage_sweeps(const Launch &L, int stage, int b0, int b1);
 cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
                             long long *where, unsigned long long *count, unsigned long long cap);
@@ -285,6 +287,8 @@ cudaError_t run_stage0_zeta(const Launch &L, int tz0, int tz1);
 cudaError_t run_stage_slab(const Launch &L, int stage, int k0, int k1, int tx0, int tx1, int ty0, int ty1,
                            int tz0, int tz1);
 cudaError_t run_bc(const Launch &L, int stage, int k0, int k1);
+cudaError_t run_stage_pre(const Launch &L, int stage);
+cudaError_t run_stage_sweeps(const Launch &L, int stage, int b0, int b1);
 cudaError_t run_sensor_zero(SensorDev *S, cudaStream_t st);
 cudaError_t run_sensor_data(const Launch &L, int dir, float *feat, unsigned char *label,
                             long long *where, unsigned long long *count, unsigned long long cap);

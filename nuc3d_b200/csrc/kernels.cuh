@@ -2232,6 +2232,32 @@ cudaError_t run_stage_slab(const Launch &L, int stage, int k0, int k1, int tx0, 
   return launch_sweep<2>(P, stage, SW_RK | (stage == 2 && L.d_res_last ? SW_RES : 0));
 }
 
+// Stage 1 or 2 split by blocks, for nuc3d_solve_host's multi-block pipeline: run_stage_pre
+// (the ghost fluxes of every physical face; Navier-Stokes: primitives and gradients of
+// every block), then run_stage_sweeps over the blocks b0 <= b < b1 in any order (their
+// tiles of each direction's map; a block's sweeps read its neighbours' stage state and
+// viscous fluxes, which the stage before and run_stage_pre complete).  Together: the
+// kernels of launch_stage over the same tiles, without the residual.
+cudaError_t run_stage_pre(const Launch &L, int stage) {
+  cudaError_t e = run_bc(L, stage, 0, 0x7fffffff);
+  if (e != cudaSuccess || L.P.model != MODEL_NS) return e;
+  const int nt = L.tm_cells.tile_start[L.tm_cells.nblocks];
+  prim_kernel<<<nt, kCellTile, 0, L.stream>>>(L.d_blocks, L.tm_cells, L.P, L.d_state, stage);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  grad_kernel<<<nt, kCellTile, 0, L.stream>>>(L.d_blocks, L.tm_cells, L.P);
+  return cudaGetLastError();
+}
+cudaError_t run_stage_sweeps(const Launch &L, int stage, int b0, int b1) {
+  Launch P = L;
+  for (int d = 0; d < 3; ++d)
+    P.tm_dir[d] = tile_part(L.tm_dir[d], L.tm_dir[d].tile_start[b0], L.tm_dir[d].tile_start[b1]);
+  const int nsf = L.P.model == MODEL_NS ? SW_NS : 0;
+  cudaError_t e;
+  if ((e = launch_sweep<0>(P, stage, nsf)) != cudaSuccess) return e;
+  if ((e = launch_sweep<1>(P, stage, nsf)) != cudaSuccess) return e;
+  return launch_sweep<2>(P, stage, nsf | SW_RK | (stage == 2 && L.d_res_last ? SW_RES : 0));
+}
+
 cudaError_t run_bc(const Launch &L, int stage, int k0, int k1) {
   if (L.bc_tiles <= 0) return cudaSuccess;
   bc_ghost_kernel<<<L.bc_tiles, 256, 0, L.stream>>>(L.d_blocks, L.d_jobs, L.P, L.d_state, stage, k0, k1);

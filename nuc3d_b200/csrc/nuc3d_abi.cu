@@ -861,6 +861,16 @@ static bool slab_pipeline_ok(const nuc3d_ctx *c) {
 #endif
 constexpr int kHostPieces = NUC3D_HOST_PIECES;
 
+// nuc3d_solve_host's per-block stage 2 (contexts of several blocks, explicit schemes, no
+// learned sensor): the block sweeps of run_stage_sweeps.
+static bool block_pipeline_ok(const nuc3d_ctx *c) {
+  if (!c->host_pipeline || c->blocks.size() < 2 || c->P.sensor) return false;
+  for (int d = 0; d < 3; ++d)
+    if (c->P.scheme[d] == SCH_CRWENO5 || c->P.scheme[d] == SCH_HCCS || c->P.scheme[d] == SCH_HCCS77)
+      return false;
+  return true;
+}
+
 // The slabs of nuc3d_solve_host's pipeline are whole zeta chunks; a last chunk thinner than
 // kSlabMin planes joins the slab before it, so that every slab holds more planes than a
 // zeta stencil reaches (4) and a slab's stencils touch only its two neighbours' cells (and
@@ -1049,6 +1059,17 @@ int nuc3d_solve_host(nuc3d_ctx *c, double *const *q_host, int nsteps) {
     CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     c->ev_chunk.push_back(ev);
   }
+  // several blocks (explicit schemes, no sensor): stage 2 block by block, so that each
+  // block's download starts after its own zeta sweep instead of after the whole step
+  const int nb = (int)c->blocks.size();
+  const bool by_block = block_pipeline_ok(c);
+  while (by_block && (int)c->ev_zeta.size() < nb) {
+    cudaEvent_t ev;
+    CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    c->ev_zeta.push_back(ev);
+  }
+  const Launch &L = c->L;
+  auto run = [&](auto fast_fn, auto exact_fn) { return c->exact ? exact_fn() : fast_fn(); };
   auto dev = [&](const Chunk &k) { return reinterpret_cast<char *>(c->blocks[k.b].q[0]) + k.off; };
   auto host = [&](const Chunk &k) { return reinterpret_cast<char *>(q_host[k.b]) + k.off; };
   // uploads start after the work already queued on the context's stream
@@ -1063,10 +1084,30 @@ int nuc3d_solve_host(nuc3d_ctx *c, double *const *q_host, int nsteps) {
     }
     CUDA_TRY(cudaEventRecord(c->ev_h2d, c->h2d));
     CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_h2d, 0));
-    if (int r = nuc3d_step(c, 1)) return r;
-    CUDA_TRY(cudaEventRecord(c->ev_step, c->stream));
-    CUDA_TRY(cudaStreamWaitEvent(c->d2h, c->ev_step, 0));
+    if (by_block) {
+      // stages 0 and 1 whole; stage 2's ghost fluxes (and NS gradients) of every block,
+      // then each block's sweeps, whose last (zeta) releases that block's download
+      CUDA_TRY(cudaMemsetAsync(&c->d_state->max_eig_bits, 0, sizeof(unsigned long long), c->stream));
+      CUDA_TRY(c->stage(0, true, true));
+      CUDA_TRY(c->stage(1, true, false));
+      CUDA_TRY(run([&] { return nuc3d::fast::run_stage_pre(L, 2); },
+                   [&] { return nuc3d::exact::run_stage_pre(L, 2); }));
+      for (int b = 0; b < nb; ++b) {
+        CUDA_TRY(run([&] { return nuc3d::fast::run_stage_sweeps(L, 2, b, b + 1); },
+                     [&] { return nuc3d::exact::run_stage_sweeps(L, 2, b, b + 1); }));
+        CUDA_TRY(cudaEventRecord(c->ev_zeta[b], c->stream));
+      }
+      if (L.d_res_last)
+        CUDA_TRY(run([&] { return nuc3d::fast::run_residual(L, false); },
+                     [&] { return nuc3d::exact::run_residual(L, false); }));
+    } else {
+      if (int r = nuc3d_step(c, 1)) return r;
+      CUDA_TRY(cudaEventRecord(c->ev_step, c->stream));
+      CUDA_TRY(cudaStreamWaitEvent(c->d2h, c->ev_step, 0));
+    }
     for (size_t j = 0; j < chunks.size(); ++j) {
+      if (by_block && (j == 0 || chunks[j].b != chunks[j - 1].b))
+        CUDA_TRY(cudaStreamWaitEvent(c->d2h, c->ev_zeta[chunks[j].b], 0));
       CUDA_TRY(cudaMemcpyAsync(host(chunks[j]), dev(chunks[j]), chunks[j].bytes,
                                cudaMemcpyDeviceToHost, c->d2h));
       CUDA_TRY(cudaEventRecord(c->ev_chunk[j], c->d2h));

@@ -90,3 +90,41 @@ def test_uneven_blocks_fast(case):
     scale = max(float(np.max(np.abs(a))) for a in qref)
     err = max(float(np.max(np.abs(a - b))) for a, b in zip(q, qref))
     assert err <= 1e-11 * scale, err / scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("exact", [True, False])
+def test_solve_host_by_block_equals_device_steps(exact):
+    """nuc3d_solve_host on the 24 uneven blocks (one host array each): stage 2 runs block by
+    block after every block's ghost fluxes and gradients, and each block's download starts
+    after its own zeta sweep.  The same 3 steps as on the device-resident state, bit for bit:
+    every block, time, dt and the residual; the whole-step path (pipeline off) too."""
+    import nuc3d_b200 as nb
+    blocks, types, ids, params = _setup()
+
+    def make():
+        cfg = nb.Config(scheme_ivs=("weno5z",) * 3, riemann="AUSM", model="NavierStokes3d",
+                        reynolds=params["Reynolds"], mach=MT, prandtl=0.72, exact=exact)
+        s = nb.Solver(cfg)
+        for r, b in enumerate(blocks):
+            s.add_block(*b["shape"], types[r], ids[r])
+        for r, b in enumerate(blocks):
+            s.set_mesh(r, *b["nodes"])
+        s.finalize()
+        for r, b in enumerate(blocks):
+            s.set_q(r, b["q"])
+        return s
+
+    s1 = make()
+    s1.step(STEPS)
+    ref = [s1.get_q(r) for r in range(len(blocks))], s1.time_dt(), s1.residual()
+    s1.close()
+    for pipe in (True, False):
+        s2 = make()
+        s2.set_host_pipeline(pipe)
+        host = [np.ascontiguousarray(b["q"]).copy() for b in blocks]
+        s2.solve_host([h.ctypes.data for h in host], STEPS)
+        for r in range(len(blocks)):
+            assert np.array_equal(host[r], ref[0][r]), (pipe, r)
+        assert s2.time_dt() == ref[1] and s2.residual() == ref[2]
+        s2.close()
