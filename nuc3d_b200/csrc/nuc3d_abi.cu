@@ -929,12 +929,18 @@ static int solve_host_slabs(nuc3d_ctx *c, double *q_host, int nsteps) {
     int k0, k1;
     piece_range(p, k0, k1);
     if (k1 <= k0) return cudaSuccess;
+    // the piece's planes of the five components: one strided copy (5 rows, pitch N), or
+    // five copies where the pitch exceeds what the copy engines take (2^31 - 1 bytes)
+    const size_t off = (size_t)k0 * plane, width = (size_t)(k1 - k0) * plane * sizeof(double);
+    const size_t pitch = (size_t)b.N * sizeof(double);
+    const cudaMemcpyKind kind = up ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    if (pitch <= (size_t)0x7fffffff)
+      return up ? cudaMemcpy2DAsync(b.q[0] + off, pitch, q_host + off, pitch, width, 5, kind, st)
+                : cudaMemcpy2DAsync(q_host + off, pitch, b.q[0] + off, pitch, width, 5, kind, st);
     for (int v = 0; v < 5; ++v) {
-      const size_t off = (size_t)v * b.N + (size_t)k0 * plane, n = (size_t)(k1 - k0) * plane;
-      cudaError_t e = up ? cudaMemcpyAsync(b.q[0] + off, q_host + off, n * sizeof(double),
-                                           cudaMemcpyHostToDevice, st)
-                         : cudaMemcpyAsync(q_host + off, b.q[0] + off, n * sizeof(double),
-                                           cudaMemcpyDeviceToHost, st);
+      const size_t o = (size_t)v * b.N + off;
+      cudaError_t e = up ? cudaMemcpyAsync(b.q[0] + o, q_host + o, width, kind, st)
+                         : cudaMemcpyAsync(q_host + o, b.q[0] + o, width, kind, st);
       if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
