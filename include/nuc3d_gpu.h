@@ -259,9 +259,10 @@ int nuc3d_set_sensor_theta(nuc3d_ctx *ctx, float theta_min);
 int nuc3d_set_tiles(nuc3d_ctx *ctx, const int shape[3]);
 int nuc3d_get_tiles(nuc3d_ctx *ctx, int shape[3]);
 /* Time every shape of every explicit-scheme direction's right-hand-side sweep on the
-   current state, pipelined and not where the pipelined sweeps apply (reps launches each;
-   the state and the status word are left as they were, the RHS array is overwritten) and
-   keep the fastest per direction.  The choice is cached in the process per grid (block
+   current state, pipelined and not where the pipelined sweeps apply (two passes of reps
+   launches each, a candidate's faster pass counting; the state and the status word are
+   left as they were, the RHS array is overwritten) and keep the fastest per direction;
+   a pipelined sweep that gives up waiting for its loads returns NUC3D_ECUDA.  The choice is cached in the process per grid (block
    extents, schemes, model, build, hybrid or plain): a later context of the same grid takes
    it without timing.  shape_out (may be NULL): the shapes chosen; ms_out (may be NULL):
    9 doubles, ms per launch of direction d with shape s at [3d + s], -1 where not timed

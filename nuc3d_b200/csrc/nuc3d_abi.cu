@@ -857,7 +857,7 @@ static bool slab_pipeline_ok(const nuc3d_ctx *c) {
 }
 
 #ifndef NUC3D_HOST_PIECES
-#define NUC3D_HOST_PIECES 4  // copy pieces per slab
+#define NUC3D_HOST_PIECES 8  // copy pieces per slab (256^3: 17.45 ms per step against 17.66 with 4)
 #endif
 constexpr int kHostPieces = NUC3D_HOST_PIECES;
 
@@ -1215,6 +1215,9 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
       if (compact_scheme(c->P.scheme[d])) { best[d] = 0; continue; }
       double tbest = 1e300;
       int best_mode = (mask0 >> d) & 1;
+      // two passes over the candidates, each keeping its faster time: one disturbed
+      // measurement cannot decide the choice
+      for (int pass = 0; pass < 2; ++pass)
       for (int sh = 0; sh < kTileShapes; ++sh) {
         for (int mode = can_pipe ? 1 : 0; mode >= 0; --mode) {
           cur[d] = sh;
@@ -1231,6 +1234,9 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
           CUDA_TRY(cudaEventSynchronize(e1));
           float t = 0.0f;
           CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+          unsigned st = 0;  // a pipelined sweep that gave up waiting is a failure, not a time
+          CUDA_TRY(cudaMemcpy(&st, &c->d_state->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+          if (st & ST_PIPE_TIMEOUT) return fail(NUC3D_ECUDA, "autotune: a pipelined sweep timed out");
           const double ms = (double)t / reps;
           if (ms_out && (ms_out[3 * d + sh] < 0.0 || ms < ms_out[3 * d + sh])) ms_out[3 * d + sh] = ms;
           if (ms < tbest) { tbest = ms; best[d] = sh; best_mode = mode; }
