@@ -324,6 +324,7 @@ def ours(args):
             s.set_pipeline(args.pipe_mask if args.pipe_mask > 1 else bool(args.pipe_mask))
     else:
         tiles = s.autotune(reps=3)["shape"]
+    pipe_dirs_step = s.pipeline()  # directions the timed steps run pipelined (bit d)
 
     def barrier():
         if dist is not None:
@@ -402,7 +403,14 @@ def ours(args):
         hms = max_over_ranks(ev4.elapsed_time(ev5))
         rho_h = s.get_q(b)[0]
         s.set_sensor(None)
-        s.set_tiles(tiles)
+        # the plain grid's shapes and pipelined directions again (the hybrid's autotune set
+        # its own; the plain choice comes back from the autotuner's cache without timing)
+        if args.tiles:
+            s.set_tiles(tiles)
+            if args.pipe_mask is not None:
+                s.set_pipeline(args.pipe_mask if args.pipe_mask > 1 else bool(args.pipe_mask))
+        else:
+            s.autotune(reps=3)
         hv = whole_job_rate(world, cells, args.steps, hms)
         hybrid = {"value": hv, "unit": "Mcell-RK3-steps/s", "ms_per_step": hms / args.steps,
                   "vs_plain": hv / value, "logit_threshold": SENS.DEFAULT_THRESHOLD,
@@ -481,6 +489,7 @@ def ours(args):
                    "l2": "no flush: 3 state buffers of 671 MB + RHS + metrics = 4 GB > 126 MB L2",
                    "parallelism": f"replicas x{world} (one independent block per GPU)",
                    "tile_shapes": list(tiles),
+                   "pipelined_dirs": pipe_dirs_step,
                    "status_bits": status,
                    "energy_reset_cells": resets,
                    "energy_reset_note": "cells whose energy con2prim reset (e < 0, "
