@@ -1236,7 +1236,8 @@ int nuc3d_autotune(nuc3d_ctx *c, int reps, int shape_out[3], double ms_out[9]) {
           CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
           unsigned st = 0;  // a pipelined sweep that gave up waiting is a failure, not a time
           CUDA_TRY(cudaMemcpy(&st, &c->d_state->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
-          if (st & ST_PIPE_TIMEOUT) return fail(NUC3D_ECUDA, "autotune: a pipelined sweep timed out");
+          if (st & ~status0 & ST_PIPE_TIMEOUT)
+            return fail(NUC3D_ECUDA, "autotune: a pipelined sweep timed out");
           const double ms = (double)t / reps;
           if (ms_out && (ms_out[3 * d + sh] < 0.0 || ms < ms_out[3 * d + sh])) ms_out[3 * d + sh] = ms;
           if (ms < tbest) { tbest = ms; best[d] = sh; best_mode = mode; }
